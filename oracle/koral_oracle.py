@@ -1,0 +1,146 @@
+"""ctypes front end to the parity oracle (TEST INFRASTRUCTURE).
+
+Two CPU implementations of KORAL's hot path are reachable from here:
+
+* ``OracleGrid`` drives the C restatement in ``koral_oracle.c`` (run-time grid
+  size and scheme), built by ``oracle/Makefile`` into
+  ``oracle/_ref/libkoral_oracle.so``;
+* ``RefKoral`` drives the reference KORAL sources themselves, compiled per
+  problem by ``oracle/ref/build_ref.sh`` into ``oracle/_ref/libkref_*.so``.
+
+Only the tests, the smoke check and the CPU-baseline leg of the benchmark use
+this module; the product never imports it.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+ORACLE_LIB = os.path.join(REF_DIR, "libkoral_oracle.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _lib(path):
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"oracle library {path} is not built")
+    return ctypes.CDLL(path)
+
+
+class OracleGrid:
+    """One grid of the C restatement oracle."""
+
+    ARR = dict(u=0, p=1, g=2, G=3, gKr=4, gbx=5, gby=6, gbz=7, Gbx=8, Gby=9, Gbz=10,
+               flbx=11, flby=12, flbz=13, xbx=14, xby=15, xbz=16, xcx=17, xcy=18, xcz=19, emf=20)
+
+    _lib_handle = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib_handle is None:
+            L = _lib(ORACLE_LIB)
+            L.ko_grid_create.restype = ctypes.c_void_p
+            L.ko_grid_create.argtypes = [ctypes.c_int] * 6
+            L.ko_grid_destroy.argtypes = [ctypes.c_void_p]
+            L.ko_array.restype = _dp
+            L.ko_array.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            L.ko_scalar.restype = ctypes.c_double
+            L.ko_scalar.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            L.ko_set_scalar.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+            L.ko_set_physics.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+            L.ko_set_floors.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 5
+            L.ko_set_uniform_grid.argtypes = [ctypes.c_void_p, _dp, _dp]
+            L.ko_layout.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+            for fn in ("ko_set_minkowski_metric", "ko_set_bc", "ko_calc_wavespeeds", "ko_calc_u2p",
+                       "ko_save_timesteps", "ko_begin_run", "ko_init_orszag_tang"):
+                getattr(L, fn).argtypes = [ctypes.c_void_p]
+            L.ko_begin_step.argtypes = [ctypes.c_void_p]
+            L.ko_begin_step.restype = ctypes.c_double
+            L.ko_rk2_step.argtypes = [ctypes.c_void_p]
+            L.ko_op_explicit.argtypes = [ctypes.c_void_p, ctypes.c_double]
+            cls._lib_handle = L
+        return cls._lib_handle
+
+    def __init__(self, nx, ny, nz, ng, nv=9, axisym=0):
+        self.L = self.lib()
+        self.h = self.L.ko_grid_create(nx, ny, nz, ng, nv, axisym)
+        lay = (ctypes.c_int * 16)()
+        self.L.ko_layout(self.h, lay)
+        self.nx, self.ny, self.nz, self.ng, self.nv, self.sx, self.sy, self.sz, self.szmet = lay[:9]
+
+    def close(self):
+        if self.h:
+            self.L.ko_grid_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def array(self, name):
+        ptr = self.L.ko_array(self.h, self.ARR[name])
+        if name in ("u", "p"):
+            shape = (self.sz, self.sy, self.sx, self.nv)
+        else:
+            raise KeyError(name)
+        return np.ctypeslib.as_array(ptr, shape=shape)
+
+    def scalar(self, i):
+        return self.L.ko_scalar(self.h, i)
+
+    def set_physics(self, gamma, tsteplim, int_order, fluxmethod):
+        self.L.ko_set_physics(self.h, gamma, tsteplim, int_order, fluxmethod)
+
+    def set_uniform_grid(self, lo, hi):
+        lo = (ctypes.c_double * 3)(*lo)
+        hi = (ctypes.c_double * 3)(*hi)
+        self.L.ko_set_uniform_grid(self.h, lo, hi)
+
+    def __getattr__(self, name):
+        fn = getattr(self.lib(), "ko_" + name)
+        return lambda *a: fn(self.h, *a)
+
+
+def orszag_tang_oracle(n=128):
+    """Relativistic Orszag-Tang vortex on an n x n periodic grid, set up
+    exactly as the reference plug-in oracle/ref/problems/ORSZAGREL does."""
+    G = OracleGrid(n, n, 1, 3, 9)
+    G.set_physics(5.0 / 3.0, 0.5, 2, 0)
+    G.set_uniform_grid([0.0, 0.0, -1.0], [2 * np.pi, 2 * np.pi, 1.0])
+    G.set_minkowski_metric()
+    G.init_orszag_tang()
+    G.begin_run()
+    return G
+
+
+class RefKoral:
+    """The reference KORAL build for one problem (compile-time grid)."""
+
+    def __init__(self, libname):
+        path = os.path.join(REF_DIR, libname)
+        self.L = _lib(path)
+        sz = (ctypes.c_int * 16)()
+        self.L.kref_sizes(sz)
+        (self.nx, self.ny, self.nz, self.ng, self.nv, self.sx, self.sy, self.sz, self.szmet,
+         self.int_order, self.fluxmethod, self.timestepping, self.magn, self.rad, self.coords) = sz[:15]
+        self.L.kref_begin_step.restype = ctypes.c_double
+        self.L.op_explicit.argtypes = [ctypes.c_double, ctypes.c_double]
+        self.L.op_implicit.argtypes = [ctypes.c_double, ctypes.c_double]
+
+    def init(self):
+        self.L.kref_init()
+
+    def step(self, n=1):
+        return self.L.kref_nsteps(n)
+
+    def array(self, name, shape=None):
+        ptr = _dp.in_dll(self.L, name)
+        if shape is None:
+            shape = (self.sz, self.sy, self.sx, self.nv)
+        return np.ctypeslib.as_array(ptr, shape=shape)
+
+    def scalar(self, name):
+        return ctypes.c_double.in_dll(self.L, name).value
+
+    def set_scalar(self, name, v):
+        ctypes.c_double.in_dll(self.L, name).value = v
