@@ -1,0 +1,326 @@
+#!/usr/bin/env python
+"""Benchmark: FP64 zone-cycles/s of KORAL's per-step hot path on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload ot128]
+
+A step is one full RK2 time step (ko.c:571-626: two explicit operators and two
+inversions with fixups and boundary conditions) of the workload.  Workloads:
+
+  ot128   relativistic Orszag-Tang vortex, 128x128, PPM + LLF + flux-CT,
+          Minkowski, Gamma = 5/3, CFL 0.5 (the reference's CPU-runnable case)
+
+value  = cells x timed steps / device time (CUDA events on the library's own
+         stream, L2 flushed between steps, inputs resident in HBM)
+e2e    = same metric through the C-ABI with host buffers: every step uploads
+         u and p from pinned host memory, runs the step and downloads u and p
+N > 1  : one process per GPU (torchrun), each rank runs its own replica of the
+         workload (the path is one subdomain per GPU: replicas only), device
+         time is the maximum over ranks, value counts the cells of all ranks.
+--impl reference times the reference KORAL sources themselves (oracle/_ref,
+OpenMP build) on the host cores, same workload and metric.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 zone-cycles/s (1 B200)"
+UNIT = "zone-cycles/s"
+
+WORKLOADS = {
+    "ot128": dict(desc="relativistic Orszag-Tang vortex 128x128 (Minkowski, PPM+LLF+flux-CT, RK2, CFL 0.5, Gamma 5/3)",
+                  n=128, ref_lib="libkref_orszagrel_128_omp.so", ref_serial="libkref_orszagrel_128.so"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ot128", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.samples.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        mx = max(float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, nm in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path (oracle/_ref builds of the reference sources)
+# ---------------------------------------------------------------------------
+REF_CHILD = r"""
+import ctypes, json, os, sys, time
+sys.path.insert(0, {root!r})
+from oracle.koral_oracle import RefKoral
+R = RefKoral({lib!r}); R.init()
+R.step({warm})
+t0 = time.perf_counter(); R.step({steps}); t1 = time.perf_counter()
+print(json.dumps({{"seconds": t1 - t0, "cells": R.nx * R.ny * R.nz, "steps": {steps}}}))
+"""
+
+
+def run_reference_cpu(wl, steps, warm, threads):
+    lib = wl["ref_lib"] if threads > 1 else wl["ref_serial"]
+    path = os.path.join(ROOT, "oracle", "_ref", lib)
+    if not os.path.exists(path):
+        return None, f"{lib} not built (needs the reference tree at build time)"
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    code = REF_CHILD.format(root=ROOT, lib=lib, warm=warm, steps=steps)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=1800)
+    line = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    if r.returncode != 0 or not line:
+        return None, (r.stderr or r.stdout)[-300:]
+    d = json.loads(line[-1])
+    return d["cells"] * d["steps"] / d["seconds"], None
+
+
+def reference_arm(args, wl, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    # each step is one full RK2 step of the reference on all host cores
+    val, err = run_reference_cpu(wl, max(1, args.steps), max(0, args.warmup), threads)
+    if val is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    line = {
+        "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wl["n"] ** 2 / val * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["desc"], "parallelism": "openmp host threads"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{args.steps} RK2 steps after {args.warmup} warm-up steps"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def our_arm(args, wl, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import koral_b200
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    from koral_b200 import build
+    build.build()
+
+    n = wl["n"]
+    s = koral_b200.orszag_tang(n)
+    ext = torch.cuda.ExternalStream(s.stream, device=dev)
+    cells = n * n
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # 256 MB > 126 MB L2
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        dist = dist_
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up (graph capture happens here)
+    s.rk2_steps(max(1, args.warmup), graph=True)
+
+    def timed_steps(k, profile=False):
+        """k steps, L2 flushed before each; returns summed device ms."""
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+        if profile:
+            s.profile(True)
+            s.profile_reset()
+        for i in range(k):
+            with torch.cuda.stream(ext):
+                flush.fill_(float(i))
+                starts[i].record(ext)
+            if profile:
+                s.rk2_steps(1, graph=False)
+            else:
+                s.rk2_steps(1, graph=True)
+            with torch.cuda.stream(ext):
+                ends[i].record(ext)
+        torch.cuda.synchronize(dev)
+        if profile:
+            s.profile(False)
+        return sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+
+    barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = s.launches
+    with ClockSampler(local_rank) as clk:
+        ms = timed_steps(args.steps)
+    launches = s.launches - launches0
+    torch.cuda.synchronize(dev)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = cells * args.steps * world / (ms_max / 1e3)
+
+    # per-kernel device times (events around each launch, separate pass)
+    timed_steps(min(args.steps, 50), profile=True)
+    prof = s.profile_read()
+    total = sum(v[0] for v in prof.values())
+    top = max(prof.items(), key=lambda kv: kv[1][0])
+
+    # e2e through the C-ABI with pinned host buffers
+    shape = s.shape
+    hu = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+    hp = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+    u0, p0 = s.download_state()
+    hu.numpy()[...] = u0
+    hp.numpy()[...] = p0
+    L = koral_b200.lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    pu = ctypes.cast(hu.data_ptr(), dp)
+    pp = ctypes.cast(hp.data_ptr(), dp)
+    ke = max(1, min(args.steps, 100))
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(ext):
+        e0.record(ext)
+    for _ in range(ke):
+        koral_b200._check(L.kgpu_upload_state(s.h, pu, pp), "upload")
+        koral_b200._check(L.kgpu_rk2_steps(s.h, 1), "step")
+        koral_b200._check(L.kgpu_download_state(s.h, pu, pp), "download")
+    with torch.cuda.stream(ext):
+        e1.record(ext)
+    torch.cuda.synchronize(dev)
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = cells * ke * world / (float(t.item()) / 1e3)
+    state_bytes = 2 * int(np.prod(shape)) * 8
+
+    if rank != 0:
+        return
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    # algorithmic bytes of the face-flux kernels: 16*NV bytes per face
+    # (read the primitives once, write the face flux once)
+    nv = 9
+    nfaces = (n + 1) * (n + 2)
+    flux_ms = prof["k_flux_x"][0] / max(1, prof["k_flux_x"][1])
+    flux_gbs = 16 * nv * nfaces / (flux_ms / 1e3) / 1e9 if flux_ms > 0 else None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["desc"], "cells_per_gpu": cells, "l2": "flushed (256 MB write) before every step",
+                   "parallelism": "replicas" if world > 1 else "single subdomain", "graph": "one CUDA graph per RK2 step"},
+        "roofline": {"kernel": "k_flux_x", "bound": "hbm", "achieved": flux_gbs, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": (flux_gbs / hbm_peak) if flux_gbs else None, "traffic": None,
+                     "peak_source": peak_src, "algorithmic_bytes_per_launch": 16 * nv * nfaces},
+        "kernels": {k: {"ms_per_launch": v[0] / max(1, v[1]), "share": v[0] / total if total else 0.}
+                    for k, v in prof.items() if v[1]},
+        "top_kernel": top[0],
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        val, err = run_reference_cpu(wl, 10, 2, threads)
+        if val is not None:
+            line["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": threads, "kind": "reference",
+                                    "sample": "10 RK2 steps of the same workload after 2 warm-up steps"}
+        else:
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
+                                    "sample": f"unavailable: {err}"}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    wl = WORKLOADS[args.workload]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args, wl, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        our_arm(args, wl, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

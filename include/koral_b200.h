@@ -1,0 +1,177 @@
+/*
+ * koral_b200 — C-ABI boundary of the B200 (sm_100a) implementation of
+ * KORAL's per-step hot path.
+ *
+ * The reference is a C code whose time loop (solve_the_problem, ko.c:259-914)
+ * calls a small set of grid operators on global arrays, and whose per-cell
+ * solvers take plain double arrays plus a struct geometry.  This header
+ * exposes the same operators and solvers behind an opaque device context:
+ * the host keeps KORAL's own loop and calls these entry points instead of the
+ * CPU routines; state, metric tables and flags live in HBM between calls.
+ *
+ * Conventions
+ *  - All arrays crossing this boundary are HOST pointers in KORAL's own
+ *    layout: cell arrays are [SZ][SY][SX][NV] doubles with ghost cells
+ *    (ko.h:505-508), metric tables hold gSIZE=20 doubles per point
+ *    (g_{mu nu} in [i][j], d ln(gdet)/dx^i in [i][4], gdet in [3][4]; the
+ *    inverse table holds g^{mu nu} and the g_tt perturbation in [3][4]),
+ *    Christoffel tables hold 64 doubles per point (ko.h:113, misc.c:122-186).
+ *  - Every function returns 0 on success and a negative KGPU_E* code on
+ *    failure; no function aborts the process.
+ *  - One context is used by one host thread; calls are ordered on the
+ *    context's CUDA stream.  Functions that return data to the host
+ *    synchronise that stream.
+ */
+#ifndef KORAL_B200_H
+#define KORAL_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KGPU_ABI_VERSION 1
+
+/* error codes */
+#define KGPU_OK 0
+#define KGPU_EINVAL (-1)      /* bad argument or unsupported configuration   */
+#define KGPU_ECUDA (-2)       /* a CUDA runtime call failed                   */
+#define KGPU_ENOMEM (-3)      /* device allocation failed                     */
+#define KGPU_ESTATE (-4)      /* call out of order (e.g. no metric uploaded)  */
+
+/* reconstruction / Riemann solver / time integrator choices
+ * (INT_ORDER, FLUXMETHOD, TIMESTEPPING; choices.h:150-160, mnemonics.h:117-124) */
+#define KGPU_PPM 2
+#define KGPU_MP5 4
+#define KGPU_LAXF 0
+#define KGPU_HLL 1
+
+/* which state array an array-algebra call addresses (u, p, ut0, ut1) */
+#define KGPU_ARR_U 0
+#define KGPU_ARR_P 1
+#define KGPU_ARR_UT0 2
+#define KGPU_ARR_UT1 3
+
+typedef struct kgpu_ctx kgpu_ctx;
+
+/* Compile-time choices of a KORAL problem build (define.h/choices.h),
+ * given at run time here. */
+typedef struct {
+  int nx, ny, nz;          /* TNX, TNY, TNZ (one subdomain)                  */
+  int ng;                  /* ghost layers, NG (3 for PPM, 4 for MP5)        */
+  int nv;                  /* variables per cell, NV (9: MHD)                 */
+  int int_order;           /* KGPU_PPM or KGPU_MP5                           */
+  int fluxmethod;          /* KGPU_LAXF or KGPU_HLL                          */
+  int axisym_metric;       /* METRICAXISYMMETRIC: one phi slice of metric     */
+  int periodic[3];         /* PERIODIC_XBC/YBC/ZBC                            */
+  double gamma;            /* GAMMA                                           */
+  double tsteplim;         /* TSTEPLIM (Courant number)                       */
+  double rhofloor;         /* RHOFLOOR                                        */
+  double uurhoratiomin;    /* UURHORATIOMIN                                   */
+  double uurhoratiomax;    /* UURHORATIOMAX                                   */
+  double b2rhoratiomax;    /* B2RHORATIOMAX                                   */
+  double gammamaxhd;       /* GAMMAMAXHD                                      */
+  double u2pconv;          /* U2PCONV                                         */
+} kgpu_config;
+
+/* Fill a config with KORAL's defaults (choices.h) for an nx x ny x nz grid. */
+int kgpu_default_config(kgpu_config *cfg, int nx, int ny, int nz);
+
+/* Allocates the device state for one subdomain (initialize_arrays,
+ * misc.c:98-289) on the current CUDA device. */
+int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out);
+int kgpu_destroy(kgpu_ctx *ctx);
+
+/* Cell-face coordinates per axis, KORAL layout xb[ic+NG], ic in [-NG, N+NG]
+ * (set_grid, finite.c:1629-1699).  Also sets the minimum cell sizes used
+ * for the first time step. */
+int kgpu_upload_grid(kgpu_ctx *ctx, const double *xb_x, const double *xb_y, const double *xb_z);
+/* Uniform grid in code coordinates, as calc_xb (problem.c:9-36) builds it. */
+int kgpu_set_uniform_grid(kgpu_ctx *ctx, const double lo[3], const double hi[3]);
+
+/* Metric tables as calc_metric (metric.c:3866-4075) leaves them: centres
+ * (g, G, gKr) and the three face sets (gbx..gbz, Gbx..Gbz). */
+int kgpu_upload_metric(kgpu_ctx *ctx, const double *g, const double *G, const double *gKr,
+                       const double *gbx, const double *gby, const double *gbz,
+                       const double *Gbx, const double *Gby, const double *Gbz);
+/* Flat spacetime (MINKCOORDS) tables generated on the device. */
+int kgpu_set_minkowski_metric(kgpu_ctx *ctx);
+
+/* Conserved (u) and primitive (p) arrays, whole padded grid. */
+int kgpu_upload_state(kgpu_ctx *ctx, const double *u, const double *p);
+int kgpu_download_state(kgpu_ctx *ctx, double *u, double *p);
+int kgpu_download_array(kgpu_ctx *ctx, int which, double *out);
+
+/* Grid operators of KORAL's time loop. ------------------------------------ */
+/* op_explicit(t,dt), finite.c:646-1234 (set_bc, wavespeeds, reconstruction,
+ * face fluxes, flux-CT, unsplit update with metric source terms). */
+int kgpu_op_explicit(kgpu_ctx *ctx, double t, double dt);
+/* op_implicit(t,dt), finite.c:1241-1292: radiation source; a no-op for MHD. */
+int kgpu_op_implicit(kgpu_ctx *ctx, double t, double dt);
+/* calc_u2p(), finite.c:501-561: inversion, floors, fixups, set_bc. */
+int kgpu_calc_u2p(kgpu_ctx *ctx);
+/* set_bc(t,ifinit), finite.c:2752-4463. */
+int kgpu_set_bc(kgpu_ctx *ctx, double t, int ifinit);
+/* save_timesteps(), finite.c:404-496 (no SELFTIMESTEP: nothing to store). */
+int kgpu_save_timesteps(kgpu_ctx *ctx);
+/* copyi_u(factor,src,dst), finite.c:2492; addi_u(f1,a,f2,b,c), finite.c:2545. */
+int kgpu_copyi_u(kgpu_ctx *ctx, double factor, int src, int dst);
+int kgpu_addi_u(kgpu_ctx *ctx, double f1, int a, double f2, int b, int c);
+
+/* Time-step bookkeeping of solve_the_problem (ko.c:290-313, 399-425). ----- */
+/* Initial 1/dt from max_ws = 10000 (ko.c:290-300). */
+int kgpu_begin_run(kgpu_ctx *ctx);
+/* dt = 1/tstepdenmax, then reset of the running maximum (ko.c:399-425). */
+int kgpu_begin_step(kgpu_ctx *ctx, double *dt_out);
+int kgpu_get_tstepdenmax(kgpu_ctx *ctx, double *out);
+int kgpu_set_tstepdenmax(kgpu_ctx *ctx, double v);
+
+/* Whole RK2 steps (ko.c:571-626) enqueued on the device without a host
+ * round trip: dt stays in device memory.  nsteps >= 1. */
+int kgpu_rk2_steps(kgpu_ctx *ctx, int nsteps);
+/* Same, replayed from a CUDA graph captured on the first call. */
+int kgpu_rk2_steps_graph(kgpu_ctx *ctx, int nsteps);
+
+/* Counters of the last calc_u2p calls since kgpu_reset_counters:
+ * out[0] cells flagged for fixup, out[1] entropy inversions,
+ * out[2] failed inversions (old primitives kept), out[3] negative densities. */
+int kgpu_get_counters(kgpu_ctx *ctx, unsigned long long out[4]);
+int kgpu_reset_counters(kgpu_ctx *ctx);
+
+/* Problem set-up helpers (host-side, then uploaded). ---------------------- */
+/* Relativistic Orszag-Tang vortex on the current grid (Minkowski metric). */
+int kgpu_init_orszag_tang(kgpu_ctx *ctx);
+
+/* Batched per-cell solvers (host arrays, n cells, one metric point each:
+ * g and G hold 20 doubles per cell).  They replace per-cell calls of
+ *   int u2p(ldouble *uu, ldouble *pp, void *geom, int corrected[3],
+ *           int fixups[2], int type)                          u2p.c:176
+ *   int p2u(ldouble *p, ldouble *u, void *geom)               p2u.c:40
+ *   int check_floors_mhd(ldouble *pp, int whichvel, void *geom) u2p.c:492
+ * pp is input (initial guess) and output; status[i] is u2p's return value. */
+int kgpu_u2p_cells(int n, const kgpu_config *cfg, const double *uu, double *pp,
+                   const double *g, const double *G, int *status, int *fixup);
+int kgpu_p2u_cells(int n, const kgpu_config *cfg, const double *pp, double *uu,
+                   const double *g, const double *G);
+
+/* Instrumentation. ------------------------------------------------------- */
+/* The context's CUDA stream (cudaStream_t), for events and copies that must
+ * be ordered with the operators. */
+int kgpu_get_stream(kgpu_ctx *ctx, void **stream);
+/* When enabled, every launch outside a CUDA graph is bracketed by CUDA
+ * events; kgpu_profile_read returns the summed device time and launch count
+ * of one kernel kind (0 <= kernel < kgpu_num_kernels()) and its name. */
+int kgpu_profile_enable(kgpu_ctx *ctx, int on);
+int kgpu_profile_read(kgpu_ctx *ctx, int kernel, double *total_ms, long long *count, const char **name);
+int kgpu_profile_reset(kgpu_ctx *ctx);
+int kgpu_num_kernels(void);
+/* Kernels launched by this context so far (graph replays included). */
+int kgpu_launch_count(kgpu_ctx *ctx, long long *out);
+
+/* Last CUDA error string of this thread's most recent failing call. */
+const char *kgpu_last_error(void);
+int kgpu_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,317 @@
+"""koral_b200: B200 (sm_100a) implementation of KORAL's per-step hot path.
+
+The package is a thin host-side mirror of KORAL's own operator interface
+(op_explicit, op_implicit, calc_u2p, set_bc, copyi_u, addi_u, save_timesteps,
+finite.c) over the C-ABI library ``_lib/libkoral_b200.so`` declared in
+``include/koral_b200.h``.  Arrays cross the boundary in KORAL's layout
+(cell-major, variable fastest, ghost cells included: ``[SZ][SY][SX][NV]``).
+
+There is no CPU fallback: if the CUDA library is missing or no GPU is
+visible, constructing a ``Subdomain`` raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libkoral_b200.so")
+
+PPM, MP5 = 2, 4
+LAXF, HLL = 0, 1
+ARR_U, ARR_P, ARR_UT0, ARR_UT1 = 0, 1, 2, 3
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class KgpuError(RuntimeError):
+    pass
+
+
+class Config(ctypes.Structure):
+    """kgpu_config of include/koral_b200.h."""
+
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("ng", ctypes.c_int), ("nv", ctypes.c_int),
+        ("int_order", ctypes.c_int), ("fluxmethod", ctypes.c_int),
+        ("axisym_metric", ctypes.c_int), ("periodic", ctypes.c_int * 3),
+        ("gamma", ctypes.c_double), ("tsteplim", ctypes.c_double),
+        ("rhofloor", ctypes.c_double), ("uurhoratiomin", ctypes.c_double),
+        ("uurhoratiomax", ctypes.c_double), ("b2rhoratiomax", ctypes.c_double),
+        ("gammamaxhd", ctypes.c_double), ("u2pconv", ctypes.c_double),
+    ]
+
+
+_LIB = None
+
+
+def lib():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise KgpuError(f"{LIB_PATH} is missing: build it with koral_b200.build.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        sig = {
+            "kgpu_default_config": [ctypes.POINTER(Config), ctypes.c_int, ctypes.c_int, ctypes.c_int],
+            "kgpu_create": [ctypes.POINTER(Config), ctypes.POINTER(vp)],
+            "kgpu_destroy": [vp],
+            "kgpu_upload_grid": [vp, _dp, _dp, _dp],
+            "kgpu_set_uniform_grid": [vp, _dp, _dp],
+            "kgpu_upload_metric": [vp] + [_dp] * 9,
+            "kgpu_set_minkowski_metric": [vp],
+            "kgpu_upload_state": [vp, _dp, _dp],
+            "kgpu_download_state": [vp, _dp, _dp],
+            "kgpu_download_array": [vp, ctypes.c_int, _dp],
+            "kgpu_op_explicit": [vp, ctypes.c_double, ctypes.c_double],
+            "kgpu_op_implicit": [vp, ctypes.c_double, ctypes.c_double],
+            "kgpu_calc_u2p": [vp],
+            "kgpu_set_bc": [vp, ctypes.c_double, ctypes.c_int],
+            "kgpu_save_timesteps": [vp],
+            "kgpu_copyi_u": [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int],
+            "kgpu_addi_u": [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int],
+            "kgpu_begin_run": [vp],
+            "kgpu_begin_step": [vp, _dp],
+            "kgpu_get_tstepdenmax": [vp, _dp],
+            "kgpu_set_tstepdenmax": [vp, ctypes.c_double],
+            "kgpu_rk2_steps": [vp, ctypes.c_int],
+            "kgpu_rk2_steps_graph": [vp, ctypes.c_int],
+            "kgpu_get_counters": [vp, ctypes.POINTER(ctypes.c_ulonglong)],
+            "kgpu_reset_counters": [vp],
+            "kgpu_init_orszag_tang": [vp],
+            "kgpu_u2p_cells": [ctypes.c_int, ctypes.POINTER(Config), _dp, _dp, _dp, _dp,
+                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+            "kgpu_p2u_cells": [ctypes.c_int, ctypes.POINTER(Config), _dp, _dp, _dp, _dp],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        L.kgpu_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.kgpu_profile_enable.argtypes = [vp, ctypes.c_int]
+        L.kgpu_profile_read.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_longlong),
+                                        ctypes.POINTER(ctypes.c_char_p)]
+        L.kgpu_profile_reset.argtypes = [vp]
+        L.kgpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.kgpu_last_error.restype = ctypes.c_char_p
+        L.kgpu_abi_version.restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def _check(rc, what):
+    if rc != 0:
+        msg = lib().kgpu_last_error().decode(errors="replace")
+        raise KgpuError(f"{what} failed with code {rc}: {msg}")
+
+
+def _ptr(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def default_config(nx, ny, nz, **kw):
+    c = Config()
+    _check(lib().kgpu_default_config(ctypes.byref(c), nx, ny, nz), "kgpu_default_config")
+    for k, v in kw.items():
+        if k == "periodic":
+            for i in range(3):
+                c.periodic[i] = int(v[i])
+        else:
+            setattr(c, k, v)
+    return c
+
+
+class Subdomain:
+    """One KORAL tile resident on the current GPU.
+
+    Methods are named after the reference routines they replace and keep
+    their argument meaning (finite.c:501-2620, ko.c:290-626).
+    """
+
+    def __init__(self, cfg):
+        self.cfg = cfg
+        self.L = lib()
+        h = ctypes.c_void_p()
+        _check(self.L.kgpu_create(ctypes.byref(cfg), ctypes.byref(h)), "kgpu_create")
+        self.h = h
+        ng = cfg.ng
+        self.sx = cfg.nx + 2 * ng
+        self.sy = cfg.ny + 2 * ng if cfg.ny > 1 else 1
+        self.sz = cfg.nz + 2 * ng if cfg.nz > 1 else 1
+        self.nv = cfg.nv
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.kgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        return (self.sz, self.sy, self.sx, self.nv)
+
+    # set-up
+    def set_uniform_grid(self, lo, hi):
+        lo = np.ascontiguousarray(lo, dtype=np.float64)
+        hi = np.ascontiguousarray(hi, dtype=np.float64)
+        _check(self.L.kgpu_set_uniform_grid(self.h, _ptr(lo), _ptr(hi)), "kgpu_set_uniform_grid")
+
+    def upload_grid(self, xbx, xby, xbz):
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (xbx, xby, xbz)]
+        _check(self.L.kgpu_upload_grid(self.h, *[_ptr(x) for x in a]), "kgpu_upload_grid")
+
+    def set_minkowski_metric(self):
+        _check(self.L.kgpu_set_minkowski_metric(self.h), "kgpu_set_minkowski_metric")
+
+    def upload_metric(self, g, G, gKr, gbx, gby, gbz, Gbx, Gby, Gbz):
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (g, G, gKr, gbx, gby, gbz, Gbx, Gby, Gbz)]
+        _check(self.L.kgpu_upload_metric(self.h, *[_ptr(x) for x in a]), "kgpu_upload_metric")
+
+    def init_orszag_tang(self):
+        _check(self.L.kgpu_init_orszag_tang(self.h), "kgpu_init_orszag_tang")
+
+    # state transfer
+    def upload_state(self, u, p):
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.shape)
+        p = np.ascontiguousarray(p, dtype=np.float64).reshape(self.shape)
+        _check(self.L.kgpu_upload_state(self.h, _ptr(u), _ptr(p)), "kgpu_upload_state")
+
+    def download_state(self):
+        u = np.empty(self.shape)
+        p = np.empty(self.shape)
+        _check(self.L.kgpu_download_state(self.h, _ptr(u), _ptr(p)), "kgpu_download_state")
+        return u, p
+
+    def download(self, which):
+        a = np.empty(self.shape)
+        _check(self.L.kgpu_download_array(self.h, which, _ptr(a)), "kgpu_download_array")
+        return a
+
+    # KORAL operators
+    def op_explicit(self, t, dt):
+        _check(self.L.kgpu_op_explicit(self.h, t, dt), "kgpu_op_explicit")
+
+    def op_implicit(self, t, dt):
+        _check(self.L.kgpu_op_implicit(self.h, t, dt), "kgpu_op_implicit")
+
+    def calc_u2p(self):
+        _check(self.L.kgpu_calc_u2p(self.h), "kgpu_calc_u2p")
+
+    def set_bc(self, t=0.0, ifinit=0):
+        _check(self.L.kgpu_set_bc(self.h, t, ifinit), "kgpu_set_bc")
+
+    def save_timesteps(self):
+        _check(self.L.kgpu_save_timesteps(self.h), "kgpu_save_timesteps")
+
+    def copyi_u(self, factor, src, dst):
+        _check(self.L.kgpu_copyi_u(self.h, factor, src, dst), "kgpu_copyi_u")
+
+    def addi_u(self, f1, a, f2, b, c):
+        _check(self.L.kgpu_addi_u(self.h, f1, a, f2, b, c), "kgpu_addi_u")
+
+    # time-step bookkeeping
+    def begin_run(self):
+        _check(self.L.kgpu_begin_run(self.h), "kgpu_begin_run")
+
+    def begin_step(self):
+        dt = ctypes.c_double()
+        _check(self.L.kgpu_begin_step(self.h, ctypes.byref(dt)), "kgpu_begin_step")
+        return dt.value
+
+    @property
+    def tstepdenmax(self):
+        v = ctypes.c_double()
+        _check(self.L.kgpu_get_tstepdenmax(self.h, ctypes.byref(v)), "kgpu_get_tstepdenmax")
+        return v.value
+
+    @tstepdenmax.setter
+    def tstepdenmax(self, v):
+        _check(self.L.kgpu_set_tstepdenmax(self.h, float(v)), "kgpu_set_tstepdenmax")
+
+    def rk2_steps(self, n=1, graph=False):
+        fn = self.L.kgpu_rk2_steps_graph if graph else self.L.kgpu_rk2_steps
+        _check(fn(self.h, int(n)), "kgpu_rk2_steps")
+
+    def counters(self):
+        a = (ctypes.c_ulonglong * 4)()
+        _check(self.L.kgpu_get_counters(self.h, a), "kgpu_get_counters")
+        return dict(fixups=a[0], entropy=a[1], failed=a[2], negrho=a[3])
+
+    @property
+    def stream(self):
+        """The context's cudaStream_t as an integer handle."""
+        v = ctypes.c_void_p()
+        _check(self.L.kgpu_get_stream(self.h, ctypes.byref(v)), "kgpu_get_stream")
+        return v.value or 0
+
+    def profile(self, on=True):
+        _check(self.L.kgpu_profile_enable(self.h, int(on)), "kgpu_profile_enable")
+
+    def profile_reset(self):
+        _check(self.L.kgpu_profile_reset(self.h), "kgpu_profile_reset")
+
+    def profile_read(self):
+        """{kernel name: (total ms, launches)} since the last reset."""
+        out = {}
+        for k in range(self.L.kgpu_num_kernels()):
+            ms = ctypes.c_double()
+            n = ctypes.c_longlong()
+            nm = ctypes.c_char_p()
+            _check(self.L.kgpu_profile_read(self.h, k, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(nm)),
+                   "kgpu_profile_read")
+            out[nm.value.decode()] = (ms.value, n.value)
+        return out
+
+    @property
+    def launches(self):
+        v = ctypes.c_longlong()
+        _check(self.L.kgpu_launch_count(self.h, ctypes.byref(v)), "kgpu_launch_count")
+        return v.value
+
+    def reset_counters(self):
+        _check(self.L.kgpu_reset_counters(self.h), "kgpu_reset_counters")
+
+
+def orszag_tang(n=128, graph_ok=True):
+    """Relativistic Orszag-Tang vortex on an n x n periodic grid."""
+    cfg = default_config(n, n, 1, ng=3, int_order=PPM, fluxmethod=LAXF, gamma=5.0 / 3.0, tsteplim=0.5)
+    s = Subdomain(cfg)
+    s.set_uniform_grid([0.0, 0.0, -1.0], [2 * np.pi, 2 * np.pi, 1.0])
+    s.set_minkowski_metric()
+    s.init_orszag_tang()
+    s.begin_run()
+    return s
+
+
+def u2p_cells(cfg, uu, pp, g, G):
+    """Batched u2p (u2p.c:176) of n independent cells; returns (pp, status, fixup)."""
+    uu = np.ascontiguousarray(uu, dtype=np.float64)
+    pp = np.ascontiguousarray(pp, dtype=np.float64).copy()
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    n = uu.shape[0]
+    st = np.zeros(n, dtype=np.int32)
+    fx = np.zeros(n, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    _check(lib().kgpu_u2p_cells(n, ctypes.byref(cfg), _ptr(uu), _ptr(pp), _ptr(g), _ptr(G),
+                                st.ctypes.data_as(ip), fx.ctypes.data_as(ip)), "kgpu_u2p_cells")
+    return pp, st, fx
+
+
+def p2u_cells(cfg, pp, g, G):
+    """Batched p2u (p2u.c:40) of n independent cells."""
+    pp = np.ascontiguousarray(pp, dtype=np.float64)
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    uu = np.empty_like(pp)
+    _check(lib().kgpu_p2u_cells(pp.shape[0], ctypes.byref(cfg), _ptr(pp), _ptr(uu), _ptr(g), _ptr(G)),
+           "kgpu_p2u_cells")
+    return uu

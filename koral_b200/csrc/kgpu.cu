@@ -1,0 +1,1397 @@
+// Kernels and C-ABI of the B200 implementation of KORAL's MHD hot path.
+//
+// Data layout in HBM: every cell array is structure-of-arrays,
+// [variable][z][y][x] with KORAL's ghost padding, so that a warp reads 32
+// consecutive x-cells of one variable in one coalesced transaction.  The
+// metric tables are [component][point]; with an axisymmetric metric only one
+// phi slice is stored, which keeps them L2-resident.
+//
+// One explicit operator (op_explicit, finite.c:646-1234) is four launches:
+//   k_wavespeeds  cell speeds of loop_1 + the CFL maximum (atomic on bits)
+//   k_flux<d>     per face: reconstruction of both sides, floors, fluxes,
+//                 p2u of both states and the LLF/HLL combination, fused; the
+//                 reference's face-state and one-sided-flux arrays never
+//                 reach HBM
+//   k_emf         corner EMFs of flux-CT (magn.c:199-297)
+//   k_update      metric source terms and the unsplit update; the
+//                 magnetic-field fluxes that flux_ct() rewrites are formed
+//                 here directly from the EMFs (magn.c:300-337)
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "../../include/koral_b200.h"
+#include "kgpu_physics.cuh"
+
+using namespace kgpu;
+
+// ---------------------------------------------------------------------------
+// error plumbing
+// ---------------------------------------------------------------------------
+static thread_local char g_lasterr[256] = "";
+static int set_err(const char *what, cudaError_t e) {
+  snprintf(g_lasterr, sizeof(g_lasterr), "%s: %s", what, cudaGetErrorString(e));
+  return KGPU_ECUDA;
+}
+#define CK(call)                                  \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return set_err(#call, e_); \
+  } while (0)
+#define CKL(what)                                 \
+  do {                                            \
+    cudaError_t e_ = cudaGetLastError();          \
+    if (e_ != cudaSuccess) return set_err(what, e_); \
+  } while (0)
+
+extern "C" const char *kgpu_last_error(void) { return g_lasterr; }
+extern "C" int kgpu_abi_version(void) { return KGPU_ABI_VERSION; }
+
+// ---------------------------------------------------------------------------
+// launch geometry: a 3D index box flattened with x fastest
+// ---------------------------------------------------------------------------
+struct Box {
+  int x0, y0, z0, nx, ny, nz;
+  long n() const { return (long)nx * ny * nz; }
+};
+__device__ inline bool box_coord(const Box &b, long t, int &ix, int &iy, int &iz) {
+  if (t >= (long)b.nx * b.ny * b.nz) return false;
+  ix = b.x0 + (int)(t % b.nx);
+  long r = t / b.nx;
+  iy = b.y0 + (int)(r % b.ny);
+  iz = b.z0 + (int)(r / b.ny);
+  return true;
+}
+static inline unsigned nblocks(long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+__device__ inline bool in_domain(const Grid &G, int ix, int iy, int iz) {
+  return ix >= 0 && ix < G.nx && iy >= 0 && iy < G.ny && iz >= 0 && iz < G.nz;
+}
+// finite.c:2641-2666: ghost cells that touch the domain through a face only
+__device__ inline bool outside_gc(const Grid &G, int ix, int iy, int iz) {
+  bool inx = ix >= 0 && ix < G.nx, iny = iy >= 0 && iy < G.ny, inz = iz >= 0 && iz < G.nz;
+  return !((!inx && iny && inz) || (inx && !iny && inz) || (inx && iny && !inz) || (inx && iny && inz));
+}
+
+__device__ inline void load_cell(const double *arr, long ncell, long c, int nv, double *v) {
+  for (int iv = 0; iv < nv; iv++) v[iv] = arr[iv * ncell + c];
+}
+__device__ inline void store_cell(double *arr, long ncell, long c, int nv, const double *v) {
+  for (int iv = 0; iv < nv; iv++) arr[iv * ncell + c] = v[iv];
+}
+
+// ---------------------------------------------------------------------------
+// boundary conditions (set_bc, finite.c:2752-2803; set_bc_core 2673-2748)
+// ---------------------------------------------------------------------------
+__global__ void k_bc_faces(Grid G, Box b) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  if (in_domain(G, ix, iy, iz) || outside_gc(G, ix, iy, iz)) return;
+  int iix = ix, iiy = iy, iiz = iz;
+  if (ix < 0 || ix >= G.nx) {
+    if (ix < 0) iix = ix + G.nx;
+    if (ix > G.nx - 1) iix = ix - G.nx;
+  } else if (iy < 0 || iy >= G.ny) {
+    if (iy < 0) iiy = iy + G.ny;
+    if (iy > G.ny - 1) iiy = iy - G.ny;
+    if (G.ny < G.ng) iiy = 0;
+  } else {
+    if (iz < 0) iiz = iz + G.nz;
+    if (iz > G.nz - 1) iiz = iz - G.nz;
+    if (G.nz < G.ng) iiz = 0;
+  }
+  long c = cell_index(G, ix, iy, iz), s = cell_index(G, iix, iiy, iiz);
+  double pp[NVMAX], uu[NVMAX];
+  load_cell(G.p, G.ncell, s, G.nv, pp);
+  Geom g;
+  geom_centre(G, ix, iy, iz, g);
+  p2u_full(G, pp, uu, g);
+  store_cell(G.p, G.ncell, c, G.nv, pp);
+  store_cell(G.u, G.ncell, c, G.nv, uu);
+}
+
+// Corners of a 2D periodic domain, filled as the reference does
+// (finite.c:3075-3328): the first NG-1 cells of the two edges next to each
+// corner copy the adjacent edge ghost row/column, the diagonal cells take
+// the periodic image (written there as the mean of two equal cells).
+__device__ inline void corner2d_op(const Grid &G, int op, int &tx, int &ty, int &ax, int &ay, int &bx, int &by) {
+  const int NX = G.nx, NY = G.ny, NG = G.ng;
+  int per = 2 * NG;             // ops per corner
+  int corner = op / per, k = op % per;
+  // within a corner: k < 2(NG-1): copies (two per i); then the two diagonal cells
+  if (k < 2 * (NG - 1)) {
+    int i = k / 2, second = k % 2;
+    switch (corner) {
+      case 0:  // bottom-left
+        if (!second) { tx = -NG + i; ty = -1; ax = bx = -NG + i; ay = by = 0; }
+        else { tx = -1; ty = -NG + i; ax = bx = 0; ay = by = -NG + i; }
+        break;
+      case 1:  // top-left
+        if (!second) { tx = -NG + i; ty = NY; ax = bx = -NG + i; ay = by = NY - 1; }
+        else { tx = -1; ty = NY + i + 1; ax = bx = 0; ay = by = NY + i + 1; }
+        break;
+      case 2:  // bottom-right
+        if (!second) { tx = NX + i + 1; ty = -1; ax = bx = NX + i + 1; ay = by = 0; }
+        else { tx = NX; ty = -NG + i; ax = bx = NX - 1; ay = by = -NG + i; }
+        break;
+      default:  // top-right
+        if (!second) { tx = NX + i + 1; ty = NY; ax = bx = NX + i + 1; ay = by = NY - 1; }
+        else { tx = NX; ty = NY + i + 1; ax = bx = NX - 1; ay = by = NY + i + 1; }
+        break;
+    }
+    return;
+  }
+  int j = k - 2 * (NG - 1);    // 0: first diagonal cell, 1: second
+  switch (corner) {
+    case 0: tx = -1 - j; ty = -1 - j; ax = bx = NX - 1 - j; ay = by = -1 - j; break;
+    case 1: tx = -1 - j; ty = NY + j; ax = bx = NX - 1 - j; ay = by = NY + j; break;
+    case 2: tx = NX + j; ty = -1 - j; ax = bx = 0 + j; ay = by = -1 - j; break;
+    default: tx = NX + j; ty = NY + j; ax = bx = 0 + j; ay = by = NY + j; break;
+  }
+}
+__global__ void k_bc_corners2d(Grid G) {
+  int op = blockIdx.x * blockDim.x + threadIdx.x;
+  if (op >= 8 * G.ng) return;
+  int tx, ty, ax, ay, bx, by;
+  corner2d_op(G, op, tx, ty, ax, ay, bx, by);
+  int k = op % (2 * G.ng);
+  bool avg = k >= 2 * (G.ng - 1);
+  long ca = cell_index(G, ax, ay, 0), cb = cell_index(G, bx, by, 0), c = cell_index(G, tx, ty, 0);
+  double pp[NVMAX], uu[NVMAX];
+  for (int iv = 0; iv < G.nv; iv++) {
+    double a = G.p[iv * G.ncell + ca];
+    pp[iv] = avg ? .5 * (a + G.p[iv * G.ncell + cb]) : a;
+  }
+  Geom g;
+  geom_centre(G, tx, ty, 0, g);
+  p2u_full(G, pp, uu, g);
+  store_cell(G.p, G.ncell, c, G.nv, pp);
+  store_cell(G.u, G.ncell, c, G.nv, uu);
+}
+
+// ---------------------------------------------------------------------------
+// wavespeeds and the CFL reduction (calc_wavespeeds finite.c:567-599,
+// save_wavespeeds 295-398)
+// ---------------------------------------------------------------------------
+__device__ inline void atomic_max_pos(double *addr, double v) {
+  if (!(v == v)) return;   // NaN never wins, as with the reference's '>' test
+  atomicMax((long long *)addr, __double_as_longlong(v));
+}
+
+__global__ void k_wavespeeds(Grid G, Box b) {
+  int ix, iy, iz;
+  double tsd = -1.;
+  if (box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) {
+    long c = cell_index(G, ix, iy, iz);
+    double pp[NVMAX];
+    load_cell(G.p, G.ncell, c, G.nv, pp);
+    Geom g;
+    geom_centre(G, ix, iy, iz, g);
+    double al[3], ar[3];
+    wavespeeds(G, pp, g, al, ar);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      G.al[d][c] = al[d];
+      G.ar[d][c] = ar[d];
+    }
+    if (in_domain(G, ix, iy, iz)) {
+      double wsx = dmax(fabs(al[0]), fabs(ar[0]));
+      double wsy = dmax(fabs(al[1]), fabs(ar[1]));
+      double wsz = dmax(fabs(al[2]), fabs(ar[2]));
+      double dx = size_x(G, ix, 0), dy = size_x(G, iy, 1), dz = size_x(G, iz, 2);
+      double tstepden;
+      if (G.nz > 1 && G.ny > 1) tstepden = wsx / dx + wsy / dy + wsz / dz;
+      else if (G.nz == 1 && G.ny > 1) tstepden = wsx / dx + wsy / dy;
+      else if (G.ny == 1 && G.nz > 1) tstepden = wsx / dx + wsz / dz;
+      else tstepden = wsx / dx;
+      tsd = tstepden / G.tsteplim;
+    }
+  }
+  // warp-level maximum, one atomic per warp
+  for (int o = 16; o > 0; o >>= 1) {
+    double other = __shfl_xor_sync(0xffffffffu, tsd, o);
+    tsd = other > tsd ? other : tsd;
+  }
+  if ((threadIdx.x & 31) == 0 && tsd > 0.) atomic_max_pos(&G.scal[S_TSTEPDENMAX], tsd);
+}
+
+// ---------------------------------------------------------------------------
+// fused face flux (finite.c:694-1014 and 1297-1624)
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(128) k_flux(Grid G, Box b) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const int nv = G.nv;
+  const int i = D == 0 ? ix : (D == 1 ? iy : iz);
+  const long stride = D == 0 ? 1 : (D == 1 ? (long)G.sx : (long)G.sx * G.sy);
+  const long cR = cell_index(G, ix, iy, iz);     // cell i (right of the face)
+  const long cL = cR - stride;                   // cell i-1
+  double dx[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) dx[k] = size_x(G, i - 3 + k, D);
+
+  // face states: left = right-face value of cell i-1, right = left-face
+  // value of cell i (avg2point of each cell, finite.c:89-289)
+  double pL[NVMAX], pR[NVMAX];
+  for (int iv = 0; iv < nv; iv++) {
+    const double *pv = G.p + iv * G.ncell + cR;
+    double v0 = pv[-3 * stride], v1 = pv[-2 * stride], v2 = pv[-stride], v3 = pv[0], v4 = pv[stride], v5 = pv[2 * stride];
+    if (G.int_order == 4) {
+      pL[iv] = mp5_face(v0, v1, v2, v3, v4);
+      pR[iv] = mp5_face(v5, v4, v3, v2, v1);
+    } else {
+      double ul, ur;
+      ppm(v0, v1, v2, v3, v4, dx[0], dx[1], dx[2], dx[3], dx[4], ul, ur);
+      pL[iv] = ur;
+      ppm(v1, v2, v3, v4, v5, dx[1], dx[2], dx[3], dx[4], dx[5], ul, ur);
+      pR[iv] = ul;
+    }
+  }
+
+  Geom g;
+  geom_face(G, ix, iy, iz, D, g);
+  const bool magn = nv > B3;
+  double fL[NVMAX], uL[NVMAX], fR[NVMAX], uR[NVMAX];
+  {
+    check_floors_mhd(G, pL, g);
+    Kin k;
+    kinematics(pL, g, magn, k);
+    flux_prime(G, pL, D, g, k, fL);
+    p2u_mhd(G, pL, uL, g, k);
+  }
+  {
+    check_floors_mhd(G, pR, g);
+    Kin k;
+    kinematics(pR, g, magn, k);
+    flux_prime(G, pR, D, g, k, fR);
+    p2u_mhd(G, pR, uR, g, k);
+  }
+  double ap1l = G.al[D][cR], ap1r = G.ar[D][cR], am1l = G.al[D][cL], am1r = G.ar[D][cL];
+  double ap1 = dmax(fabs(ap1l), fabs(ap1r)), am1 = dmax(fabs(am1l), fabs(am1r));
+  double ag = dmax(ap1, am1);
+  double al = dmin(ap1l, am1l);
+  double ar = dmax(ap1r, am1r);
+  const long f = face_index(G, ix, iy, iz, D);
+  double *out = G.flb[D] + f;
+  const long nf = G.nface[D];
+  for (int iv = 0; iv < nv; iv++) {
+    double fs;
+    if (G.fluxmethod == 0) {
+      fs = .5 * (fR[iv] + fL[iv] - ag * (uR[iv] - uL[iv]));
+    } else {
+      if (al > 0.) fs = fL[iv];
+      else if (ar < 0.) fs = fL[iv];   // the reference takes the left flux here too (finite.c:1410)
+      else fs = (-al * fR[iv] + ar * fL[iv] + al * ar * (uR[iv] - uL[iv])) / (ar - al);
+    }
+    out[iv * nf] = fs;
+  }
+}
+
+// zero fluxes outside the Riemann range (finite.c:1520, 1620): only needed
+// for directions of size one, whose face fluxes the update reads
+__global__ void k_zero_flux(Grid G, int d) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  long n = G.nface[d] * G.nv;
+  if (t < n) G.flb[d][t] = 0.;
+}
+
+// ---------------------------------------------------------------------------
+// flux-CT corner EMFs (magn.c:199-297)
+// ---------------------------------------------------------------------------
+struct Acc {
+  double s;
+  bool first;
+  __device__ Acc() : s(0.), first(true) {}
+  __device__ void add(double v, bool neg) {
+    if (first) { s = neg ? -v : v; first = false; }
+    else s = neg ? s - v : s + v;
+  }
+};
+
+__global__ void k_emf(Grid G, Box b) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const int NX = G.nx, NY = G.ny, NZ = G.nz;
+  const double *fx = G.flb[0], *fy = G.flb[1], *fz = G.flb[2];
+  const long nfx = G.nface[0], nfy = G.nface[1], nfz = G.nface[2];
+#define FXV(iv, a, b2, c) fx[(iv)*nfx + face_index(G, a, b2, c, 0)]
+#define FYV(iv, a, b2, c) fy[(iv)*nfy + face_index(G, a, b2, c, 1)]
+#define FZV(iv, a, b2, c) fz[(iv)*nfz + face_index(G, a, b2, c, 2)]
+  const long ne = (long)(NX + 1) * (NY + 1) * (NZ + 1);
+  const long e = emf_index(G, ix, iy, iz);
+  double c1 = ((NY > 1) && (NZ > 1)) ? 0.25 : 0.5;
+  double c2 = ((NX > 1) && (NZ > 1)) ? 0.25 : 0.5;
+  double c3 = ((NX > 1) && (NY > 1)) ? 0.25 : 0.5;
+  if ((NY > 1) || (NZ > 1)) {
+    Acc a;
+    if (NY > 1) { a.add(FYV(B3, ix, iy, iz), false); a.add(FYV(B3, ix, iy, iz - 1), false); }
+    if (NZ > 1) { a.add(FZV(B2, ix, iy, iz), true); a.add(FZV(B2, ix, iy - 1, iz), true); }
+    G.emf[0 * ne + e] = c1 * (a.s);
+  } else G.emf[0 * ne + e] = 0.;
+  if ((NX > 1) || (NZ > 1)) {
+    Acc a;
+    if (NZ > 1) { a.add(FZV(B1, ix, iy, iz), false); a.add(FZV(B1, ix - 1, iy, iz), false); }
+    if (NX > 1) { a.add(FXV(B3, ix, iy, iz), true); a.add(FXV(B3, ix, iy, iz - 1), true); }
+    G.emf[1 * ne + e] = c2 * (a.s);
+  } else G.emf[1 * ne + e] = 0.;
+  if ((NX > 1) || (NY > 1)) {
+    Acc a;
+    if (NX > 1) { a.add(FXV(B2, ix, iy, iz), false); a.add(FXV(B2, ix, iy - 1, iz), false); }
+    if (NY > 1) { a.add(FYV(B1, ix, iy, iz), true); a.add(FYV(B1, ix - 1, iy, iz), true); }
+    G.emf[2 * ne + e] = c3 * (a.s);
+  } else G.emf[2 * ne + e] = 0.;
+#undef FXV
+#undef FYV
+#undef FZV
+}
+
+// ---------------------------------------------------------------------------
+// unsplit update with metric source terms (finite.c:1062-1160,
+// f_metric_source_term_arb physics.c:324-465)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_update(Grid G, Box b, const double *dtp, double fac, double *save) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const int nv = G.nv;
+  const long c = cell_index(G, ix, iy, iz);
+  const double dt = fac * dtp[0];
+  double pp[NVMAX];
+  load_cell(G.p, G.ncell, c, nv, pp);
+  Geom g;
+  geom_centre(G, ix, iy, iz, g);
+  Kin k;
+  kinematics(pp, g, nv > B3, k);
+  // T^{mu nu} (calc_Tij) then T^mu_nu (indices_2221)
+  double T[4][4];
+  {
+    double rho = pp[0], uu = pp[1];
+    double pr = (G.gamma - 1.) * uu;
+    double w = rho + uu + pr;
+    double eta = w + k.bsq;
+    double ptot = pr + 0.5 * k.bsq;
+    double Tu[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int bb = 0; bb < 4; bb++) Tu[a][bb] = eta * k.ucon[a] * k.ucon[bb] + ptot * g.GG[a][bb] - k.bcon[a] * k.bcon[bb];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int bb = 0; bb < 4; bb++) {
+        double s = 0.;
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) s += Tu[a][kk] * g.gg[kk][bb];
+        T[a][bb] = s;
+      }
+  }
+  double ms[NVMAX];
+  for (int iv = 0; iv < nv; iv++) ms[iv] = 0.;
+  {
+    const long mi = met_index(G, ix, iy, iz);
+    const double gdetu = g.gdet;
+    double s1 = 0., s2 = 0., s3 = 0., s4 = 0.;
+    for (int kk = 0; kk < 4; kk++)
+      for (int l = 0; l < 4; l++) {
+        double gt = gdetu * T[kk][l];
+        const double *K = G.gkr + (long)(l * 16 + kk) * G.nmet + mi;
+        s1 += gt * __ldg(K + 0 * 4 * G.nmet);
+        s2 += gt * __ldg(K + 1 * 4 * G.nmet);
+        s3 += gt * __ldg(K + 2 * 4 * G.nmet);
+        s4 += gt * __ldg(K + 3 * 4 * G.nmet);
+      }
+    ms[1] = s1; ms[2] = s2; ms[3] = s3; ms[4] = s4;
+  }
+  const double dx = size_x(G, ix, 0), dy = size_x(G, iy, 1), dz = size_x(G, iz, 2);
+  const long fxl = face_index(G, ix, iy, iz, 0), fxr = face_index(G, ix + 1, iy, iz, 0);
+  const long fyl = face_index(G, ix, iy, iz, 1), fyr = face_index(G, ix, iy + 1, iz, 1);
+  const long fzl = face_index(G, ix, iy, iz, 2), fzr = face_index(G, ix, iy, iz + 1, 2);
+  const long ne = (long)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
+#define EMFV(comp, a, b2, c2) G.emf[((comp)-1) * ne + emf_index(G, a, b2, c2)]
+  for (int iv = 0; iv < nv; iv++) {
+    double flxl = G.flb[0][iv * G.nface[0] + fxl], flxr = G.flb[0][iv * G.nface[0] + fxr];
+    double flyl = G.flb[1][iv * G.nface[1] + fyl], flyr = G.flb[1][iv * G.nface[1] + fyr];
+    double flzl = G.flb[2][iv * G.nface[2] + fzl], flzr = G.flb[2][iv * G.nface[2] + fzr];
+    if (nv > B3 && iv >= B1) {
+      // fluxes rewritten by flux_ct (magn.c:300-337)
+      if (G.nx > 1) {
+        if (iv == B1) { flxl = 0.; flxr = 0.; }
+        if (iv == B2) {
+          flxl = 0.5 * (EMFV(3, ix, iy, iz) + EMFV(3, ix, iy + 1, iz));
+          flxr = 0.5 * (EMFV(3, ix + 1, iy, iz) + EMFV(3, ix + 1, iy + 1, iz));
+        }
+        if (iv == B3) {
+          flxl = -0.5 * (EMFV(2, ix, iy, iz) + EMFV(2, ix, iy, iz + 1));
+          flxr = -0.5 * (EMFV(2, ix + 1, iy, iz) + EMFV(2, ix + 1, iy, iz + 1));
+        }
+      }
+      if (G.ny > 1) {
+        if (iv == B1) {
+          flyl = -0.5 * (EMFV(3, ix, iy, iz) + EMFV(3, ix + 1, iy, iz));
+          flyr = -0.5 * (EMFV(3, ix, iy + 1, iz) + EMFV(3, ix + 1, iy + 1, iz));
+        }
+        if (iv == B2) { flyl = 0.; flyr = 0.; }
+        if (iv == B3) {
+          flyl = 0.5 * (EMFV(1, ix, iy, iz) + EMFV(1, ix, iy, iz + 1));
+          flyr = 0.5 * (EMFV(1, ix, iy + 1, iz) + EMFV(1, ix, iy + 1, iz + 1));
+        }
+      }
+      if (G.nz > 1) {
+        if (iv == B1) {
+          flzl = 0.5 * (EMFV(2, ix, iy, iz) + EMFV(2, ix + 1, iy, iz));
+          flzr = 0.5 * (EMFV(2, ix, iy, iz + 1) + EMFV(2, ix + 1, iy, iz + 1));
+        }
+        if (iv == B2) {
+          flzl = -0.5 * (EMFV(1, ix, iy, iz) + EMFV(1, ix, iy + 1, iz));
+          flzr = -0.5 * (EMFV(1, ix, iy, iz + 1) + EMFV(1, ix, iy + 1, iz + 1));
+        }
+        if (iv == B3) { flzl = 0.; flzr = 0.; }
+      }
+    }
+    double du = -(flxr - flxl) * dt / dx - (flyr - flyl) * dt / dy - (flzr - flzl) * dt / dz;
+    double uold = G.u[iv * G.ncell + c];
+    double val = uold + du + ms[iv] * dt;
+    if (save) save[iv * G.ncell + c] = uold;
+    G.u[iv * G.ncell + c] = val;
+  }
+#undef EMFV
+}
+
+// ---------------------------------------------------------------------------
+// conserved -> primitives over the domain (calc_u2p finite.c:501-561,
+// calc_primitives u2p.c:13-133) and neighbour-average fixups
+// (cell_fixup finite.c:4467-4631)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_u2p(Grid G, Box b) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+  double uu[NVMAX], pp[NVMAX];
+  load_cell(G.u, G.ncell, c, G.nv, uu);
+  load_cell(G.p, G.ncell, c, G.nv, pp);
+  Geom g;
+  geom_centre(G, ix, iy, iz, g);
+  int fix = 0;
+  int ret = u2p(G, uu, pp, g, fix);
+  if (uu[0] / g.gdet < 0.) atomicAdd(&G.cnt[C_NEGRHO], 1ull);
+  if (ret == -1) atomicAdd(&G.cnt[C_ENTROPY], 1ull);
+  if (ret == -3) atomicAdd(&G.cnt[C_FAIL], 1ull);
+  if (fix) atomicAdd(&G.cnt[C_FIXUP], 1ull);
+  check_floors_mhd(G, pp, g);
+  p2u_full(G, pp, uu, g);
+  store_cell(G.p, G.ncell, c, G.nv, pp);
+  store_cell(G.u, G.ncell, c, G.nv, uu);
+  G.flag[c] = fix;
+}
+
+// The reference visits cells in loop_0 order (x outer, z inner) and clears
+// each flag as it goes, so a neighbour that precedes the cell in that order
+// always counts as good, one that follows counts when its own inversion
+// succeeded.  Neighbour values are the post-inversion primitives.
+__global__ void k_fixup(Grid G, Box b, int *fixmark) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+  if (G.flag[c] == 0) return;
+  const int NX = G.nx, NY = G.ny, NZ = G.nz, nv = G.nv;
+  int nb[6][3] = {{ix - 1, iy, iz}, {ix + 1, iy, iz}, {ix, iy - 1, iz}, {ix, iy + 1, iz}, {ix, iy, iz - 1}, {ix, iy, iz + 1}};
+  bool inr[6] = {ix - 1 >= 0, ix + 1 < NX, iy - 1 >= 0, iy + 1 < NY, iz - 1 >= 0, iz + 1 < NZ};
+  bool before[6] = {true, false, true, false, true, false};
+  double acc[NVMAX];
+  for (int iv = 0; iv < nv; iv++) acc[iv] = 0.;
+  int in = 0;
+  long nbc[6];
+  for (int k = 0; k < 6; k++) {
+    if (!inr[k]) continue;
+    long n = cell_index(G, nb[k][0], nb[k][1], nb[k][2]);
+    if (before[k] || G.flag[n] == 0) nbc[in++] = n;
+  }
+  fixmark[c] = 0;
+  if (!((NZ == 1 && NY == 1 && in >= 1) || (NZ == 1 && in >= 2) || (NY == 1 && in >= 2) || in >= 3)) return;
+  double pp[NVMAX], uu[NVMAX];
+  for (int iv = 0; iv < nv; iv++) {
+    if (iv != RHO && iv < B1) {
+      double s = 0.;
+      for (int k = 0; k < in; k++) s += G.p[iv * G.ncell + nbc[k]];
+      pp[iv] = s / (double)in;
+    } else
+      pp[iv] = G.p[iv * G.ncell + c];
+  }
+  Geom g;
+  geom_centre(G, ix, iy, iz, g);
+  p2u_full(G, pp, uu, g);
+  store_cell(G.pfix, G.ncell, c, nv, pp);
+  store_cell(G.ufix, G.ncell, c, nv, uu);
+  fixmark[c] = 1;
+}
+
+// apply fixups; optionally finish an RK2 step: u = ut0 + (u - ut1)
+// (addi_u pair of ko.c:614-615)
+__global__ void k_commit(Grid G, Box b, const int *fixmark, int combine) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+  const int nv = G.nv;
+  if (G.flag[c] != 0) {
+    if (fixmark[c]) {
+      for (int iv = 0; iv < nv; iv++) {
+        G.p[iv * G.ncell + c] = G.pfix[iv * G.ncell + c];
+        G.u[iv * G.ncell + c] = G.ufix[iv * G.ncell + c];
+      }
+    }
+    G.flag[c] = 0;
+  }
+  if (combine) {
+    for (int iv = 0; iv < nv; iv++) {
+      long i = iv * G.ncell + c;
+      double ut2 = 1. * G.u[i] + (-1.) * G.ut1[i];
+      G.u[i] = 1. * G.ut0[i] + 1. * ut2;
+    }
+  }
+}
+
+__global__ void k_begin_step(Grid G) {
+  G.scal[S_DT] = 1. / G.scal[S_TSTEPDENMAX];
+  G.scal[S_TSTEPDENMAX] = -1.;
+}
+
+__global__ void k_copy_domain(Grid G, Box b, double f, const double *src, double *dst) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  long c = cell_index(G, ix, iy, iz);
+  for (int iv = 0; iv < G.nv; iv++) dst[iv * G.ncell + c] = f * src[iv * G.ncell + c];
+}
+__global__ void k_add_domain(Grid G, Box b, double f1, const double *a, double f2, const double *bb, double *c3) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  long c = cell_index(G, ix, iy, iz);
+  for (int iv = 0; iv < G.nv; iv++) c3[iv * G.ncell + c] = f1 * a[iv * G.ncell + c] + f2 * bb[iv * G.ncell + c];
+}
+
+// KORAL layout [cell][var] <-> device [var][cell]
+__global__ void k_aos_to_soa(const double *aos, double *soa, long n, int nv) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= n * nv) return;
+  long c = t / nv;
+  int iv = (int)(t % nv);
+  soa[iv * n + c] = aos[t];
+}
+__global__ void k_soa_to_aos(const double *soa, double *aos, long n, int nv) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= n * nv) return;
+  long c = t / nv;
+  int iv = (int)(t % nv);
+  aos[t] = soa[iv * n + c];
+}
+__global__ void k_minkowski(double *met, long npts) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= npts) return;
+  for (int k = 0; k < 40; k++) met[k * npts + t] = 0.;
+  met[0 * npts + t] = -1.;
+  met[6 * npts + t] = 1.;
+  met[12 * npts + t] = 1.;
+  met[18 * npts + t] = 1.;
+  met[19 * npts + t] = 1.;         // gdet
+  met[20 * npts + t] = -1.;
+  met[26 * npts + t] = 1.;
+  met[32 * npts + t] = 1.;
+  met[38 * npts + t] = 1.;
+}
+__global__ void k_fill(double *a, long n, double v) {
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t < n) a[t] = v;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+enum KernelId { K_BC = 0, K_WAVESPEEDS, K_FLUX0, K_FLUX1, K_FLUX2, K_EMF, K_UPDATE, K_U2P, K_FIXUP, K_COMMIT,
+                K_BEGIN, K_NKERNELS };
+static const char *kKernelNames[K_NKERNELS] = {"k_bc", "k_wavespeeds", "k_flux_x", "k_flux_y", "k_flux_z", "k_emf",
+                                               "k_update", "k_u2p", "k_fixup", "k_commit", "k_begin_step"};
+
+struct ProfRec {
+  int id;
+  cudaEvent_t a, b;
+};
+
+struct kgpu_ctx {
+  kgpu_config cfg;
+  bool profiling = false;
+  std::vector<ProfRec> prof;        // events of the launches since the last read
+  std::vector<cudaEvent_t> evpool;  // recycled events
+  double prof_ms[K_NKERNELS] = {0};
+  long long prof_n[K_NKERNELS] = {0};
+  long long launches = 0;           // kernels launched by this context
+  long long graph_launches = 0;     // kernels in one captured RK2 step
+  Grid G;
+  cudaStream_t stream;
+  std::vector<void *> allocs;
+  double *stage;        // AoS staging for uploads / downloads
+  int *fixmark;
+  double min_dx, min_dy, min_dz;
+  bool have_grid, have_metric;
+  std::vector<double> hxb[3];
+  cudaGraph_t graph;
+  cudaGraphExec_t graph_exec;
+  bool graph_ready;
+};
+
+static cudaEvent_t pool_event(kgpu_ctx *c) {
+  if (!c->evpool.empty()) {
+    cudaEvent_t e = c->evpool.back();
+    c->evpool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+// brackets one launch with events when profiling; counts every launch
+struct LaunchScope {
+  kgpu_ctx *c;
+  ProfRec r;
+  LaunchScope(kgpu_ctx *ctx, int id) : c(ctx) {
+    c->launches++;
+    if (c->profiling) {
+      r.id = id;
+      r.a = pool_event(c);
+      r.b = pool_event(c);
+      cudaEventRecord(r.a, c->stream);
+    }
+  }
+  ~LaunchScope() {
+    if (c->profiling) {
+      cudaEventRecord(r.b, c->stream);
+      c->prof.push_back(r);
+    }
+  }
+};
+
+static int dalloc(kgpu_ctx *c, void **p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes ? bytes : 8);
+  if (e != cudaSuccess) {
+    set_err("cudaMalloc", e);
+    return KGPU_ENOMEM;
+  }
+  c->allocs.push_back(*p);
+  return 0;
+}
+
+extern "C" int kgpu_default_config(kgpu_config *cfg, int nx, int ny, int nz) {
+  if (!cfg || nx < 1 || ny < 1 || nz < 1) return KGPU_EINVAL;
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->nx = nx; cfg->ny = ny; cfg->nz = nz;
+  cfg->ng = 3; cfg->nv = 9;
+  cfg->int_order = KGPU_PPM;
+  cfg->fluxmethod = KGPU_LAXF;
+  cfg->axisym_metric = 0;
+  cfg->periodic[0] = cfg->periodic[1] = cfg->periodic[2] = 1;
+  cfg->gamma = 5. / 3.;
+  cfg->tsteplim = 0.5;
+  cfg->rhofloor = 1.e-50;          // choices.h:319-329
+  cfg->uurhoratiomin = 1.e-50;     // choices.h:55-58
+  cfg->uurhoratiomax = 1.e2;       // choices.h:65-68
+  cfg->b2rhoratiomax = 100.;       // choices.h:110-113
+  cfg->gammamaxhd = 100.;          // choices.h:331-333
+  cfg->u2pconv = 1.e-10;           // choices.h:457-459
+  return 0;
+}
+
+static void fill_grid_params(Grid &G, const kgpu_config &c) {
+  memset(&G, 0, sizeof(G));
+  G.nx = c.nx; G.ny = c.ny; G.nz = c.nz; G.ng = c.ng; G.nv = c.nv;
+  G.sx = c.nx + 2 * c.ng; G.ngcx = c.ng;
+  G.sy = c.ny > 1 ? c.ny + 2 * c.ng : 1; G.ngcy = c.ny > 1 ? c.ng : 0;
+  G.sz = c.nz > 1 ? c.nz + 2 * c.ng : 1; G.ngcz = c.nz > 1 ? c.ng : 0;
+  G.axisym = c.axisym_metric;
+  G.szmet = G.axisym ? 1 : G.sz;
+  G.ngczmet = G.axisym ? 0 : G.ngcz;
+  G.ncell = (long)G.sx * G.sy * G.sz;
+  G.nmet = (long)G.sx * G.sy * G.szmet;
+  G.nfmet[0] = (long)(G.sx + 1) * G.sy * G.szmet;
+  G.nfmet[1] = (long)G.sx * (G.sy + 1) * G.szmet;
+  G.nfmet[2] = (long)G.sx * G.sy * (G.szmet + 1);
+  G.nface[0] = (long)(G.sx + 1) * G.sy * G.sz;
+  G.nface[1] = (long)G.sx * (G.sy + 1) * G.sz;
+  G.nface[2] = (long)G.sx * G.sy * (G.sz + 1);
+  G.gamma = c.gamma; G.tsteplim = c.tsteplim;
+  G.int_order = c.int_order; G.fluxmethod = c.fluxmethod;
+  G.rhofloor = c.rhofloor; G.uurhoratiomin = c.uurhoratiomin; G.uurhoratiomax = c.uurhoratiomax;
+  G.b2rhoratiomax = c.b2rhoratiomax; G.gammamaxhd = c.gammamaxhd; G.u2pconv = c.u2pconv;
+}
+
+static int check_config(const kgpu_config *c) {
+  if (!c || c->nx < 1 || c->ny < 1 || c->nz < 1) return KGPU_EINVAL;
+  if (c->nv != 9) return KGPU_EINVAL;               // MHD with magnetic field
+  if (c->int_order != KGPU_PPM && c->int_order != KGPU_MP5) return KGPU_EINVAL;
+  if (c->int_order == KGPU_PPM && c->ng < 3) return KGPU_EINVAL;
+  if (c->int_order == KGPU_MP5 && c->ng < 4) return KGPU_EINVAL;
+  if (c->fluxmethod != KGPU_LAXF && c->fluxmethod != KGPU_HLL) return KGPU_EINVAL;
+  if (c->nx < c->ng) return KGPU_EINVAL;
+  if (!(c->gamma > 1.) || !(c->tsteplim > 0.)) return KGPU_EINVAL;
+  return 0;
+}
+
+extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
+  if (!out) return KGPU_EINVAL;
+  *out = nullptr;
+  int r = check_config(cfg);
+  if (r) return r;
+  if (!(cfg->periodic[0] && cfg->periodic[1] && cfg->periodic[2])) return KGPU_EINVAL;
+  kgpu_ctx *c = new kgpu_ctx();
+  c->cfg = *cfg;
+  fill_grid_params(c->G, *cfg);
+  Grid &G = c->G;
+  c->have_grid = c->have_metric = false;
+  c->graph_ready = false;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return set_err("cudaStreamCreate", e);
+  }
+  const size_t d8 = sizeof(double);
+  const long ncv = G.ncell * G.nv;
+  void *p;
+#define AL(ptr, bytes)                           \
+  do {                                           \
+    if ((r = dalloc(c, &p, (bytes))) != 0) {     \
+      kgpu_destroy(c);                           \
+      return r;                                  \
+    }                                            \
+    ptr = (decltype(ptr))p;                      \
+  } while (0)
+  AL(G.u, ncv * d8); AL(G.p, ncv * d8); AL(G.ut0, ncv * d8); AL(G.ut1, ncv * d8);
+  AL(G.pfix, ncv * d8); AL(G.ufix, ncv * d8); AL(c->stage, ncv * d8);
+  int n[3] = {G.nx, G.ny, G.nz};
+  for (int d = 0; d < 3; d++) {
+    double *xb;
+    AL(xb, (n[d] + 1 + 2 * G.ng) * d8);
+    G.xb[d] = xb;
+    AL(G.flb[d], G.nface[d] * G.nv * d8);
+    AL(G.al[d], G.ncell * d8);
+    AL(G.ar[d], G.ncell * d8);
+    double *mf;
+    AL(mf, G.nfmet[d] * 40 * d8);
+    G.met_f[d] = mf;
+  }
+  double *mc, *kr;
+  AL(mc, G.nmet * 40 * d8); G.met_c = mc;
+  AL(kr, G.nmet * 64 * d8); G.gkr = kr;
+  AL(G.emf, 3L * (G.nx + 1) * (G.ny + 1) * (G.nz + 1) * d8);
+  AL(G.flag, G.ncell * sizeof(int));
+  AL(c->fixmark, G.ncell * sizeof(int));
+  AL(G.scal, S_NSCAL * d8);
+  AL(G.cnt, C_NCNT * sizeof(unsigned long long));
+#undef AL
+  CK(cudaMemsetAsync(G.u, 0, ncv * d8, c->stream));
+  CK(cudaMemsetAsync(G.p, 0, ncv * d8, c->stream));
+  CK(cudaMemsetAsync(G.ut0, 0, ncv * d8, c->stream));
+  CK(cudaMemsetAsync(G.ut1, 0, ncv * d8, c->stream));
+  for (int d = 0; d < 3; d++) {
+    CK(cudaMemsetAsync(G.flb[d], 0, G.nface[d] * G.nv * d8, c->stream));
+    CK(cudaMemsetAsync(G.al[d], 0, G.ncell * d8, c->stream));
+    CK(cudaMemsetAsync(G.ar[d], 0, G.ncell * d8, c->stream));
+  }
+  CK(cudaMemsetAsync(G.emf, 0, 3L * (G.nx + 1) * (G.ny + 1) * (G.nz + 1) * d8, c->stream));
+  CK(cudaMemsetAsync(G.flag, 0, G.ncell * sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->fixmark, 0, G.ncell * sizeof(int), c->stream));
+  CK(cudaMemsetAsync(G.scal, 0, S_NSCAL * d8, c->stream));
+  CK(cudaMemsetAsync(G.cnt, 0, C_NCNT * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync((void *)G.gkr, 0, G.nmet * 64 * d8, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *out = c;
+  return 0;
+}
+
+extern "C" int kgpu_destroy(kgpu_ctx *c) {
+  if (!c) return KGPU_EINVAL;
+  if (c->graph_ready) {
+    cudaGraphExecDestroy(c->graph_exec);
+    cudaGraphDestroy(c->graph);
+  }
+  cudaStreamSynchronize(c->stream);
+  for (auto &r : c->prof) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : c->evpool) cudaEventDestroy(e);
+  for (void *p : c->allocs) cudaFree(p);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+// minimal cell sizes as set_grid computes them, including its comparison of
+// dy and dz against the running minimum in x (finite.c:1672-1686)
+static void min_sizes(kgpu_ctx *c) {
+  const kgpu_config &k = c->cfg;
+  double mdx = -1, mdy = -1, mdz = -1;
+  auto sz = [&](int ic, int d) { return c->hxb[d][ic + 1 + k.ng] - c->hxb[d][ic + k.ng]; };
+  for (int ix = 0; ix < k.nx; ix++)
+    for (int iy = 0; iy < k.ny; iy++)
+      for (int iz = 0; iz < k.nz; iz++) {
+        double dx = sz(ix, 0), dy = sz(iy, 1), dz = sz(iz, 2);
+        if ((dx < mdx || mdx < 0.)) mdx = dx;
+        if ((dy < mdx || mdy < 0.)) mdy = dy;
+        if ((dz < mdx || mdz < 0.)) mdz = dz;
+      }
+  c->min_dx = mdx; c->min_dy = mdy; c->min_dz = mdz;
+}
+
+extern "C" int kgpu_upload_grid(kgpu_ctx *c, const double *xbx, const double *xby, const double *xbz) {
+  if (!c || !xbx || !xby || !xbz) return KGPU_EINVAL;
+  const double *src[3] = {xbx, xby, xbz};
+  int n[3] = {c->cfg.nx, c->cfg.ny, c->cfg.nz};
+  for (int d = 0; d < 3; d++) {
+    c->hxb[d].assign(src[d], src[d] + n[d] + 1 + 2 * c->cfg.ng);
+    CK(cudaMemcpyAsync((void *)c->G.xb[d], src[d], (n[d] + 1 + 2 * c->cfg.ng) * sizeof(double), cudaMemcpyHostToDevice,
+                       c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  min_sizes(c);
+  c->have_grid = true;
+  return 0;
+}
+
+extern "C" int kgpu_set_uniform_grid(kgpu_ctx *c, const double lo[3], const double hi[3]) {
+  if (!c || !lo || !hi) return KGPU_EINVAL;
+  int n[3] = {c->cfg.nx, c->cfg.ny, c->cfg.nz}, ng = c->cfg.ng;
+  std::vector<double> xb[3];
+  for (int d = 0; d < 3; d++) {
+    double c0 = lo[d], c1 = hi[d], dc = (c1 - c0) / (double)n[d];   // problem.c:9-36
+    xb[d].resize(n[d] + 1 + 2 * ng);
+    for (int i = -ng; i <= n[d] + ng; i++) xb[d][i + ng] = c0 + (double)(i)*dc;
+  }
+  return kgpu_upload_grid(c, xb[0].data(), xb[1].data(), xb[2].data());
+}
+
+// KORAL metric tables ([point][20]) -> [component][point]
+static int upload_met(kgpu_ctx *c, const double *g, const double *Gi, double *dst, long npts) {
+  std::vector<double> h(npts * 40);
+  for (long i = 0; i < npts; i++)
+    for (int k = 0; k < 20; k++) {
+      h[k * npts + i] = g[i * 20 + k];
+      h[(20 + k) * npts + i] = Gi[i * 20 + k];
+    }
+  CK(cudaMemcpyAsync(dst, h.data(), npts * 40 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_upload_metric(kgpu_ctx *c, const double *g, const double *Gi, const double *gKr, const double *gbx,
+                                  const double *gby, const double *gbz, const double *Gbx, const double *Gby,
+                                  const double *Gbz) {
+  if (!c || !g || !Gi || !gKr || !gbx || !gby || !gbz || !Gbx || !Gby || !Gbz) return KGPU_EINVAL;
+  Grid &G = c->G;
+  int r;
+  if ((r = upload_met(c, g, Gi, (double *)G.met_c, G.nmet))) return r;
+  const double *gb[3] = {gbx, gby, gbz}, *Gb[3] = {Gbx, Gby, Gbz};
+  for (int d = 0; d < 3; d++)
+    if ((r = upload_met(c, gb[d], Gb[d], (double *)G.met_f[d], G.nfmet[d]))) return r;
+  std::vector<double> h(G.nmet * 64);
+  for (long i = 0; i < G.nmet; i++)
+    for (int k = 0; k < 64; k++) h[k * G.nmet + i] = gKr[i * 64 + k];
+  CK(cudaMemcpyAsync((void *)G.gkr, h.data(), G.nmet * 64 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_metric = true;
+  return 0;
+}
+
+extern "C" int kgpu_set_minkowski_metric(kgpu_ctx *c) {
+  if (!c) return KGPU_EINVAL;
+  Grid &G = c->G;
+  k_minkowski<<<nblocks(G.nmet, 256), 256, 0, c->stream>>>((double *)G.met_c, G.nmet);
+  for (int d = 0; d < 3; d++)
+    k_minkowski<<<nblocks(G.nfmet[d], 256), 256, 0, c->stream>>>((double *)G.met_f[d], G.nfmet[d]);
+  k_fill<<<nblocks(G.nmet * 64, 256), 256, 0, c->stream>>>((double *)G.gkr, G.nmet * 64, 0.);
+  CKL("k_minkowski");
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_metric = true;
+  return 0;
+}
+
+extern "C" int kgpu_upload_state(kgpu_ctx *c, const double *u, const double *p) {
+  if (!c || !u || !p) return KGPU_EINVAL;
+  Grid &G = c->G;
+  const long n = G.ncell;
+  const double *src[2] = {u, p};
+  double *dst[2] = {G.u, G.p};
+  for (int k = 0; k < 2; k++) {
+    CK(cudaMemcpyAsync(c->stage, src[k], n * G.nv * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    k_aos_to_soa<<<nblocks(n * G.nv, 256), 256, 0, c->stream>>>(c->stage, dst[k], n, G.nv);
+    CKL("k_aos_to_soa");
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+static double *arr_ptr(kgpu_ctx *c, int which) {
+  switch (which) {
+    case KGPU_ARR_U: return c->G.u;
+    case KGPU_ARR_P: return c->G.p;
+    case KGPU_ARR_UT0: return c->G.ut0;
+    case KGPU_ARR_UT1: return c->G.ut1;
+    default: return nullptr;
+  }
+}
+
+extern "C" int kgpu_download_array(kgpu_ctx *c, int which, double *out) {
+  if (!c || !out) return KGPU_EINVAL;
+  double *src = arr_ptr(c, which);
+  if (!src) return KGPU_EINVAL;
+  Grid &G = c->G;
+  const long n = G.ncell;
+  k_soa_to_aos<<<nblocks(n * G.nv, 256), 256, 0, c->stream>>>(src, c->stage, n, G.nv);
+  CKL("k_soa_to_aos");
+  CK(cudaMemcpyAsync(out, c->stage, n * G.nv * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_download_state(kgpu_ctx *c, double *u, double *p) {
+  int r = kgpu_download_array(c, KGPU_ARR_U, u);
+  if (r) return r;
+  return kgpu_download_array(c, KGPU_ARR_P, p);
+}
+
+// ---------------------------------------------------------------------------
+// operator launchers (all asynchronous on the context stream)
+// ---------------------------------------------------------------------------
+static Box domain_box(const Grid &G) { return Box{0, 0, 0, G.nx, G.ny, G.nz}; }
+
+static int launch_bc(kgpu_ctx *c) {
+  Grid &G = c->G;
+  Box b{-G.ngcx, -G.ngcy, -G.ngcz, G.sx, G.sy, G.sz};
+  { LaunchScope ls(c, K_BC); k_bc_faces<<<nblocks(b.n(), 128), 128, 0, c->stream>>>(G, b); }
+  CKL("k_bc_faces");
+  if (G.nz == 1 && G.ny > 1) {
+    LaunchScope ls(c, K_BC);
+    k_bc_corners2d<<<1, 8 * G.ng > 32 ? 64 : 32, 0, c->stream>>>(G);
+    CKL("k_bc_corners2d");
+  }
+  return 0;
+}
+
+static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *save) {
+  Grid &G = c->G;
+  const int lim = G.int_order == 4 ? 2 : 1;
+  int lx = G.nx > 1 ? lim : 0, ly = G.ny > 1 ? lim : 0, lz = G.nz > 1 ? lim : 0;
+  Box wb{-lx, -ly, -lz, G.nx + 2 * lx, G.ny + 2 * ly, G.nz + 2 * lz};
+  { LaunchScope ls(c, K_WAVESPEEDS); k_wavespeeds<<<nblocks(wb.n(), 128), 128, 0, c->stream>>>(G, wb); }
+  CKL("k_wavespeeds");
+  int ey0 = G.ny > 1 ? -1 : 0, eny = G.ny > 1 ? G.ny + 2 : 1;
+  int ez0 = G.nz > 1 ? -1 : 0, enz = G.nz > 1 ? G.nz + 2 : 1;
+  int ex0 = -1, enx = G.nx + 2;
+  if (G.nx > 1) {
+    Box b{0, ey0, ez0, G.nx + 1, eny, enz};
+    LaunchScope ls(c, K_FLUX0);
+    k_flux<0><<<nblocks(b.n(), 128), 128, 0, c->stream>>>(G, b);
+    CKL("k_flux<0>");
+  }
+  if (G.ny > 1) {
+    Box b{ex0, 0, ez0, enx, G.ny + 1, enz};
+    LaunchScope ls(c, K_FLUX1);
+    k_flux<1><<<nblocks(b.n(), 128), 128, 0, c->stream>>>(G, b);
+    CKL("k_flux<1>");
+  }
+  if (G.nz > 1) {
+    Box b{ex0, ey0, 0, enx, eny, G.nz + 1};
+    LaunchScope ls(c, K_FLUX2);
+    k_flux<2><<<nblocks(b.n(), 128), 128, 0, c->stream>>>(G, b);
+    CKL("k_flux<2>");
+  }
+  Box eb{0, 0, 0, G.nx + 1, G.ny + 1, G.nz + 1};
+  { LaunchScope ls(c, K_EMF); k_emf<<<nblocks(eb.n(), 128), 128, 0, c->stream>>>(G, eb); }
+  CKL("k_emf");
+  Box db = domain_box(G);
+  { LaunchScope ls(c, K_UPDATE); k_update<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, dtp, fac, save); }
+  CKL("k_update");
+  return 0;
+}
+
+static int launch_u2p(kgpu_ctx *c, int combine) {
+  Grid &G = c->G;
+  Box db = domain_box(G);
+  { LaunchScope ls(c, K_U2P); k_u2p<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db); }
+  CKL("k_u2p");
+  { LaunchScope ls(c, K_FIXUP); k_fixup<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, c->fixmark); }
+  CKL("k_fixup");
+  { LaunchScope ls(c, K_COMMIT); k_commit<<<nblocks(db.n(), 256), 256, 0, c->stream>>>(G, db, c->fixmark, combine); }
+  CKL("k_commit");
+  return launch_bc(c);
+}
+
+static int ready(kgpu_ctx *c) {
+  if (!c) return KGPU_EINVAL;
+  if (!c->have_grid || !c->have_metric) return KGPU_ESTATE;
+  return 0;
+}
+
+extern "C" int kgpu_set_bc(kgpu_ctx *c, double t, int ifinit) {
+  (void)t; (void)ifinit;
+  int r = ready(c);
+  if (r) return r;
+  return launch_bc(c);
+}
+
+extern "C" int kgpu_op_explicit(kgpu_ctx *c, double t, double dt) {
+  (void)t;
+  int r = ready(c);
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->G.scal + S_T, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if ((r = launch_bc(c))) return r;
+  if ((r = launch_explicit(c, c->G.scal + S_T, 1., nullptr))) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_op_implicit(kgpu_ctx *c, double t, double dt) {
+  (void)t; (void)dt;
+  return c ? 0 : KGPU_EINVAL;
+}
+
+extern "C" int kgpu_calc_u2p(kgpu_ctx *c) {
+  int r = ready(c);
+  if (r) return r;
+  if ((r = launch_u2p(c, 0))) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_save_timesteps(kgpu_ctx *c) { return c ? 0 : KGPU_EINVAL; }
+
+extern "C" int kgpu_copyi_u(kgpu_ctx *c, double factor, int src, int dst) {
+  if (!c) return KGPU_EINVAL;
+  double *a = arr_ptr(c, src), *b = arr_ptr(c, dst);
+  if (!a || !b) return KGPU_EINVAL;
+  Box db = domain_box(c->G);
+  k_copy_domain<<<nblocks(db.n(), 256), 256, 0, c->stream>>>(c->G, db, factor, a, b);
+  CKL("k_copy_domain");
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_addi_u(kgpu_ctx *c, double f1, int a, double f2, int b, int cc) {
+  if (!c) return KGPU_EINVAL;
+  double *pa = arr_ptr(c, a), *pb = arr_ptr(c, b), *pc = arr_ptr(c, cc);
+  if (!pa || !pb || !pc) return KGPU_EINVAL;
+  Box db = domain_box(c->G);
+  k_add_domain<<<nblocks(db.n(), 256), 256, 0, c->stream>>>(c->G, db, f1, pa, f2, pb, pc);
+  CKL("k_add_domain");
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_begin_run(kgpu_ctx *c) {
+  int r = ready(c);
+  if (r) return r;
+  double mws = 10000., tsd;
+  const kgpu_config &k = c->cfg;
+  if (k.nz > 1) tsd = mws / c->min_dx + mws / c->min_dy + mws / c->min_dz;
+  else if (k.ny > 1) tsd = mws / c->min_dx + mws / c->min_dy;
+  else tsd = mws / c->min_dx;
+  tsd /= k.tsteplim;
+  return kgpu_set_tstepdenmax(c, tsd);
+}
+
+extern "C" int kgpu_set_tstepdenmax(kgpu_ctx *c, double v) {
+  if (!c) return KGPU_EINVAL;
+  CK(cudaMemcpyAsync(c->G.scal + S_TSTEPDENMAX, &v, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_get_tstepdenmax(kgpu_ctx *c, double *out) {
+  if (!c || !out) return KGPU_EINVAL;
+  CK(cudaMemcpyAsync(out, c->G.scal + S_TSTEPDENMAX, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_begin_step(kgpu_ctx *c, double *dt_out) {
+  if (!c) return KGPU_EINVAL;
+  k_begin_step<<<1, 1, 0, c->stream>>>(c->G);
+  CKL("k_begin_step");
+  if (dt_out) CK(cudaMemcpyAsync(dt_out, c->G.scal + S_DT, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+// one RK2 step (ko.c:571-626) with dt in device memory
+static int enqueue_rk2(kgpu_ctx *c) {
+  Grid &G = c->G;
+  int r;
+  { LaunchScope ls(c, K_BEGIN); k_begin_step<<<1, 1, 0, c->stream>>>(G); }
+  CKL("k_begin_step");
+  if ((r = launch_explicit(c, G.scal + S_DT, 0.5, G.ut0))) return r;   // ut0 = U^n
+  if ((r = launch_u2p(c, 0))) return r;
+  if ((r = launch_explicit(c, G.scal + S_DT, 1.0, G.ut1))) return r;   // ut1 = U^{n+1/2}
+  if ((r = launch_u2p(c, 1))) return r;                                // u = ut0 + (u - ut1)
+  return 0;
+}
+
+extern "C" int kgpu_rk2_steps(kgpu_ctx *c, int nsteps) {
+  int r = ready(c);
+  if (r) return r;
+  if (nsteps < 1) return KGPU_EINVAL;
+  for (int s = 0; s < nsteps; s++)
+    if ((r = enqueue_rk2(c))) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_rk2_steps_graph(kgpu_ctx *c, int nsteps) {
+  int r = ready(c);
+  if (r) return r;
+  if (nsteps < 1) return KGPU_EINVAL;
+  if (!c->graph_ready) {
+    bool prof = c->profiling;
+    c->profiling = false;
+    long long before = c->launches;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    r = enqueue_rk2(c);
+    c->graph_launches = c->launches - before;
+    c->launches = before;
+    c->profiling = prof;
+    cudaGraph_t gph;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &gph);
+    if (r) return r;
+    if (e != cudaSuccess) return set_err("cudaStreamEndCapture", e);
+    CK(cudaGraphInstantiate(&c->graph_exec, gph, 0));
+    c->graph = gph;
+    c->graph_ready = true;
+  }
+  for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(c->graph_exec, c->stream));
+  c->launches += c->graph_launches * nsteps;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_get_counters(kgpu_ctx *c, unsigned long long out[4]) {
+  if (!c || !out) return KGPU_EINVAL;
+  unsigned long long h[C_NCNT];
+  CK(cudaMemcpyAsync(h, c->G.cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < 4; i++) out[i] = h[i];
+  return 0;
+}
+
+extern "C" int kgpu_reset_counters(kgpu_ctx *c) {
+  if (!c) return KGPU_EINVAL;
+  CK(cudaMemsetAsync(c->G.cnt, 0, C_NCNT * sizeof(unsigned long long), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// problem set-up on the host (same arithmetic as the reference plug-in, run
+// with the host C library) then uploaded
+// ---------------------------------------------------------------------------
+extern "C" int kgpu_init_orszag_tang(kgpu_ctx *c) {
+  int r = ready(c);
+  if (r) return r;
+  const kgpu_config &k = c->cfg;
+  Grid &G = c->G;
+  const long n = G.ncell;
+  std::vector<double> u(n * G.nv, 0.), p(n * G.nv, 0.);
+  Geom g;
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 5; b++) g.gg[a][b] = g.GG[a][b] = 0.;
+  g.gg[0][0] = -1.; g.gg[1][1] = g.gg[2][2] = g.gg[3][3] = 1.; g.gg[3][4] = 1.;
+  g.GG[0][0] = -1.; g.GG[1][1] = g.GG[2][2] = g.GG[3][3] = 1.; g.GG[3][4] = 0.;
+  g.gdet = 1.; g.gttpert = 0.;
+  for (int ix = 0; ix < k.nx; ix++)
+    for (int iy = 0; iy < k.ny; iy++)
+      for (int iz = 0; iz < k.nz; iz++) {
+        // cell centres, finite.c:1647: x = (xb[i+1] + xb[i]) / 2
+        double xx = .5 * (c->hxb[0][ix + 1 + k.ng] + c->hxb[0][ix + k.ng]);
+        double yy = .5 * (c->hxb[1][iy + 1 + k.ng] + c->hxb[1][iy + k.ng]);
+        // VEL3 -> VELR (relele.c:208-232) for the coordinate three-velocity
+        double v3[4] = {0., -0.5 * sin(yy), 0.5 * sin(xx), 0.};
+        double a = 0., b = 0., uc[4];
+        for (int i = 1; i < 4; i++) {
+          a += 2. * v3[i] * g.gg[0][i];
+          for (int j = 1; j < 4; j++) b += v3[i] * v3[j] * g.gg[i][j];
+        }
+        uc[0] = sqrt(-1. / (g.gg[0][0] + a + b));
+        for (int i = 1; i < 4; i++) uc[i] = v3[i] * uc[0];
+        for (int i = 1; i < 4; i++) uc[i] = uc[i] - uc[0] * g.GG[0][i] / g.GG[0][0];
+        double pp[NVMAX], uu[NVMAX];
+        pp[RHO] = 25. / (36. * M_PI);
+        pp[UU] = (5. / (12. * M_PI)) / (k.gamma - 1.);
+        pp[VX] = uc[1]; pp[VY] = uc[2]; pp[VZ] = uc[3];
+        pp[B1] = -sin(yy) / sqrt(4. * M_PI);
+        pp[B2] = sin(2. * xx) / sqrt(4. * M_PI);
+        pp[B3] = 0.;
+        pp[ENTR] = calc_Sfromu(k.gamma, pp[RHO], pp[UU]);
+        p2u_full(G, pp, uu, g);
+        long cidx = cell_index(G, ix, iy, iz);
+        for (int iv = 0; iv < G.nv; iv++) {
+          u[cidx * G.nv + iv] = uu[iv];
+          p[cidx * G.nv + iv] = pp[iv];
+        }
+      }
+  if ((r = kgpu_upload_state(c, u.data(), p.data()))) return r;
+  if ((r = launch_bc(c))) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// batched per-cell solvers
+// ---------------------------------------------------------------------------
+__global__ void k_u2p_cells(Grid G, int n, const double *uu, double *pp, const double *met, int *status, int *fixup) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Geom g;
+  load_geom(met, n, i, g);
+  double u[NVMAX], p[NVMAX];
+  for (int iv = 0; iv < G.nv; iv++) {
+    u[iv] = uu[(long)iv * n + i];
+    p[iv] = pp[(long)iv * n + i];
+  }
+  int fix = 0;
+  int ret = u2p(G, u, p, g, fix);
+  for (int iv = 0; iv < G.nv; iv++) pp[(long)iv * n + i] = p[iv];
+  status[i] = ret;
+  fixup[i] = fix;
+}
+__global__ void k_p2u_cells(Grid G, int n, const double *pp, double *uu, const double *met) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Geom g;
+  load_geom(met, n, i, g);
+  double u[NVMAX], p[NVMAX];
+  for (int iv = 0; iv < G.nv; iv++) p[iv] = pp[(long)iv * n + i];
+  p2u_full(G, p, u, g);
+  for (int iv = 0; iv < G.nv; iv++) uu[(long)iv * n + i] = u[iv];
+}
+
+static void to_soa(const double *aos, std::vector<double> &soa, int n, int m) {
+  soa.resize((size_t)n * m);
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < m; k++) soa[(size_t)k * n + i] = aos[(size_t)i * m + k];
+}
+
+struct DevBuf {
+  void *p = nullptr;
+  ~DevBuf() { if (p) cudaFree(p); }
+};
+
+extern "C" int kgpu_u2p_cells(int n, const kgpu_config *cfg, const double *uu, double *pp, const double *g,
+                              const double *Gi, int *status, int *fixup) {
+  if (n < 0 || !cfg || (n > 0 && (!uu || !pp || !g || !Gi || !status || !fixup))) return KGPU_EINVAL;
+  if (cfg->nv != 9) return KGPU_EINVAL;
+  if (n == 0) return 0;
+  Grid G;
+  fill_grid_params(G, *cfg);
+  std::vector<double> su, sp, sm((size_t)n * 40), tmp;
+  to_soa(uu, su, n, G.nv);
+  to_soa(pp, sp, n, G.nv);
+  to_soa(g, tmp, n, 20);
+  memcpy(sm.data(), tmp.data(), (size_t)n * 20 * sizeof(double));
+  to_soa(Gi, tmp, n, 20);
+  memcpy(sm.data() + (size_t)n * 20, tmp.data(), (size_t)n * 20 * sizeof(double));
+  DevBuf du, dp, dm, ds, df;
+  CK(cudaMalloc(&du.p, su.size() * 8)); CK(cudaMalloc(&dp.p, sp.size() * 8));
+  CK(cudaMalloc(&dm.p, sm.size() * 8)); CK(cudaMalloc(&ds.p, n * 4)); CK(cudaMalloc(&df.p, n * 4));
+  CK(cudaMemcpy(du.p, su.data(), su.size() * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dp.p, sp.data(), sp.size() * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dm.p, sm.data(), sm.size() * 8, cudaMemcpyHostToDevice));
+  k_u2p_cells<<<nblocks(n, 128), 128>>>(G, n, (double *)du.p, (double *)dp.p, (double *)dm.p, (int *)ds.p, (int *)df.p);
+  CKL("k_u2p_cells");
+  CK(cudaMemcpy(sp.data(), dp.p, sp.size() * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(status, ds.p, n * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(fixup, df.p, n * 4, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < G.nv; k++) pp[(size_t)i * G.nv + k] = sp[(size_t)k * n + i];
+  return 0;
+}
+
+extern "C" int kgpu_p2u_cells(int n, const kgpu_config *cfg, const double *pp, double *uu, const double *g,
+                              const double *Gi) {
+  if (n < 0 || !cfg || (n > 0 && (!uu || !pp || !g || !Gi))) return KGPU_EINVAL;
+  if (cfg->nv != 9) return KGPU_EINVAL;
+  if (n == 0) return 0;
+  Grid G;
+  fill_grid_params(G, *cfg);
+  std::vector<double> sp, sm((size_t)n * 40), tmp, su((size_t)n * G.nv);
+  to_soa(pp, sp, n, G.nv);
+  to_soa(g, tmp, n, 20);
+  memcpy(sm.data(), tmp.data(), (size_t)n * 20 * sizeof(double));
+  to_soa(Gi, tmp, n, 20);
+  memcpy(sm.data() + (size_t)n * 20, tmp.data(), (size_t)n * 20 * sizeof(double));
+  DevBuf du, dp, dm;
+  CK(cudaMalloc(&du.p, su.size() * 8)); CK(cudaMalloc(&dp.p, sp.size() * 8)); CK(cudaMalloc(&dm.p, sm.size() * 8));
+  CK(cudaMemcpy(dp.p, sp.data(), sp.size() * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dm.p, sm.data(), sm.size() * 8, cudaMemcpyHostToDevice));
+  k_p2u_cells<<<nblocks(n, 128), 128>>>(G, n, (double *)dp.p, (double *)du.p, (double *)dm.p);
+  CKL("k_p2u_cells");
+  CK(cudaMemcpy(su.data(), du.p, su.size() * 8, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < G.nv; k++) uu[(size_t)i * G.nv + k] = su[(size_t)k * n + i];
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// instrumentation
+// ---------------------------------------------------------------------------
+extern "C" int kgpu_get_stream(kgpu_ctx *c, void **stream) {
+  if (!c || !stream) return KGPU_EINVAL;
+  *stream = (void *)c->stream;
+  return 0;
+}
+
+extern "C" int kgpu_profile_enable(kgpu_ctx *c, int on) {
+  if (!c) return KGPU_EINVAL;
+  c->profiling = on != 0;
+  return 0;
+}
+
+static int drain_profile(kgpu_ctx *c) {
+  CK(cudaStreamSynchronize(c->stream));
+  for (auto &r : c->prof) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, r.a, r.b));
+    c->prof_ms[r.id] += ms;
+    c->prof_n[r.id] += 1;
+    c->evpool.push_back(r.a);
+    c->evpool.push_back(r.b);
+  }
+  c->prof.clear();
+  return 0;
+}
+
+extern "C" int kgpu_profile_read(kgpu_ctx *c, int kernel, double *total_ms, long long *count, const char **name) {
+  if (!c || kernel < 0 || kernel >= K_NKERNELS) return KGPU_EINVAL;
+  int r = drain_profile(c);
+  if (r) return r;
+  if (total_ms) *total_ms = c->prof_ms[kernel];
+  if (count) *count = c->prof_n[kernel];
+  if (name) *name = kKernelNames[kernel];
+  return 0;
+}
+
+extern "C" int kgpu_profile_reset(kgpu_ctx *c) {
+  if (!c) return KGPU_EINVAL;
+  int r = drain_profile(c);
+  if (r) return r;
+  for (int k = 0; k < K_NKERNELS; k++) {
+    c->prof_ms[k] = 0.;
+    c->prof_n[k] = 0;
+  }
+  return 0;
+}
+
+extern "C" int kgpu_launch_count(kgpu_ctx *c, long long *out) {
+  if (!c || !out) return KGPU_EINVAL;
+  *out = c->launches;
+  return 0;
+}
+
+extern "C" int kgpu_num_kernels(void) { return K_NKERNELS; }

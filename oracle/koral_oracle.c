@@ -1617,3 +1617,43 @@ void ko_set_floors(ko_grid *G, double rhofloor, double uurhomin, double uurhomax
   G->b2rhoratiomax = b2rhomax;
   G->gammamaxhd = gammamax;
 }
+
+/* ------------------------------------------------------------------ */
+/* batched per-cell entry points for solver-level parity tests:        */
+/* n cells, each with its own metric point (20 doubles of g and of G)  */
+/* ------------------------------------------------------------------ */
+int ko_u2p_batch(const ko_grid *G, int n, const double *uu, double *pp, const double *g, const double *Gm,
+                 int *status, int *fixup)
+{
+  int i;
+  for (i = 0; i < n; i++) {
+    ko_geom geom;
+    int corrected[3], fixups[2];
+    ko_geom_from(g + (long)i * 20, Gm + (long)i * 20, &geom);
+    status[i] = ko_u2p(G, uu + (long)i * G->nv, pp + (long)i * G->nv, &geom, corrected, fixups);
+    fixup[i] = fixups[0];
+  }
+  return 0;
+}
+
+int ko_p2u_batch(const ko_grid *G, int n, const double *pp, double *uu, const double *g, const double *Gm)
+{
+  int i;
+  for (i = 0; i < n; i++) {
+    ko_geom geom;
+    ko_geom_from(g + (long)i * 20, Gm + (long)i * 20, &geom);
+    ko_p2u_mhd(G, pp + (long)i * G->nv, uu + (long)i * G->nv, &geom);
+  }
+  return 0;
+}
+
+int ko_floors_batch(const ko_grid *G, int n, double *pp, const double *g, const double *Gm, int *ret)
+{
+  int i;
+  for (i = 0; i < n; i++) {
+    ko_geom geom;
+    ko_geom_from(g + (long)i * 20, Gm + (long)i * 20, &geom);
+    ret[i] = ko_check_floors_mhd(G, pp + (long)i * G->nv, &geom);
+  }
+  return 0;
+}

@@ -110,6 +110,12 @@ int ko_rk2_step(ko_grid *G);
 /* initial data: relativistic Orszag-Tang vortex on the current grid */
 void ko_init_orszag_tang(ko_grid *G);
 
+/* batched per-cell calls (parameters taken from G) */
+int ko_u2p_batch(const ko_grid *G, int n, const double *uu, double *pp, const double *g, const double *Gm,
+                 int *status, int *fixup);
+int ko_p2u_batch(const ko_grid *G, int n, const double *pp, double *uu, const double *g, const double *Gm);
+int ko_floors_batch(const ko_grid *G, int n, double *pp, const double *g, const double *Gm, int *ret);
+
 /* accessors for the ctypes wrapper */
 double *ko_array(ko_grid *G, int which);
 int ko_layout(const ko_grid *G, int *out);

@@ -60,6 +60,10 @@ class OracleGrid:
             L.ko_begin_step.restype = ctypes.c_double
             L.ko_rk2_step.argtypes = [ctypes.c_void_p]
             L.ko_op_explicit.argtypes = [ctypes.c_void_p, ctypes.c_double]
+            ip = ctypes.POINTER(ctypes.c_int)
+            L.ko_u2p_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, ip, ip]
+            L.ko_p2u_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp]
+            L.ko_floors_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, ip]
             cls._lib_handle = L
         return cls._lib_handle
 
@@ -88,8 +92,34 @@ class OracleGrid:
     def scalar(self, i):
         return self.L.ko_scalar(self.h, i)
 
+    def u2p_batch(self, uu, pp, g, G):
+        """Per-cell u2p (u2p.c:176) on n independent cells; returns (pp, status, fixup)."""
+        uu = np.ascontiguousarray(uu, dtype=np.float64)
+        pp = np.ascontiguousarray(pp, dtype=np.float64).copy()
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        G = np.ascontiguousarray(G, dtype=np.float64)
+        n = uu.shape[0]
+        st = np.zeros(n, dtype=np.int32)
+        fx = np.zeros(n, dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        self.L.ko_u2p_batch(self.h, n, uu.ctypes.data_as(_dp), pp.ctypes.data_as(_dp), g.ctypes.data_as(_dp),
+                            G.ctypes.data_as(_dp), st.ctypes.data_as(ip), fx.ctypes.data_as(ip))
+        return pp, st, fx
+
+    def p2u_batch(self, pp, g, G):
+        pp = np.ascontiguousarray(pp, dtype=np.float64)
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        G = np.ascontiguousarray(G, dtype=np.float64)
+        uu = np.empty_like(pp)
+        self.L.ko_p2u_batch(self.h, pp.shape[0], pp.ctypes.data_as(_dp), uu.ctypes.data_as(_dp),
+                            g.ctypes.data_as(_dp), G.ctypes.data_as(_dp))
+        return uu
+
     def set_physics(self, gamma, tsteplim, int_order, fluxmethod):
         self.L.ko_set_physics(self.h, gamma, tsteplim, int_order, fluxmethod)
+
+    def set_floors(self, rhofloor, uurhomin, uurhomax, b2rhomax, gammamax):
+        self.L.ko_set_floors(self.h, rhofloor, uurhomin, uurhomax, b2rhomax, gammamax)
 
     def set_uniform_grid(self, lo, hi):
         lo = (ctypes.c_double * 3)(*lo)
