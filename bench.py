@@ -7,6 +7,10 @@
 A step is one full RK2 time step (ko.c:571-626: two explicit operators and two
 inversions with fixups and boundary conditions) of the workload.  Workloads:
 
+  torus   (default) 3D magnetised Kerr torus, 192x96x64: spin 0.9, MKS2
+          coordinates, r in [1.8, 1000], Fishbone-Moncrief torus r_in = 6,
+          r_max = 12, Gamma = 13/9, beta_min = 100, 2% seeded pressure noise,
+          density floor 1e-4 r^-1.5, MP5 + HLL + flux-CT, RK2, CFL 0.5
   ot128   relativistic Orszag-Tang vortex, 128x128, PPM + LLF + flux-CT,
           Minkowski, Gamma = 5/3, CFL 0.5 (the reference's CPU-runnable case)
 
@@ -36,18 +40,31 @@ METRIC = "FP64 zone-cycles/s (1 B200)"
 UNIT = "zone-cycles/s"
 
 WORKLOADS = {
+    "torus": dict(desc="3D magnetised Kerr torus 192x96x64 (a=0.9 MKS2, FM torus r_in=6 r_max=12, Gamma 13/9, "
+                       "beta_min 100, 2% noise, MP5+HLL+flux-CT, RK2, CFL 0.5)",
+                  shape=(192, 96, 64), ref_lib="libkref_fmtorus_omp.so", ref_serial="libkref_fmtorus.so",
+                  ref_sample_steps=4),
     "ot128": dict(desc="relativistic Orszag-Tang vortex 128x128 (Minkowski, PPM+LLF+flux-CT, RK2, CFL 0.5, Gamma 5/3)",
-                  n=128, ref_lib="libkref_orszagrel_128_omp.so", ref_serial="libkref_orszagrel_128.so"),
+                  shape=(128, 128, 1), ref_lib="libkref_orszagrel_128_omp.so", ref_serial="libkref_orszagrel_128.so",
+                  ref_sample_steps=40),
 }
+
+
+def make_subdomain(kgpu, name):
+    wl = WORKLOADS[name]
+    nx, ny, nz = wl["shape"]
+    if name == "torus":
+        return kgpu.fm_torus(nx, ny, nz)
+    return kgpu.orszag_tang(nx)
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ot128", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="torus", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -130,22 +147,29 @@ def run_reference_cpu(wl, steps, warm, threads):
     return d["cells"] * d["steps"] / d["seconds"], None
 
 
+def cells_of(wl):
+    nx, ny, nz = wl["shape"]
+    return nx * ny * nz
+
+
 def reference_arm(args, wl, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    # each step is one full RK2 step of the reference on all host cores
-    val, err = run_reference_cpu(wl, max(1, args.steps), max(0, args.warmup), threads)
+    # one full RK2 step of the reference on all host cores per step, at most
+    # ref_sample_steps of them (a full-size CPU step takes seconds)
+    nsteps = max(1, min(args.steps, wl["ref_sample_steps"]))
+    val, err = run_reference_cpu(wl, nsteps, min(max(0, args.warmup), 1), threads)
     if val is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
         return
     line = {
         "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wl["n"] ** 2 / val * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": cells_of(wl) / val * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": wl["desc"], "parallelism": "openmp host threads"},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"{args.steps} RK2 steps after {args.warmup} warm-up steps"},
+                         "sample": f"{nsteps} full RK2 steps after {min(max(0, args.warmup), 1)} warm-up step(s)"},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -164,10 +188,10 @@ def our_arm(args, wl, rank, world, local_rank):
     from koral_b200 import build
     build.build()
 
-    n = wl["n"]
-    s = koral_b200.orszag_tang(n)
+    s = make_subdomain(koral_b200, args.workload)
     ext = torch.cuda.ExternalStream(s.stream, device=dev)
-    cells = n * n
+    nx, ny, nz = wl["shape"]
+    cells = nx * ny * nz
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # 256 MB > 126 MB L2
 
     dist = None
@@ -265,7 +289,7 @@ def our_arm(args, wl, rank, world, local_rank):
     # algorithmic bytes of the face-flux kernels: 16*NV bytes per face
     # (read the primitives once, write the face flux once)
     nv = 9
-    nfaces = (n + 1) * (n + 2)
+    nfaces = (nx + 1) * (ny + 2 if ny > 1 else 1) * (nz + 2 if nz > 1 else 1)
     flux_ms = prof["k_flux_x"][0] / max(1, prof["k_flux_x"][1])
     flux_gbs = 16 * nv * nfaces / (flux_ms / 1e3) / 1e9 if flux_ms > 0 else None
 
@@ -287,10 +311,11 @@ def our_arm(args, wl, rank, world, local_rank):
     }
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        val, err = run_reference_cpu(wl, 10, 2, threads)
+        ns = max(1, wl["ref_sample_steps"] // 2)
+        val, err = run_reference_cpu(wl, ns, 1, threads)
         if val is not None:
             line["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": threads, "kind": "reference",
-                                    "sample": "10 RK2 steps of the same workload after 2 warm-up steps"}
+                                    "sample": f"{ns} full RK2 steps of the same workload after 1 warm-up step"}
         else:
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
                                     "sample": f"unavailable: {err}"}

@@ -51,6 +51,18 @@ extern "C" {
 #define KGPU_ARR_UT0 2
 #define KGPU_ARR_UT1 3
 
+/* boundary conditions per axis (set_bc_core finite.c:2673-2748 and the
+ * problem plug-ins' calc_bc):
+ *  PERIODIC       primitives copied from the periodic image, conserved from p2u
+ *  OUTFLOW        primitives copied from the nearest domain cell, p2u
+ *  REFLECT        mirror image with the normal velocity and normal magnetic
+ *                 field reversed (polar axis), p2u
+ *  PERIODIC_COPY  conserved and primitives both copied from the periodic image */
+#define KGPU_BC_PERIODIC 0
+#define KGPU_BC_OUTFLOW 1
+#define KGPU_BC_REFLECT 2
+#define KGPU_BC_PERIODIC_COPY 3
+
 typedef struct kgpu_ctx kgpu_ctx;
 
 /* Compile-time choices of a KORAL problem build (define.h/choices.h),
@@ -62,7 +74,7 @@ typedef struct {
   int int_order;           /* KGPU_PPM or KGPU_MP5                           */
   int fluxmethod;          /* KGPU_LAXF or KGPU_HLL                          */
   int axisym_metric;       /* METRICAXISYMMETRIC: one phi slice of metric     */
-  int periodic[3];         /* PERIODIC_XBC/YBC/ZBC                            */
+  int bc[3];               /* boundary kind per axis, KGPU_BC_* below         */
   double gamma;            /* GAMMA                                           */
   double tsteplim;         /* TSTEPLIM (Courant number)                       */
   double rhofloor;         /* RHOFLOOR                                        */
@@ -93,6 +105,10 @@ int kgpu_set_uniform_grid(kgpu_ctx *ctx, const double lo[3], const double hi[3])
 int kgpu_upload_metric(kgpu_ctx *ctx, const double *g, const double *G, const double *gKr,
                        const double *gbx, const double *gby, const double *gbz,
                        const double *Gbx, const double *Gby, const double *Gbz);
+/* Radius-dependent density floor (RHOFLOOR_BH, u2p.c:546-557) tabulated per
+ * x-index: at cell centres (SX values, ic in [-NG, NX+NG)) and at x-faces
+ * (SX+1 values).  Pass null pointers to switch it off. */
+int kgpu_set_density_floor(kgpu_ctx *ctx, const double *centres, const double *xfaces);
 /* Flat spacetime (MINKCOORDS) tables generated on the device. */
 int kgpu_set_minkowski_metric(kgpu_ctx *ctx);
 
@@ -141,6 +157,37 @@ int kgpu_reset_counters(kgpu_ctx *ctx);
 /* Relativistic Orszag-Tang vortex on the current grid (Minkowski metric). */
 int kgpu_init_orszag_tang(kgpu_ctx *ctx);
 
+/* Magnetised Kerr torus in modified Kerr-Schild coordinates (MKS2). ------ */
+typedef struct {
+  double spin;               /* black-hole spin a                              */
+  double r0, h0;             /* MKS2 parameters: r = exp(x1)+r0, theta(x2; h0) */
+  double r_lo, r_hi;         /* radial extent of the grid                      */
+  double x2_lo, x2_hi;       /* extent in the theta code coordinate            */
+  double rin, rmax;          /* torus inner edge and pressure maximum          */
+  double kappa;              /* polytropic constant of the torus               */
+  double noise;              /* relative amplitude of the pressure noise       */
+  unsigned long long seed;   /* seed of the per-cell noise                     */
+  double atm_rho0, atm_uu0;  /* atmosphere rho0 r^-1.5, u0 r^-2.5 (and floor)  */
+  double maxbeta;            /* max pmag/pgas after normalisation (1/beta_min) */
+} kgpu_torus_params;
+
+/* The benchmark torus: a = 0.9, r in [1.8, 1000], r_in = 6, r_max = 12. */
+int kgpu_default_torus_params(kgpu_torus_params *tp);
+/* Metric tables of MKS2 Kerr on the given faces, KORAL layout (host-only,
+ * no GPU needed); same argument order as kgpu_upload_metric. */
+int kgpu_mks2_metric_tables(double a, double r0, double h0, int nx, int ny, int nz, int ng, int axisym,
+                            const double *xbx, const double *xby, const double *xbz, double *g, double *G,
+                            double *gKr, double *gbx, double *gby, double *gbz, double *Gbx, double *Gby,
+                            double *Gbz);
+/* Fishbone-Moncrief torus state (host-only), KORAL layout, ghosts zero. */
+int kgpu_fm_torus_state(const kgpu_torus_params *tp, const kgpu_config *cfg, const double *xbx, const double *xby,
+                        const double *xbz, const double *g, const double *G, double *u, double *p);
+/* Density floor table of the torus (host-only), as kgpu_set_density_floor takes it. */
+int kgpu_fm_torus_floor(const kgpu_torus_params *tp, int nx, int ng, const double *xbx, double *centres,
+                        double *xfaces);
+/* Whole set-up on a context: grid, metric, floor, state, boundaries, first dt. */
+int kgpu_init_fm_torus(kgpu_ctx *ctx, const kgpu_torus_params *tp);
+
 /* Batched per-cell solvers (host arrays, n cells, one metric point each:
  * g and G hold 20 doubles per cell).  They replace per-cell calls of
  *   int u2p(ldouble *uu, ldouble *pp, void *geom, int corrected[3],
@@ -166,6 +213,13 @@ int kgpu_profile_reset(kgpu_ctx *ctx);
 int kgpu_num_kernels(void);
 /* Kernels launched by this context so far (graph replays included). */
 int kgpu_launch_count(kgpu_ctx *ctx, long long *out);
+
+/* Face fluxes of the last explicit operator along axis d (flbx/flby/flbz,
+ * KORAL layout [face][NV]) and the corner EMFs of flux-CT (emf, KORAL layout
+ * [(NZ+1)(NY+1)(NX+1)][3]).  The magnetic-field components of the face
+ * fluxes are the Riemann fluxes before flux_ct rewrites them. */
+int kgpu_download_flux(kgpu_ctx *ctx, int d, double *out);
+int kgpu_download_emf(kgpu_ctx *ctx, double *out);
 
 /* Last CUDA error string of this thread's most recent failing call. */
 const char *kgpu_last_error(void);

@@ -18,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libkoral_b200.so")
 
 PPM, MP5 = 2, 4
+BC_PERIODIC, BC_OUTFLOW, BC_REFLECT, BC_PERIODIC_COPY = 0, 1, 2, 3
 LAXF, HLL = 0, 1
 ARR_U, ARR_P, ARR_UT0, ARR_UT1 = 0, 1, 2, 3
 
@@ -35,11 +36,24 @@ class Config(ctypes.Structure):
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
         ("ng", ctypes.c_int), ("nv", ctypes.c_int),
         ("int_order", ctypes.c_int), ("fluxmethod", ctypes.c_int),
-        ("axisym_metric", ctypes.c_int), ("periodic", ctypes.c_int * 3),
+        ("axisym_metric", ctypes.c_int), ("bc", ctypes.c_int * 3),
         ("gamma", ctypes.c_double), ("tsteplim", ctypes.c_double),
         ("rhofloor", ctypes.c_double), ("uurhoratiomin", ctypes.c_double),
         ("uurhoratiomax", ctypes.c_double), ("b2rhoratiomax", ctypes.c_double),
         ("gammamaxhd", ctypes.c_double), ("u2pconv", ctypes.c_double),
+    ]
+
+
+class TorusParams(ctypes.Structure):
+    """kgpu_torus_params of include/koral_b200.h."""
+
+    _fields_ = [
+        ("spin", ctypes.c_double), ("r0", ctypes.c_double), ("h0", ctypes.c_double),
+        ("r_lo", ctypes.c_double), ("r_hi", ctypes.c_double),
+        ("x2_lo", ctypes.c_double), ("x2_hi", ctypes.c_double),
+        ("rin", ctypes.c_double), ("rmax", ctypes.c_double), ("kappa", ctypes.c_double),
+        ("noise", ctypes.c_double), ("seed", ctypes.c_ulonglong),
+        ("atm_rho0", ctypes.c_double), ("atm_uu0", ctypes.c_double), ("maxbeta", ctypes.c_double),
     ]
 
 
@@ -62,6 +76,7 @@ def lib():
             "kgpu_set_uniform_grid": [vp, _dp, _dp],
             "kgpu_upload_metric": [vp] + [_dp] * 9,
             "kgpu_set_minkowski_metric": [vp],
+            "kgpu_set_density_floor": [vp, _dp, _dp],
             "kgpu_upload_state": [vp, _dp, _dp],
             "kgpu_download_state": [vp, _dp, _dp],
             "kgpu_download_array": [vp, ctypes.c_int, _dp],
@@ -84,6 +99,13 @@ def lib():
             "kgpu_u2p_cells": [ctypes.c_int, ctypes.POINTER(Config), _dp, _dp, _dp, _dp,
                                ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
             "kgpu_p2u_cells": [ctypes.c_int, ctypes.POINTER(Config), _dp, _dp, _dp, _dp],
+            "kgpu_default_torus_params": [ctypes.POINTER(TorusParams)],
+            "kgpu_mks2_metric_tables": [ctypes.c_double] * 3 + [ctypes.c_int] * 5 + [_dp] * 12,
+            "kgpu_fm_torus_state": [ctypes.POINTER(TorusParams), ctypes.POINTER(Config)] + [_dp] * 7,
+            "kgpu_fm_torus_floor": [ctypes.POINTER(TorusParams), ctypes.c_int, ctypes.c_int, _dp, _dp, _dp],
+            "kgpu_init_fm_torus": [vp, ctypes.POINTER(TorusParams)],
+            "kgpu_download_flux": [vp, ctypes.c_int, _dp],
+            "kgpu_download_emf": [vp, _dp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -116,9 +138,9 @@ def default_config(nx, ny, nz, **kw):
     c = Config()
     _check(lib().kgpu_default_config(ctypes.byref(c), nx, ny, nz), "kgpu_default_config")
     for k, v in kw.items():
-        if k == "periodic":
+        if k == "bc":
             for i in range(3):
-                c.periodic[i] = int(v[i])
+                c.bc[i] = int(v[i])
         else:
             setattr(c, k, v)
     return c
@@ -168,12 +190,24 @@ class Subdomain:
         a = [np.ascontiguousarray(x, dtype=np.float64) for x in (xbx, xby, xbz)]
         _check(self.L.kgpu_upload_grid(self.h, *[_ptr(x) for x in a]), "kgpu_upload_grid")
 
+    def set_density_floor(self, centres, xfaces):
+        if centres is None:
+            _check(self.L.kgpu_set_density_floor(self.h, None, None), "kgpu_set_density_floor")
+            return
+        c = np.ascontiguousarray(centres, dtype=np.float64)
+        f = np.ascontiguousarray(xfaces, dtype=np.float64)
+        _check(self.L.kgpu_set_density_floor(self.h, _ptr(c), _ptr(f)), "kgpu_set_density_floor")
+
     def set_minkowski_metric(self):
         _check(self.L.kgpu_set_minkowski_metric(self.h), "kgpu_set_minkowski_metric")
 
     def upload_metric(self, g, G, gKr, gbx, gby, gbz, Gbx, Gby, Gbz):
         a = [np.ascontiguousarray(x, dtype=np.float64) for x in (g, G, gKr, gbx, gby, gbz, Gbx, Gby, Gbz)]
         _check(self.L.kgpu_upload_metric(self.h, *[_ptr(x) for x in a]), "kgpu_upload_metric")
+
+    def init_fm_torus(self, tp=None):
+        tp = tp or torus_params()
+        _check(self.L.kgpu_init_fm_torus(self.h, ctypes.byref(tp)), "kgpu_init_fm_torus")
 
     def init_orszag_tang(self):
         _check(self.L.kgpu_init_orszag_tang(self.h), "kgpu_init_orszag_tang")
@@ -189,6 +223,18 @@ class Subdomain:
         p = np.empty(self.shape)
         _check(self.L.kgpu_download_state(self.h, _ptr(u), _ptr(p)), "kgpu_download_state")
         return u, p
+
+    def download_flux(self, d):
+        nf = [(self.sx + 1) * self.sy * self.sz, self.sx * (self.sy + 1) * self.sz, self.sx * self.sy * (self.sz + 1)][d]
+        a = np.empty((nf, self.nv))
+        _check(self.L.kgpu_download_flux(self.h, d, _ptr(a)), "kgpu_download_flux")
+        return a
+
+    def download_emf(self):
+        c = self.cfg
+        a = np.empty(((c.nx + 1) * (c.ny + 1) * (c.nz + 1), 3))
+        _check(self.L.kgpu_download_emf(self.h, _ptr(a)), "kgpu_download_emf")
+        return a
 
     def download(self, which):
         a = np.empty(self.shape)
@@ -315,3 +361,56 @@ def p2u_cells(cfg, pp, g, G):
     _check(lib().kgpu_p2u_cells(pp.shape[0], ctypes.byref(cfg), _ptr(pp), _ptr(uu), _ptr(g), _ptr(G)),
            "kgpu_p2u_cells")
     return uu
+
+
+def torus_params(**kw):
+    tp = TorusParams()
+    _check(lib().kgpu_default_torus_params(ctypes.byref(tp)), "kgpu_default_torus_params")
+    for k, v in kw.items():
+        setattr(tp, k, v)
+    return tp
+
+
+def torus_config(nx=192, ny=96, nz=64):
+    """Config of the magnetised Kerr torus: MP5 + HLL, MKS2 axisymmetric
+    metric, outflow / polar reflection / periodic phi boundaries."""
+    return default_config(nx, ny, nz, ng=4, int_order=MP5, fluxmethod=HLL, axisym_metric=1,
+                          bc=(BC_OUTFLOW, BC_REFLECT, BC_PERIODIC_COPY), gamma=13.0 / 9.0, tsteplim=0.5,
+                          uurhoratiomin=1e-10, uurhoratiomax=1e2, b2rhoratiomax=100.0)
+
+
+def fm_torus(nx=192, ny=96, nz=64, tp=None):
+    """The benchmark torus on the current GPU, initialised by the product's
+    own metric and Fishbone-Moncrief set-up."""
+    s = Subdomain(torus_config(nx, ny, nz))
+    s.init_fm_torus(tp)
+    return s
+
+
+def mks2_metric_tables(tp, cfg, xb):
+    """Host-side MKS2 metric tables (KORAL layout) for faces xb = (xbx, xby, xbz)."""
+    sx = cfg.nx + 2 * cfg.ng
+    sy = cfg.ny + 2 * cfg.ng if cfg.ny > 1 else 1
+    sz = cfg.nz + 2 * cfg.ng if cfg.nz > 1 else 1
+    sm = 1 if cfg.axisym_metric else sz
+    shapes = [sx * sy * sm * 20, sx * sy * sm * 20, sx * sy * sm * 64,
+              (sx + 1) * sy * sm * 20, sx * (sy + 1) * sm * 20, sx * sy * (sm + 1) * 20,
+              (sx + 1) * sy * sm * 20, sx * (sy + 1) * sm * 20, sx * sy * (sm + 1) * 20]
+    out = [np.zeros(n) for n in shapes]
+    xb = [np.ascontiguousarray(x, dtype=np.float64) for x in xb]
+    _check(lib().kgpu_mks2_metric_tables(tp.spin, tp.r0, tp.h0, cfg.nx, cfg.ny, cfg.nz, cfg.ng, cfg.axisym_metric,
+                                         *[_ptr(x) for x in xb], *[_ptr(o) for o in out]), "kgpu_mks2_metric_tables")
+    return out
+
+
+def fm_torus_state(tp, cfg, xb, g, G):
+    sx = cfg.nx + 2 * cfg.ng
+    sy = cfg.ny + 2 * cfg.ng
+    sz = cfg.nz + 2 * cfg.ng
+    u = np.zeros((sz, sy, sx, cfg.nv))
+    p = np.zeros((sz, sy, sx, cfg.nv))
+    xb = [np.ascontiguousarray(x, dtype=np.float64) for x in xb]
+    _check(lib().kgpu_fm_torus_state(ctypes.byref(tp), ctypes.byref(cfg), *[_ptr(x) for x in xb],
+                                     _ptr(np.ascontiguousarray(g)), _ptr(np.ascontiguousarray(G)), _ptr(u), _ptr(p)),
+           "kgpu_fm_torus_state")
+    return u, p

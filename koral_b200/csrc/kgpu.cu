@@ -91,25 +91,37 @@ __global__ void k_bc_faces(Grid G, Box b) {
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
   if (in_domain(G, ix, iy, iz) || outside_gc(G, ix, iy, iz)) return;
-  int iix = ix, iiy = iy, iiz = iz;
-  if (ix < 0 || ix >= G.nx) {
-    if (ix < 0) iix = ix + G.nx;
-    if (ix > G.nx - 1) iix = ix - G.nx;
-  } else if (iy < 0 || iy >= G.ny) {
-    if (iy < 0) iiy = iy + G.ny;
-    if (iy > G.ny - 1) iiy = iy - G.ny;
-    if (G.ny < G.ng) iiy = 0;
+  int d = (ix < 0 || ix >= G.nx) ? 0 : ((iy < 0 || iy >= G.ny) ? 1 : 2);
+  int c3[3] = {ix, iy, iz}, n3[3] = {G.nx, G.ny, G.nz};
+  int s3[3] = {ix, iy, iz};
+  const int kind = G.bc[d];
+  const int i = c3[d], n = n3[d];
+  bool flip = false;
+  if (kind == KGPU_BC_OUTFLOW) {
+    s3[d] = i < 0 ? 0 : n - 1;
+  } else if (kind == KGPU_BC_REFLECT) {
+    s3[d] = i < 0 ? -i - 1 : 2 * n - i - 1;
+    flip = true;
   } else {
-    if (iz < 0) iiz = iz + G.nz;
-    if (iz > G.nz - 1) iiz = iz - G.nz;
-    if (G.nz < G.ng) iiz = 0;
+    if (i < 0) s3[d] = i + n;
+    if (i > n - 1) s3[d] = i - n;
+    if (d > 0 && n < G.ng) s3[d] = 0;   // finite.c:2705, 2720
   }
-  long c = cell_index(G, ix, iy, iz), s = cell_index(G, iix, iiy, iiz);
+  long c = cell_index(G, ix, iy, iz), s = cell_index(G, s3[0], s3[1], s3[2]);
   double pp[NVMAX], uu[NVMAX];
   load_cell(G.p, G.ncell, s, G.nv, pp);
-  Geom g;
-  geom_centre(G, ix, iy, iz, g);
-  p2u_full(G, pp, uu, g);
+  if (flip) {
+    // the component normal to the boundary: VX/B1 for x, VY/B2 for y, VZ/B3 for z
+    pp[VX + d] = -pp[VX + d];
+    pp[B1 + d] = -pp[B1 + d];
+  }
+  if (kind == KGPU_BC_PERIODIC_COPY) {
+    load_cell(G.u, G.ncell, s, G.nv, uu);
+  } else {
+    Geom g;
+    geom_centre(G, ix, iy, iz, g);
+    p2u_full(G, pp, uu, g);
+  }
   store_cell(G.p, G.ncell, c, G.nv, pp);
   store_cell(G.u, G.ncell, c, G.nv, uu);
 }
@@ -171,6 +183,107 @@ __global__ void k_bc_corners2d(Grid G) {
   p2u_full(G, pp, uu, g);
   store_cell(G.p, G.ncell, c, G.nv, pp);
   store_cell(G.u, G.ncell, c, G.nv, uu);
+}
+
+// Edges and corners of a 3D domain with physical boundaries, in the
+// reference's order (finite.c:3330-3705): edges elongated along z, then
+// along y, then along x, each filling the first NG-1 cells of the two faces
+// next to the edge from the adjacent ghost row and two diagonal cells as
+// means of their neighbours; then the eight NG^3 corner blocks copy the
+// nearest domain corner cell.  A pass reads only cells that earlier passes
+// (or the face fill) wrote, so the lines of one pass run in parallel.
+__device__ inline void set_from(const Grid &G, int tx, int ty, int tz, int s1x, int s1y, int s1z, int s2x, int s2y,
+                                int s2z, bool avg) {
+  long c = cell_index(G, tx, ty, tz), a = cell_index(G, s1x, s1y, s1z), b = cell_index(G, s2x, s2y, s2z);
+  double pp[NVMAX], uu[NVMAX];
+  for (int iv = 0; iv < G.nv; iv++) {
+    double va = G.p[iv * G.ncell + a];
+    pp[iv] = avg ? .5 * (va + G.p[iv * G.ncell + b]) : va;
+  }
+  Geom g;
+  geom_centre(G, tx, ty, tz, g);
+  p2u_full(G, pp, uu, g);
+  store_cell(G.p, G.ncell, c, G.nv, pp);
+  store_cell(G.u, G.ncell, c, G.nv, uu);
+}
+// one line of one elongated-edge pass.  Edge axis c, the two other axes
+// (a, b); corner k: bit 1 = high end of a, bit 0 = high end of b; position t
+// along c in [-NG, N_c+NG).  In (a, b) coordinates, with the ghost layers
+// counted outwards, the reference writes for i = 0..NG-2
+//   lo,lo: (-NG+i,-1)<-(-NG+i,0)      (-1,-NG+i)<-(0,-NG+i)
+//   lo,hi: (-NG+i,NB)<-(-NG+i,NB-1)   (-1,NB+i+1)<-(0,NB+i+1)
+//   hi,lo: (NA,-NG+i)<-(NA-1,-NG+i)   (NA+i+1,-1)<-(NA+i+1,0)
+//   hi,hi: (NA+i+1,NB)<-(NA+i+1,NB-1) (NA,NB+i+1)<-(NA-1,NB+i+1)
+// and then the two diagonal cells as means of their inner neighbours.
+// (x, y, z) of the cell at (va, vb) in the (a, b) plane and t along c;
+// plain selects, no indexed local array
+__device__ inline void at3(int c, int a, int b, int t, int va, int vb, int &x, int &y, int &z) {
+  x = a == 0 ? va : (b == 0 ? vb : t);
+  y = a == 1 ? va : (b == 1 ? vb : t);
+  z = a == 2 ? va : (b == 2 ? vb : t);
+  (void)c;
+}
+// target (ta, tb) and source (sa, sb) of copy j of ghost layer i
+__device__ inline void edge_copy(bool hiA, bool hiB, int NG, int NA, int NB, int i, int j, int &ta, int &tb, int &sa,
+                                 int &sb) {
+  if (!hiA && !hiB) {
+    if (j == 0) { ta = -NG + i; tb = -1; sa = -NG + i; sb = 0; }
+    else { ta = -1; tb = -NG + i; sa = 0; sb = -NG + i; }
+  } else if (!hiA && hiB) {
+    if (j == 0) { ta = -NG + i; tb = NB; sa = -NG + i; sb = NB - 1; }
+    else { ta = -1; tb = NB + i + 1; sa = 0; sb = NB + i + 1; }
+  } else if (hiA && !hiB) {
+    if (j == 0) { ta = NA; tb = -NG + i; sa = NA - 1; sb = -NG + i; }
+    else { ta = NA + i + 1; tb = -1; sa = NA + i + 1; sb = 0; }
+  } else {
+    if (j == 0) { ta = NA + i + 1; tb = NB; sa = NA + i + 1; sb = NB - 1; }
+    else { ta = NA; tb = NB + i + 1; sa = NA - 1; sb = NB + i + 1; }
+  }
+}
+__global__ void k_bc_edges3d(Grid G, int c, int a, int b) {
+  const int NG = G.ng;
+  const int NA = a == 0 ? G.nx : (a == 1 ? G.ny : G.nz);
+  const int NB = b == 0 ? G.nx : (b == 1 ? G.ny : G.nz);
+  const int NC = c == 0 ? G.nx : (c == 1 ? G.ny : G.nz);
+  int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  int len = NC + 2 * NG;
+  if (tid >= 4 * len) return;
+  const int k = tid / len, t = tid % len - NG;
+  const bool hiA = (k >> 1) & 1, hiB = k & 1;
+  int x, y, z, x1, y1, z1, x2, y2, z2;
+  for (int i = 0; i < NG - 1; i++)
+    for (int j = 0; j < 2; j++) {
+      int ta, tb, sa, sb;
+      edge_copy(hiA, hiB, NG, NA, NB, i, j, ta, tb, sa, sb);
+      at3(c, a, b, t, ta, tb, x, y, z);
+      at3(c, a, b, t, sa, sb, x1, y1, z1);
+      set_from(G, x, y, z, x1, y1, z1, x1, y1, z1, false);
+    }
+  // diagonal cells: g1 = first ghost layer in both a and b, g2 = second;
+  // mean of (g.a, g.b - sB) and (g.a - sA, g.b), s pointing out of the domain
+  const int sA = hiA ? 1 : -1, sB = hiB ? 1 : -1;
+  const int g1a = hiA ? NA : -1, g1b = hiB ? NB : -1;
+  at3(c, a, b, t, g1a, g1b, x, y, z);
+  at3(c, a, b, t, g1a, g1b - sB, x1, y1, z1);
+  at3(c, a, b, t, g1a - sA, g1b, x2, y2, z2);
+  set_from(G, x, y, z, x1, y1, z1, x2, y2, z2, true);
+  const int g2a = g1a + sA, g2b = g1b + sB;
+  at3(c, a, b, t, g2a, g2b, x, y, z);
+  at3(c, a, b, t, g2a, g2b - sB, x1, y1, z1);
+  at3(c, a, b, t, g2a - sA, g2b, x2, y2, z2);
+  set_from(G, x, y, z, x1, y1, z1, x2, y2, z2, true);
+}
+__global__ void k_bc_corners3d(Grid G) {
+  const int NG = G.ng;
+  int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  int per = NG * NG * NG;
+  if (tid >= 8 * per) return;
+  int k = tid / per, r = tid % per;
+  bool hx = k & 1, hy = (k >> 1) & 1, hz = (k >> 2) & 1;
+  int ox = r % NG, oy = (r / NG) % NG, oz = r / (NG * NG);
+  int tx = hx ? G.nx + ox : -NG + ox, ty = hy ? G.ny + oy : -NG + oy, tz = hz ? G.nz + oz : -NG + oz;
+  int sx = hx ? G.nx - 1 : 0, sy = hy ? G.ny - 1 : 0, sz = hz ? G.nz - 1 : 0;
+  set_from(G, tx, ty, tz, sx, sy, sz, sx, sy, sz, false);
 }
 
 // ---------------------------------------------------------------------------
@@ -257,15 +370,17 @@ __global__ void __launch_bounds__(128) k_flux(Grid G, Box b) {
   geom_face(G, ix, iy, iz, D, g);
   const bool magn = nv > B3;
   double fL[NVMAX], uL[NVMAX], fR[NVMAX], uR[NVMAX];
+  // density floor of this face: x-faces sit at xb[ix], the others at x[ix]
+  const double rfl = G.rhofl_c ? (D == 0 ? G.rhofl_f[ix + G.ng] : G.rhofl_c[ix + G.ng]) : -1.;
   {
-    check_floors_mhd(G, pL, g);
+    check_floors_mhd(G, pL, g, rfl);
     Kin k;
     kinematics(pL, g, magn, k);
     flux_prime(G, pL, D, g, k, fL);
     p2u_mhd(G, pL, uL, g, k);
   }
   {
-    check_floors_mhd(G, pR, g);
+    check_floors_mhd(G, pR, g, rfl);
     Kin k;
     kinematics(pR, g, magn, k);
     flux_prime(G, pR, D, g, k, fR);
@@ -481,7 +596,7 @@ __global__ void __launch_bounds__(128) k_u2p(Grid G, Box b) {
   if (ret == -1) atomicAdd(&G.cnt[C_ENTROPY], 1ull);
   if (ret == -3) atomicAdd(&G.cnt[C_FAIL], 1ull);
   if (fix) atomicAdd(&G.cnt[C_FIXUP], 1ull);
-  check_floors_mhd(G, pp, g);
+  check_floors_mhd(G, pp, g, G.rhofl_c ? G.rhofl_c[ix + G.ng] : -1.);
   p2u_full(G, pp, uu, g);
   store_cell(G.p, G.ncell, c, G.nv, pp);
   store_cell(G.u, G.ncell, c, G.nv, uu);
@@ -633,6 +748,7 @@ struct kgpu_ctx {
   std::vector<void *> allocs;
   double *stage;        // AoS staging for uploads / downloads
   int *fixmark;
+  double *rhofl_c = nullptr, *rhofl_f = nullptr;
   double min_dx, min_dy, min_dz;
   bool have_grid, have_metric;
   std::vector<double> hxb[3];
@@ -690,7 +806,7 @@ extern "C" int kgpu_default_config(kgpu_config *cfg, int nx, int ny, int nz) {
   cfg->int_order = KGPU_PPM;
   cfg->fluxmethod = KGPU_LAXF;
   cfg->axisym_metric = 0;
-  cfg->periodic[0] = cfg->periodic[1] = cfg->periodic[2] = 1;
+  cfg->bc[0] = cfg->bc[1] = cfg->bc[2] = KGPU_BC_PERIODIC;
   cfg->gamma = 5. / 3.;
   cfg->tsteplim = 0.5;
   cfg->rhofloor = 1.e-50;          // choices.h:319-329
@@ -723,6 +839,8 @@ static void fill_grid_params(Grid &G, const kgpu_config &c) {
   G.int_order = c.int_order; G.fluxmethod = c.fluxmethod;
   G.rhofloor = c.rhofloor; G.uurhoratiomin = c.uurhoratiomin; G.uurhoratiomax = c.uurhoratiomax;
   G.b2rhoratiomax = c.b2rhoratiomax; G.gammamaxhd = c.gammamaxhd; G.u2pconv = c.u2pconv;
+  for (int d = 0; d < 3; d++) G.bc[d] = c.bc[d];
+  G.rhofl_c = G.rhofl_f = nullptr;
 }
 
 static int check_config(const kgpu_config *c) {
@@ -742,7 +860,11 @@ extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
   *out = nullptr;
   int r = check_config(cfg);
   if (r) return r;
-  if (!(cfg->periodic[0] && cfg->periodic[1] && cfg->periodic[2])) return KGPU_EINVAL;
+  for (int d = 0; d < 3; d++)
+    if (cfg->bc[d] < KGPU_BC_PERIODIC || cfg->bc[d] > KGPU_BC_PERIODIC_COPY) return KGPU_EINVAL;
+  // the 2D corner fill follows the reference's periodic treatment only
+  if (cfg->nz == 1 && cfg->ny > 1 && (cfg->bc[0] != KGPU_BC_PERIODIC || cfg->bc[1] != KGPU_BC_PERIODIC))
+    return KGPU_EINVAL;
   kgpu_ctx *c = new kgpu_ctx();
   c->cfg = *cfg;
   fill_grid_params(c->G, *cfg);
@@ -902,6 +1024,30 @@ extern "C" int kgpu_upload_metric(kgpu_ctx *c, const double *g, const double *Gi
   return 0;
 }
 
+extern "C" int kgpu_set_density_floor(kgpu_ctx *c, const double *centres, const double *xfaces) {
+  if (!c) return KGPU_EINVAL;
+  Grid &G = c->G;
+  if (!centres || !xfaces) {
+    G.rhofl_c = G.rhofl_f = nullptr;
+    return 0;
+  }
+  if (!c->rhofl_c) {
+    void *p;
+    int r;
+    if ((r = dalloc(c, &p, G.sx * sizeof(double)))) return r;
+    c->rhofl_c = (double *)p;
+    if ((r = dalloc(c, &p, (G.sx + 1) * sizeof(double)))) return r;
+    c->rhofl_f = (double *)p;
+  }
+  CK(cudaMemcpyAsync(c->rhofl_c, centres, G.sx * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->rhofl_f, xfaces, (G.sx + 1) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  G.rhofl_c = c->rhofl_c;
+  G.rhofl_f = c->rhofl_f;
+  c->graph_ready = false;   // kernels take the Grid by value: re-capture
+  return 0;
+}
+
 extern "C" int kgpu_set_minkowski_metric(kgpu_ctx *c) {
   if (!c) return KGPU_EINVAL;
   Grid &G = c->G;
@@ -973,6 +1119,21 @@ static int launch_bc(kgpu_ctx *c) {
     LaunchScope ls(c, K_BC);
     k_bc_corners2d<<<1, 8 * G.ng > 32 ? 64 : 32, 0, c->stream>>>(G);
     CKL("k_bc_corners2d");
+  }
+  if (G.nz > 1 && G.ny > 1) {
+    // edges along z (a=x, b=y), along y (a=x, b=z), along x (a=y, b=z)
+    const int axes[3][3] = {{2, 0, 1}, {1, 0, 2}, {0, 1, 2}};
+    int n3[3] = {G.nx, G.ny, G.nz};
+    for (int k = 0; k < 3; k++) {
+      int cax = axes[k][0];
+      int nthreads = 4 * (n3[cax] + 2 * G.ng);
+      LaunchScope ls(c, K_BC);
+      k_bc_edges3d<<<nblocks(nthreads, 128), 128, 0, c->stream>>>(G, cax, axes[k][1], axes[k][2]);
+      CKL("k_bc_edges3d");
+    }
+    LaunchScope ls(c, K_BC);
+    k_bc_corners3d<<<nblocks(8 * G.ng * G.ng * G.ng, 128), 128, 0, c->stream>>>(G);
+    CKL("k_bc_corners3d");
   }
   return 0;
 }
@@ -1395,3 +1556,68 @@ extern "C" int kgpu_launch_count(kgpu_ctx *c, long long *out) {
 }
 
 extern "C" int kgpu_num_kernels(void) { return K_NKERNELS; }
+
+// ---------------------------------------------------------------------------
+// torus set-up on a context
+// ---------------------------------------------------------------------------
+extern "C" int kgpu_init_fm_torus(kgpu_ctx *c, const kgpu_torus_params *tp) {
+  if (!c || !tp) return KGPU_EINVAL;
+  const kgpu_config &k = c->cfg;
+  if (k.nz < 2 || k.ny < 2) return KGPU_EINVAL;
+  int r;
+  double lo[3] = {log(tp->r_lo - tp->r0), tp->x2_lo, 0.}, hi[3] = {log(tp->r_hi - tp->r0), tp->x2_hi, 2. * M_PI};
+  if ((r = kgpu_set_uniform_grid(c, lo, hi))) return r;
+  Grid &G = c->G;
+  std::vector<double> g(G.nmet * 20), Gi(G.nmet * 20), kr(G.nmet * 64);
+  std::vector<double> gb[3], Gb[3];
+  for (int d = 0; d < 3; d++) {
+    gb[d].resize(G.nfmet[d] * 20);
+    Gb[d].resize(G.nfmet[d] * 20);
+  }
+  if ((r = kgpu_mks2_metric_tables(tp->spin, tp->r0, tp->h0, k.nx, k.ny, k.nz, k.ng, k.axisym_metric,
+                                   c->hxb[0].data(), c->hxb[1].data(), c->hxb[2].data(), g.data(), Gi.data(),
+                                   kr.data(), gb[0].data(), gb[1].data(), gb[2].data(), Gb[0].data(), Gb[1].data(),
+                                   Gb[2].data())))
+    return r;
+  if ((r = kgpu_upload_metric(c, g.data(), Gi.data(), kr.data(), gb[0].data(), gb[1].data(), gb[2].data(),
+                              Gb[0].data(), Gb[1].data(), Gb[2].data())))
+    return r;
+  std::vector<double> fc(G.sx), ff(G.sx + 1);
+  if ((r = kgpu_fm_torus_floor(tp, k.nx, k.ng, c->hxb[0].data(), fc.data(), ff.data()))) return r;
+  if ((r = kgpu_set_density_floor(c, fc.data(), ff.data()))) return r;
+  std::vector<double> u(G.ncell * G.nv), p(G.ncell * G.nv);
+  if ((r = kgpu_fm_torus_state(tp, &k, c->hxb[0].data(), c->hxb[1].data(), c->hxb[2].data(), g.data(), Gi.data(),
+                               u.data(), p.data())))
+    return r;
+  if ((r = kgpu_upload_state(c, u.data(), p.data()))) return r;
+  if ((r = launch_bc(c))) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return kgpu_begin_run(c);
+}
+
+// ---------------------------------------------------------------------------
+// inspection of intermediate arrays (KORAL layout)
+// ---------------------------------------------------------------------------
+extern "C" int kgpu_download_flux(kgpu_ctx *c, int d, double *out) {
+  if (!c || !out || d < 0 || d > 2) return KGPU_EINVAL;
+  Grid &G = c->G;
+  const long nf = G.nface[d];
+  std::vector<double> h(nf * G.nv);
+  CK(cudaMemcpyAsync(h.data(), G.flb[d], nf * G.nv * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (long f = 0; f < nf; f++)
+    for (int iv = 0; iv < G.nv; iv++) out[f * G.nv + iv] = h[iv * nf + f];
+  return 0;
+}
+
+extern "C" int kgpu_download_emf(kgpu_ctx *c, double *out) {
+  if (!c || !out) return KGPU_EINVAL;
+  Grid &G = c->G;
+  const long ne = (long)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
+  std::vector<double> h(3 * ne);
+  CK(cudaMemcpyAsync(h.data(), G.emf, 3 * ne * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (long e = 0; e < ne; e++)
+    for (int k = 0; k < 3; k++) out[e * 3 + k] = h[k * ne + e];
+  return 0;
+}

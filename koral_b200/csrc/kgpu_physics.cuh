@@ -43,6 +43,8 @@ struct Grid {
   double *emf;                       // [3][(nx+1)(ny+1)(nz+1)]
   double *al[3], *ar[3];             // wavespeeds per cell and direction
   int *flag;                         // HD fixup request per cell
+  const double *rhofl_c, *rhofl_f;   // density floor per x-index (centres, x-faces), or null
+  int bc[3];                         // boundary kind per axis (KGPU_BC_*)
   double *scal;                      // device scalars (see ScalarSlot)
   unsigned long long *cnt;           // device counters
 };
@@ -71,9 +73,9 @@ KG_HD long face_index(const Grid &G, int ix, int iy, int iz, int d) {
 }
 KG_HD long facemet_index(const Grid &G, int ix, int iy, int iz, int d) {
   long kx = ix + G.ngcx, ky = (G.ny > 1 ? iy : 0) + G.ngcy;
-  long kz;
-  if (G.axisym) kz = (d == 2) ? (long)((G.nz > 1 ? iz : 0) + G.ngczmet) : 0;
-  else kz = (G.nz > 1 ? iz : 0) + G.ngcz;
+  // an axisymmetric metric keeps one phi plane for every face set
+  // (iZMET(iz) = 0 in get_gb, ko.h:125)
+  long kz = G.axisym ? 0 : (long)((G.nz > 1 ? iz : 0) + G.ngcz);
   if (d == 0) return kx + ky * (G.sx + 1) + kz * (long)G.sy * (G.sx + 1);
   if (d == 1) return kx + ky * G.sx + kz * (long)(G.sy + 1) * G.sx;
   return kx + ky * G.sx + kz * (long)G.sy * G.sx;
@@ -565,13 +567,18 @@ KG_HD int u2p(const Grid &G, const double *uu0, double *pp, const Geom &g, int &
 
 // density, internal-energy, magnetisation and Lorentz-factor floors
 // (check_floors_mhd, u2p.c:492-695, B2RHOFLOORFRAME = ZAMO)
-KG_HD int check_floors_mhd(const Grid &G, double *pp, const Geom &g) {
+KG_HD int check_floors_mhd(const Grid &G, double *pp, const Geom &g, double rhofloor_bh = -1.) {
   int ret = 0;
   const bool magn = G.nv > B3;
   double uu[NVMAX];
   p2u_full(G, pp, uu, g);
   if (pp[0] < G.rhofloor) {
     pp[0] = G.rhofloor;
+    ret = -1;
+  }
+  // radius-dependent floor (RHOFLOOR_BH, u2p.c:546-557), tabulated per x-index
+  if (rhofloor_bh > 0. && pp[0] < rhofloor_bh) {
+    pp[0] = rhofloor_bh;
     ret = -1;
   }
   if (pp[1] < G.uurhoratiomin * pp[0]) {

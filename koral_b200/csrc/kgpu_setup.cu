@@ -1,0 +1,429 @@
+// Host-side set-up of the Kerr torus problem: metric tables in modified
+// Kerr-Schild coordinates (MKS2) and Fishbone-Moncrief initial data.
+//
+// KORAL evaluates its MKS2 metric and connection from machine-generated
+// closed forms (metric.c:259-1640).  This file derives them independently:
+// the Kerr-Schild metric g_KS(r, theta) and its first derivatives are
+// written out analytically, the MKS2 metric follows from the diagonal
+// coordinate map r = exp(x1) + R0, theta = pi/2 (1 + cot(pi H0/2)
+// tan(pi H0 (x2 - 1/2))) by the chain rule, and the Christoffel symbols come
+// from the metric derivatives, Gamma^m_{nl} = g^{ms}(d_n g_{sl} + d_l g_{sn}
+// - d_s g_{nl})/2.  Afterwards the traces Gamma^m_{km} are corrected so that
+// they equal the finite-difference derivative of ln(sqrt(-g)) across the
+// cell, as calc_Krzysie_at_center does (metric.c:828-905), which keeps the
+// discrete update of a static metric exactly balanced.
+//
+// The tables use KORAL's layout (20 doubles of g_{mu nu}/d ln gdet/gdet per
+// point, 20 of g^{mu nu}/g_tt perturbation, 64 Christoffels) so they can be
+// compared with the reference's and uploaded through kgpu_upload_metric.
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <vector>
+
+#include "../../include/koral_b200.h"
+
+namespace {
+
+struct MKS2 {
+  double a, R0, H0;
+  // coordinate map and its first two derivatives
+  double r(double x1) const { return exp(x1) + R0; }
+  double drdx1(double x1) const { return exp(x1); }
+  double d2rdx1(double x1) const { return exp(x1); }
+  double th(double x2) const { return 0.5 * M_PI * (1. + tan(H0 * M_PI * (x2 - 0.5)) / tan(0.5 * M_PI * H0)); }
+  double dthdx2(double x2) const {
+    double c = cos(H0 * M_PI * (x2 - 0.5));
+    return 0.5 * M_PI * H0 * M_PI / (tan(0.5 * M_PI * H0) * c * c);
+  }
+  double d2thdx2(double x2) const {
+    double arg = H0 * M_PI * (x2 - 0.5);
+    double c = cos(arg);
+    return 0.5 * M_PI * (H0 * M_PI) * (H0 * M_PI) * 2. * tan(arg) / (tan(0.5 * M_PI * H0) * c * c);
+  }
+};
+
+// Kerr-Schild g_{mu nu}(r, theta) with its r- and theta-derivatives
+struct KSPoint {
+  double g[4][4], dgr[4][4], dgth[4][4], G[4][4];
+  double gdet;
+};
+
+void ks_point(double a, double r, double th, KSPoint &k) {
+  double s = sin(th), c = cos(th), s2 = s * s, a2 = a * a;
+  double Sig = r * r + a2 * c * c;
+  double dSr = 2. * r, dSth = -2. * a2 * c * s;
+  double q = 2. * r / Sig;
+  double dqr = 2. * (Sig - 2. * r * r) / (Sig * Sig);
+  double dqth = -2. * r * dSth / (Sig * Sig);
+  double ds2 = 2. * s * c;   // d(sin^2)/dtheta
+  memset(&k, 0, sizeof(k));
+  k.g[0][0] = -(1. - q);
+  k.g[0][1] = k.g[1][0] = q;
+  k.g[0][3] = k.g[3][0] = -a * s2 * q;
+  k.g[1][1] = 1. + q;
+  k.g[1][3] = k.g[3][1] = -a * s2 * (1. + q);
+  k.g[2][2] = Sig;
+  k.g[3][3] = s2 * (Sig + a2 * s2 * (1. + q));
+  k.dgr[0][0] = dqr;
+  k.dgr[0][1] = k.dgr[1][0] = dqr;
+  k.dgr[0][3] = k.dgr[3][0] = -a * s2 * dqr;
+  k.dgr[1][1] = dqr;
+  k.dgr[1][3] = k.dgr[3][1] = -a * s2 * dqr;
+  k.dgr[2][2] = dSr;
+  k.dgr[3][3] = s2 * (dSr + a2 * s2 * dqr);
+  k.dgth[0][0] = dqth;
+  k.dgth[0][1] = k.dgth[1][0] = dqth;
+  k.dgth[0][3] = k.dgth[3][0] = -a * (ds2 * q + s2 * dqth);
+  k.dgth[1][1] = dqth;
+  k.dgth[1][3] = k.dgth[3][1] = -a * (ds2 * (1. + q) + s2 * dqth);
+  k.dgth[2][2] = dSth;
+  k.dgth[3][3] = ds2 * (Sig + a2 * s2 * (1. + q)) + s2 * (dSth + a2 * (ds2 * (1. + q) + s2 * dqth));
+  double Del = r * r - 2. * r + a2;
+  k.G[0][0] = -(1. + q);
+  k.G[0][1] = k.G[1][0] = q;
+  k.G[1][1] = Del / Sig;
+  k.G[1][3] = k.G[3][1] = a / Sig;
+  k.G[2][2] = 1. / Sig;
+  k.G[3][3] = 1. / (Sig * s2);
+  k.gdet = Sig * fabs(s);   // sqrt(-g) > 0 also beyond the pole (theta < 0 or > pi)
+}
+
+// metric of one MKS2 point: the 20-double g and G entries of KORAL's table
+// and the (uncorrected) Christoffels
+void mks2_point(const MKS2 &m, double x1, double x2, double *g20, double *G20, double Kr[4][4][4], double &gdet) {
+  double r = m.r(x1), th = m.th(x2);
+  KSPoint k;
+  ks_point(m.a, r, th, k);
+  double J[4] = {1., m.drdx1(x1), m.dthdx2(x2), 1.};
+  double dJ1 = m.d2rdx1(x1), dJ2 = m.d2thdx2(x2);
+  double g[4][4], Gi[4][4], dg[4][4][4];   // dg[l][i][j] = d_l g_ij (MKS2)
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      g[i][j] = k.g[i][j] * J[i] * J[j];
+      Gi[i][j] = k.G[i][j] / (J[i] * J[j]);
+      dg[0][i][j] = dg[3][i][j] = 0.;
+      double dJJ1 = (i == 1 ? dJ1 * J[j] : 0.) + (j == 1 ? J[i] * dJ1 : 0.);
+      double dJJ2 = (i == 2 ? dJ2 * J[j] : 0.) + (j == 2 ? J[i] * dJ2 : 0.);
+      dg[1][i][j] = k.dgr[i][j] * J[1] * J[i] * J[j] + k.g[i][j] * dJJ1;
+      dg[2][i][j] = k.dgth[i][j] * J[2] * J[i] * J[j] + k.g[i][j] * dJJ2;
+    }
+  gdet = k.gdet * J[1] * J[2];
+  for (int mu = 0; mu < 4; mu++)
+    for (int n = 0; n < 4; n++)
+      for (int l = 0; l < 4; l++) {
+        double sum = 0.;
+        for (int s = 0; s < 4; s++) sum += Gi[mu][s] * (dg[n][s][l] + dg[l][s][n] - dg[s][n][l]);
+        Kr[mu][n][l] = 0.5 * sum;
+      }
+  // d ln gdet / dx^i (KORAL stores these in g[i][4], i < 3)
+  double s = sin(th), c = cos(th), Sig = r * r + m.a * m.a * c * c;
+  double dl1 = (2. * r / Sig) * J[1] + dJ1 / J[1];
+  double dl2 = (-2. * m.a * m.a * c * s / Sig + c / s) * J[2] + dJ2 / J[2];
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 5; j++) {
+      g20[i * 5 + j] = j < 4 ? g[i][j] : 0.;
+      G20[i * 5 + j] = j < 4 ? Gi[i][j] : 0.;
+    }
+  g20[0 * 5 + 4] = dl1;
+  g20[1 * 5 + 4] = dl2;
+  g20[2 * 5 + 4] = 0.;
+  g20[3 * 5 + 4] = gdet;
+  G20[3 * 5 + 4] = 2. * r / Sig;   // g_tt + 1 in Kerr-Schild time
+}
+
+double gdet_at(const MKS2 &m, double x1, double x2) {
+  double r = m.r(x1), th = m.th(x2), c = cos(th);
+  return (r * r + m.a * m.a * c * c) * fabs(sin(th)) * m.drdx1(x1) * m.dthdx2(x2);
+}
+
+}  // namespace
+
+extern "C" int kgpu_mks2_metric_tables(double a, double R0, double H0, int nx, int ny, int nz, int ng, int axisym,
+                                       const double *xbx, const double *xby, const double *xbz, double *g,
+                                       double *G, double *gKr, double *gbx, double *gby, double *gbz, double *Gbx,
+                                       double *Gby, double *Gbz) {
+  if (!xbx || !xby || !xbz || !g || !G || !gKr || !gbx || !gby || !gbz || !Gbx || !Gby || !Gbz) return KGPU_EINVAL;
+  if (nx < 1 || ny < 1 || nz < 1 || ng < 1) return KGPU_EINVAL;
+  MKS2 m{a, R0, H0};
+  const int sx = nx + 2 * ng, sy = ny > 1 ? ny + 2 * ng : 1, sz = nz > 1 ? nz + 2 * ng : 1;
+  const int ngy = ny > 1 ? ng : 0, ngz = nz > 1 ? ng : 0;
+  const int szm = axisym ? 1 : sz, ngzm = axisym ? 0 : ngz;
+  auto xc = [&](const double *xb, int i) { return .5 * (xb[i + 1 + ng] + xb[i + ng]); };
+  auto xf = [&](const double *xb, int i) { return xb[i + ng]; };
+  double Kr[4][4][4], gd;
+  for (int kz = 0; kz < szm; kz++)
+    for (int ky = 0; ky < sy; ky++)
+      for (int kx = 0; kx < sx; kx++) {
+        int ix = kx - ng, iy = ky - ngy;
+        double x1 = xc(xbx, ix), x2 = xc(xby, iy);
+        long pt = kx + (long)ky * sx + (long)kz * sx * sy;
+        mks2_point(m, x1, x2, g + pt * 20, G + pt * 20, Kr, gd);
+        // flux-consistent traces (calc_Krzysie_at_center, metric.c:828-905)
+        const double *xbs[3] = {xbx, xby, xbz};
+        int ic[3] = {ix, iy, kz - ngzm};
+        for (int kap = 1; kap <= 3; kap++) {
+          double Ck = Kr[0][kap][0] + Kr[1][kap][1] + Kr[2][kap][2] + Kr[3][kap][3];
+          double Sk = 1.e-300 + fabs(Kr[0][kap][0]) + fabs(Kr[1][kap][1]) + fabs(Kr[2][kap][2]) + fabs(Kr[3][kap][3]);
+          double W[4];
+          for (int mu = 0; mu < 4; mu++) W[mu] = fabs(Kr[mu][kap][mu]) / Sk;
+          double g0 = gdet_at(m, x1, x2), gu, gl, dxk;
+          const double *xbk = xbs[kap - 1];
+          int i = ic[kap - 1];
+          if (kap == 1) { gu = gdet_at(m, xf(xbx, ix + 1), x2); gl = gdet_at(m, xf(xbx, ix), x2); }
+          else if (kap == 2) { gu = gdet_at(m, x1, xf(xby, iy + 1)); gl = gdet_at(m, x1, xf(xby, iy)); }
+          else { gu = g0; gl = g0; }
+          dxk = xbk[i + 1 + ng] - xbk[i + ng];
+          double D = (gu - gl) / (dxk * g0);
+          for (int mu = 0; mu < 4; mu++) {
+            Kr[mu][kap][mu] += (D - Ck) * W[mu];
+            Kr[mu][mu][kap] = Kr[mu][kap][mu];
+          }
+        }
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j < 4; j++)
+            for (int k = 0; k < 4; k++) gKr[pt * 64 + i * 16 + j * 4 + k] = Kr[i][j][k];
+        // faces
+        long fx = kx + (long)ky * (sx + 1) + (long)kz * sy * (sx + 1);
+        mks2_point(m, xf(xbx, ix), x2, gbx + fx * 20, Gbx + fx * 20, Kr, gd);
+        if (kx == sx - 1) {
+          long fx1 = fx + 1;
+          mks2_point(m, xf(xbx, ix + 1), x2, gbx + fx1 * 20, Gbx + fx1 * 20, Kr, gd);
+        }
+        long fy = kx + (long)ky * sx + (long)kz * (sy + 1) * sx;
+        mks2_point(m, x1, xf(xby, iy), gby + fy * 20, Gby + fy * 20, Kr, gd);
+        if (ky == sy - 1) {
+          long fy1 = fy + sx;
+          mks2_point(m, x1, xf(xby, iy + 1), gby + fy1 * 20, Gby + fy1 * 20, Kr, gd);
+        }
+        long fz = kx + (long)ky * sx + (long)kz * sy * sx;
+        mks2_point(m, x1, x2, gbz + fz * 20, Gbz + fz * 20, Kr, gd);
+        if (kz == szm - 1) {
+          long fz1 = fz + (long)sx * sy;
+          mks2_point(m, x1, x2, gbz + fz1 * 20, Gbz + fz1 * 20, Kr, gd);
+        }
+      }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Fishbone & Moncrief (1976) torus: constant specific angular momentum l,
+// enthalpy from the first integral of hydrostatic equilibrium in Kerr
+// (Boyer-Lindquist, M = 1).  Same construction as the KORAL plug-in used by
+// the oracle (oracle/ref/problems/FMTORUS).
+// ---------------------------------------------------------------------------
+#include "kgpu_physics.cuh"
+
+namespace {
+
+double fm_lfish(double a, double r) {
+  double sr = sqrt(r);
+  double x = r * r - 2. * a * sr + a * a;
+  double num = x * ((-2. * a * r * x) / sqrt(2. * a * sr + (-3. + r) * r) +
+                    ((a + (-2. + r) * sr) * (r * r * r + a * a * (2. + r))) / sqrt(1. + (2. * a) / (r * sr) - 3. / r));
+  double den = r * r * r * sqrt(2. * a * sr + (-3. + r) * r) * (a * a + (-2. + r) * r);
+  return num / den;
+}
+double fm_lnh_raw(double a, double l, double r, double th) {
+  double sth = sin(th), cth = cos(th);
+  double Sigma = r * r + a * a * cth * cth;
+  double Delta = r * r - 2. * r + a * a;
+  double A = (r * r + a * a) * (r * r + a * a) - Delta * a * a * sth * sth;
+  double q = sqrt(1. + 4. * l * l * Sigma * Sigma * Delta / (A * A * sth * sth));
+  return 0.5 * log((1. + q) / (Sigma * Delta / A)) - 0.5 * q - 2. * a * r * l / A;
+}
+double fm_uphi(double a, double l, double r, double th) {
+  double sth = sin(th), cth = cos(th);
+  double Sigma = r * r + a * a * cth * cth;
+  double Delta = r * r - 2. * r + a * a;
+  double A = (r * r + a * a) * (r * r + a * a) - Delta * a * a * sth * sth;
+  double e2 = Sigma * Sigma * Delta / (A * A * sth * sth);
+  double up1 = sqrt((-1. + sqrt(1. + 4. * l * l * e2)) / 2.);
+  return 2. * a * r * sqrt(1. + up1 * up1) / sqrt(A * Sigma * Delta) + sqrt(Sigma / A) * up1 / sth;
+}
+double fm_noise(unsigned long long seed, unsigned long long idx) {
+  unsigned long long z = seed + 0x9E3779B97F4A7C15ULL * (idx + 1ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  z = z ^ (z >> 31);
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+}  // namespace
+
+// Primitive and conserved arrays (KORAL layout, whole padded grid) of the
+// magnetised torus.  g and G are the centre tables of kgpu_mks2_metric_tables
+// for the same grid.  Ghost cells are left zero: the caller applies the
+// boundary conditions (kgpu_set_bc) after uploading.
+extern "C" int kgpu_fm_torus_state(const kgpu_torus_params *tp, const kgpu_config *cfg, const double *xbx,
+                                   const double *xby, const double *xbz, const double *g, const double *G, double *u,
+                                   double *p) {
+  using namespace kgpu;
+  if (!tp || !cfg || !xbx || !xby || !xbz || !g || !G || !u || !p) return KGPU_EINVAL;
+  const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, ng = cfg->ng, nv = cfg->nv;
+  if (nv != 9 || ny < 2 || nz < 2) return KGPU_EINVAL;
+  Grid Gr;
+  memset(&Gr, 0, sizeof(Gr));
+  Gr.nx = nx; Gr.ny = ny; Gr.nz = nz; Gr.ng = ng; Gr.nv = nv;
+  Gr.sx = nx + 2 * ng; Gr.sy = ny + 2 * ng; Gr.sz = nz + 2 * ng;
+  Gr.ngcx = Gr.ngcy = Gr.ngcz = ng;
+  Gr.axisym = cfg->axisym_metric; Gr.ngczmet = Gr.axisym ? 0 : ng;
+  Gr.gamma = cfg->gamma;
+  const double GAM = cfg->gamma, a = tp->spin;
+  MKS2 m{a, tp->r0, tp->h0};
+  const long ncell = (long)Gr.sx * Gr.sy * Gr.sz;
+  for (long i = 0; i < ncell * nv; i++) u[i] = p[i] = 0.;
+  auto geom_at = [&](int ix, int iy, int iz, Geom &gm) {
+    long pt = met_index(Gr, ix, iy, iz);
+    for (int i = 0; i < 4; i++)
+      for (int j = 0; j < 5; j++) {
+        gm.gg[i][j] = g[pt * 20 + i * 5 + j];
+        gm.GG[i][j] = G[pt * 20 + i * 5 + j];
+      }
+    gm.gdet = gm.gg[3][4];
+    gm.gttpert = gm.GG[3][4];
+  };
+  auto xc = [&](const double *xb, int i) { return .5 * (xb[i + 1 + ng] + xb[i + ng]); };
+  const double l = fm_lfish(a, tp->rmax);
+  const double lnh0 = fm_lnh_raw(a, l, tp->rin, M_PI / 2.);
+  const double lnhmax = fm_lnh_raw(a, l, tp->rmax, M_PI / 2.) - lnh0;
+  const double rhomax = pow((exp(lnhmax) - 1.) * (GAM - 1.) / (tp->kappa * GAM), 1. / (GAM - 1.));
+  // vector potential A_phi at cell centres, with the ghost layers the
+  // torus boundaries give it (radial copy, theta mirror, periodic phi)
+  std::vector<double> Aphi(ncell, 0.);
+  for (int iz = 0; iz < nz; iz++)
+    for (int iy = 0; iy < ny; iy++)
+      for (int ix = 0; ix < nx; ix++) {
+        double x1 = xc(xbx, ix), x2 = xc(xby, iy);
+        double r = m.r(x1), th = m.th(x2);
+        double pp[NVMAX], uu[NVMAX];
+        double rhoatm = tp->atm_rho0 * pow(r, -1.5), uuatm = tp->atm_uu0 * pow(r, -2.5);
+        pp[RHO] = rhoatm;
+        pp[UU] = uuatm;
+        pp[VX] = pp[VY] = pp[VZ] = 0.;
+        pp[B1] = pp[B2] = pp[B3] = 0.;
+        Geom gm;
+        geom_at(ix, iy, iz, gm);
+        double lnh = fm_lnh_raw(a, l, r, th) - lnh0;
+        if (lnh > 0. && r >= tp->rin) {
+          double h = exp(lnh);
+          double rho = pow((h - 1.) * (GAM - 1.) / (tp->kappa * GAM), 1. / (GAM - 1.)) / rhomax;
+          double ui = tp->kappa * pow(rho * rhomax, GAM) / (GAM - 1.) / rhomax;
+          unsigned long long idx = (unsigned long long)ix + (unsigned long long)nx * ((unsigned long long)iy + (unsigned long long)ny * (unsigned long long)iz);
+          ui *= 1. + tp->noise * (2. * fm_noise(tp->seed, idx) - 1.);
+          // Boyer-Lindquist u^phi with u^r = u^theta = 0: the Kerr-Schild and
+          // MKS2 components equal the BL ones, u^t from the normalisation in
+          // the MKS2 metric; then the relative four-velocity
+          double uph = fm_uphi(a, l, r, th);
+          double A2 = gm.gg[0][0], B2 = 2. * gm.gg[0][3] * uph, C2 = gm.gg[3][3] * uph * uph + 1.;
+          double ut = (-B2 - sqrt(B2 * B2 - 4. * A2 * C2)) / (2. * A2);
+          if (ut < 0.) ut = (-B2 + sqrt(B2 * B2 - 4. * A2 * C2)) / (2. * A2);
+          double ucon[4] = {ut, 0., 0., uph};
+          double v[4];
+          for (int i = 1; i < 4; i++) v[i] = ucon[i] - ucon[0] * gm.GG[0][i] / gm.GG[0][0];
+          pp[RHO] = rho > rhoatm ? rho : rhoatm;
+          pp[UU] = ui > uuatm ? ui : uuatm;
+          pp[VX] = v[1]; pp[VY] = v[2]; pp[VZ] = v[3];
+          Aphi[cell_index(Gr, ix, iy, iz)] = rho - 0.2 > 0. ? rho - 0.2 : 0.;
+        }
+        pp[ENTR] = calc_Sfromu(GAM, pp[RHO], pp[UU]);
+        p2u_full(Gr, pp, uu, gm);
+        long c = cell_index(Gr, ix, iy, iz);
+        for (int iv = 0; iv < nv; iv++) {
+          p[c * nv + iv] = pp[iv];
+          u[c * nv + iv] = uu[iv];
+        }
+      }
+  auto A = [&](int ix, int iy, int iz) {
+    if (ix < 0) ix = 0;
+    if (ix > nx - 1) ix = nx - 1;
+    if (iy < 0) iy = -iy - 1;
+    if (iy > ny - 1) iy = 2 * ny - iy - 1;
+    if (iz < 0) iz += nz;
+    if (iz > nz - 1) iz -= nz;
+    return Aphi[cell_index(Gr, ix, iy, iz)];
+  };
+  // corner values (mean of the eight cells around a corner) and the curl
+  // with one-sided corner differences (calc_BfromA, magn.c:380-586)
+  auto Ac = [&](int ix, int iy, int iz) {
+    return 1. / 8. * (A(ix, iy, iz) + A(ix, iy - 1, iz) + A(ix - 1, iy, iz) + A(ix - 1, iy - 1, iz) + A(ix, iy, iz - 1) +
+                      A(ix, iy - 1, iz - 1) + A(ix - 1, iy, iz - 1) + A(ix - 1, iy - 1, iz - 1));
+  };
+  double maxbeta = 0.;
+  for (int iz = 0; iz < nz; iz++)
+    for (int iy = 0; iy < ny; iy++)
+      for (int ix = 0; ix < nx; ix++) {
+        double dx = xbx[ix + 1 + ng] - xbx[ix + ng], dy = xby[iy + 1 + ng] - xby[iy + ng];
+        double dA32 = (Ac(ix, iy + 1, iz) - Ac(ix, iy, iz) + Ac(ix + 1, iy + 1, iz) - Ac(ix + 1, iy, iz) +
+                       Ac(ix, iy + 1, iz + 1) - Ac(ix, iy, iz + 1) + Ac(ix + 1, iy + 1, iz + 1) - Ac(ix + 1, iy, iz + 1)) /
+                      (4. * dy);
+        double dA31 = (Ac(ix + 1, iy, iz) - Ac(ix, iy, iz) + Ac(ix + 1, iy + 1, iz) - Ac(ix, iy + 1, iz) +
+                       Ac(ix + 1, iy, iz + 1) - Ac(ix, iy, iz + 1) + Ac(ix + 1, iy + 1, iz + 1) - Ac(ix, iy + 1, iz + 1)) /
+                      (4. * dx);
+        Geom gm;
+        geom_at(ix, iy, iz, gm);
+        long c = cell_index(Gr, ix, iy, iz);
+        double *pp = p + c * nv;
+        pp[B1] = (0. - dA32) / gm.gdet;
+        pp[B2] = (dA31 - 0.) / gm.gdet;
+        pp[B3] = 0.;
+        Kin k;
+        kinematics(pp, gm, true, k);
+        double pmag = k.bsq / 2., pgas = (GAM - 1.) * pp[UU];
+        if (pmag / pgas > maxbeta) maxbeta = pmag / pgas;
+      }
+  const double fac = maxbeta > 0. ? sqrt(tp->maxbeta / maxbeta) : 0.;
+  for (int iz = 0; iz < nz; iz++)
+    for (int iy = 0; iy < ny; iy++)
+      for (int ix = 0; ix < nx; ix++) {
+        long c = cell_index(Gr, ix, iy, iz);
+        double *pp = p + c * nv;
+        pp[B1] *= fac;
+        pp[B2] *= fac;
+        pp[B3] *= fac;
+        Geom gm;
+        geom_at(ix, iy, iz, gm);
+        p2u_full(Gr, pp, u + c * nv, gm);
+      }
+  return 0;
+}
+
+// Density floor rho >= atm_rho0 * r^-1.5 tabulated per x-index at cell
+// centres and x-faces (the form of RHOFLOOR_BH, u2p.c:546-557).
+extern "C" int kgpu_fm_torus_floor(const kgpu_torus_params *tp, int nx, int ng, const double *xbx, double *centres,
+                                   double *xfaces) {
+  if (!tp || !xbx || !centres || !xfaces) return KGPU_EINVAL;
+  MKS2 m{tp->spin, tp->r0, tp->h0};
+  double rh = 1. + sqrt(1 - tp->spin * tp->spin);
+  double norm = tp->atm_rho0 / pow(rh, 1.5);
+  for (int ix = -ng; ix < nx + ng; ix++) {
+    double rr = m.r(.5 * (xbx[ix + 1 + ng] + xbx[ix + ng])) / rh;
+    centres[ix + ng] = norm / sqrt(rr * rr * rr);
+  }
+  for (int ix = -ng; ix <= nx + ng; ix++) {
+    double rr = m.r(xbx[ix + ng]) / rh;
+    xfaces[ix + ng] = norm / sqrt(rr * rr * rr);
+  }
+  return 0;
+}
+
+extern "C" int kgpu_default_torus_params(kgpu_torus_params *tp) {
+  if (!tp) return KGPU_EINVAL;
+  tp->spin = 0.9;
+  tp->r0 = 0.;
+  tp->h0 = 0.6;
+  tp->r_lo = 1.8;
+  tp->r_hi = 1000.;
+  tp->x2_lo = 0.005;
+  tp->x2_hi = 0.995;
+  tp->rin = 6.;
+  tp->rmax = 12.;
+  tp->kappa = 1.e-3;
+  tp->noise = 0.02;
+  tp->seed = 12345ULL;
+  tp->atm_rho0 = 1.e-4;
+  tp->atm_uu0 = 1.e-6;
+  tp->maxbeta = 0.01;
+  return 0;
+}

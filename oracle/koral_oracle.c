@@ -51,7 +51,7 @@ static long ko_face(const ko_grid *G, int ix, int iy, int iz, int idim)
 static long ko_facemet(const ko_grid *G, int ix, int iy, int iz, int idim)
 {
   long kx = ix + G->ngcx, ky = ko_iy(G, iy) + G->ngcy;
-  long kz = (G->axisym ? (idim == 2 ? (long)(ko_iz(G, iz) + G->ngczmet) : 0) : (long)(ko_iz(G, iz) + G->ngcz));
+  long kz = G->axisym ? 0 : (long)(ko_iz(G, iz) + G->ngcz);   /* iZMET(iz) = 0 when axisymmetric (ko.h:125) */
   if (idim == 0) return kx + ky * (G->sx + 1) + kz * G->sy * (G->sx + 1);
   if (idim == 1) return kx + ky * G->sx + kz * (G->sy + 1) * G->sx;
   return kx + ky * G->sx + kz * G->sy * G->sx;

@@ -172,5 +172,39 @@ class RefKoral:
     def scalar(self, name):
         return ctypes.c_double.in_dll(self.L, name).value
 
+    def physics(self):
+        out = (ctypes.c_double * 16)()
+        self.L.kref_physics(out)
+        keys = ("gamma", "tsteplim", "rhofloor", "uurhoratiomin", "uurhoratiomax", "b2rhoratiomax",
+                "gammamaxhd", "u2pconv", "spin", "axisym")
+        return dict(zip(keys, out[:10]))
+
+    def grid_faces(self):
+        """Cell-face coordinates per axis, xb[ic+NG] for ic in [-NG, N+NG]."""
+        n = (self.nx, self.ny, self.nz)
+        tot = sum(k + 1 + 2 * self.ng for k in n)
+        xb = np.ctypeslib.as_array(_dp.in_dll(self.L, "xb"), shape=(tot,)).copy()
+        out, o = [], 0
+        for k in n:
+            out.append(xb[o:o + k + 1 + 2 * self.ng])
+            o += k + 1 + 2 * self.ng
+        return out
+
+    def metric_tables(self):
+        """(g, G, gKr, gbx, gby, gbz, Gbx, Gby, Gbz) in KORAL layout."""
+        sx, sy, sm = self.sx, self.sy, self.szmet
+        sizes = dict(g=sx * sy * sm * 20, G=sx * sy * sm * 20, gKr=sx * sy * sm * 64,
+                     gbx=(sx + 1) * sy * sm * 20, Gbx=(sx + 1) * sy * sm * 20,
+                     gby=sx * (sy + 1) * sm * 20, Gby=sx * (sy + 1) * sm * 20,
+                     gbz=sx * sy * (sm + 1) * 20, Gbz=sx * sy * (sm + 1) * 20)
+        return tuple(np.ctypeslib.as_array(_dp.in_dll(self.L, k), shape=(sizes[k],)).copy()
+                     for k in ("g", "G", "gKr", "gbx", "gby", "gbz", "Gbx", "Gby", "Gbz"))
+
+    def rhofloor_table(self):
+        c = np.zeros(self.sx)
+        f = np.zeros(self.sx + 1)
+        ok = self.L.kref_rhofloor_table(c.ctypes.data_as(_dp), f.ctypes.data_as(_dp))
+        return (c, f) if ok else (None, None)
+
     def set_scalar(self, name, v):
         ctypes.c_double.in_dll(self.L, name).value = v

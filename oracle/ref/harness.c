@@ -214,3 +214,49 @@ int kref_nsteps(int n)
     r = kref_step();
   return r;
 }
+
+/* The radius-dependent density floor of check_floors_mhd (u2p.c:546-557)
+ * evaluated exactly as there, at cell centres (SX values) and x-faces
+ * (SX+1 values) of the x axis.  Returns 0 when the build has no such floor. */
+int kref_rhofloor_table(double *centres, double *xfaces)
+{
+#ifdef RHOFLOOR_BH
+  int ix;
+  for (ix = -NG; ix < NX + NG; ix++) {
+    ldouble xx[4] = {0., get_x(ix, 0), get_x(0, 1), get_x(0, 2)}, xxBL[4];
+    coco_N(xx, xxBL, MYCOORDS, BLCOORDS);
+    ldouble rr = xxBL[1] / rhorizonBL;
+    centres[ix + NG] = RHOFLOOR_BH_NORM / sqrt(rr * rr * rr);
+  }
+  for (ix = -NG; ix <= NX + NG; ix++) {
+    ldouble xx[4] = {0., get_xb(ix, 0), get_x(0, 1), get_x(0, 2)}, xxBL[4];
+    coco_N(xx, xxBL, MYCOORDS, BLCOORDS);
+    ldouble rr = xxBL[1] / rhorizonBL;
+    xfaces[ix + NG] = RHOFLOOR_BH_NORM / sqrt(rr * rr * rr);
+  }
+  return 1;
+#else
+  (void)centres; (void)xfaces;
+  return 0;
+#endif
+}
+
+/* Physics constants of this build needed to configure the GPU path. */
+int kref_physics(double *out)
+{
+  out[0] = GAMMA;
+  out[1] = TSTEPLIM;
+  out[2] = RHOFLOOR;
+  out[3] = UURHORATIOMIN;
+  out[4] = UURHORATIOMAX;
+  out[5] = B2RHORATIOMAX;
+  out[6] = GAMMAMAXHD;
+  out[7] = U2PCONV;
+  out[8] = BHSPIN;
+#ifdef METRICAXISYMMETRIC
+  out[9] = 1.;
+#else
+  out[9] = 0.;
+#endif
+  return 10;
+}

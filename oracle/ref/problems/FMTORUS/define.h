@@ -1,0 +1,68 @@
+/* 3D magnetised Kerr torus (KORAL plug-in format).
+ * Spin 0.9, MKS2 coordinates (r = exp(x1)+R0, theta concentrated towards
+ * the midplane by H0), r in [1.8, 1000] log-spaced, x2 in [0.005, 0.995]
+ * (theta just off the poles), phi in [0, 2 pi].  Fishbone-Moncrief torus
+ * with r_in = 6, r_max = 12, Gamma = 13/9, one poloidal loop from
+ * A_phi = max(rho/rho_max - 0.2, 0) normalised to beta_min = 100, 2% seeded
+ * pressure noise, density floor 1e-4 r^-1.5.  MP5 + HLL + flux-CT, RK2.
+ * The grid may be overridden with -DTNX/-DTNY/-DTNZ for small parity builds. */
+#define MYCOORDS MKS2COORDS
+#define MKSR0 0.
+#define MKSH0 0.6
+#define METRICAXISYMMETRIC
+#define BHSPIN 0.9
+#define MASS 10.
+
+#define MAGNFIELD
+#define VECPOTGIVEN
+#define TORUS_MAXBETA 0.01        /* max pmag/pgas, i.e. beta_min = 100 */
+
+#define INT_ORDER 4
+#define FLUXMETHOD HLL_FLUX
+#define TIMESTEPPING RK2
+#define TSTEPLIM 0.5
+#define FLUXLIMITER 0
+#define MINMOD_THETA 1.5
+#define GAMMA (13./9.)
+
+#define TORUS_RIN 6.
+#define TORUS_RMAX 12.
+#define TORUS_KAPPA 1.e-3
+#define TORUS_NOISE 0.02
+#define TORUS_SEED 12345ULL
+
+/* floors: rho >= 1e-4 r^-1.5 via the reference's BH floor (u2p.c:546-557),
+ * whose argument is r/r_horizon */
+#define RHOFLOOR_BH
+#define RHOFLOOR_BH_NORM (1.e-4 / pow(rhorizonBL, 1.5))
+#define UURHORATIOMIN 1.e-10
+#define UURHORATIOMAX 1.e2
+#define B2RHORATIOMAX 100.
+#define ATM_RHO0 1.e-4
+#define ATM_UU0 1.e-6
+
+#define MINX (log(1.8 - MKSR0))
+#define MAXX (log(1000. - MKSR0))
+#define MINY 0.005
+#define MAXY 0.995
+#define MINZ 0.
+#define MAXZ (2. * M_PI)
+#ifndef TNX
+#define TNX 192
+#endif
+#ifndef TNY
+#define TNY 96
+#endif
+#ifndef TNZ
+#define TNZ 64
+#endif
+#define SPECIFIC_BC
+
+#define NOUTSTOP 1e50
+#define DTOUT1 1.e50
+#define DTOUT2 1.e50
+#define SILOOUTPUT 0
+#define OUTOUTPUT 0
+#define AVGOUTPUT 0
+#define SCAOUTPUT 0
+#define RADOUTPUT 0
