@@ -200,6 +200,26 @@ int kgpu_u2p_cells(int n, const kgpu_config *cfg, const double *uu, double *pp,
 int kgpu_p2u_cells(int n, const kgpu_config *cfg, const double *pp, double *uu,
                    const double *g, const double *G);
 
+/* kgpu_u2p_cells without any memory allocation.  No counterpart in the
+ * reference: it exists for callers that cannot allocate when they invert
+ * cells (device memory owned by another allocator or pool, a region where
+ * cudaMalloc's implicit device synchronisation would stall other streams, a
+ * long-running service that must not grow the device heap).  Same arguments,
+ * layout and results as kgpu_u2p_cells; staging goes through one file-scope
+ * device array of KGPU_STATIC_MAX_CELLS cells (about 3.9 MB per device).
+ *  - n > KGPU_STATIC_MAX_CELLS returns KGPU_EINVAL; split larger batches.
+ *  - The first call on a device (that device current) looks up the array's
+ *    address with cudaGetSymbolAddress; make it before any stream capture.
+ *  - All calls share the array and it keeps the last call's contents; calls
+ *    that overlap on the GPU race on it and must be serialised by the caller.
+ *  - Copies and the kernel run on the legacy default stream and the call
+ *    returns when the results are on the host.
+ * Errors are described by kgpu_u2p_cells_static_error(). */
+#define KGPU_STATIC_MAX_CELLS 8192
+int kgpu_u2p_cells_static(int n, const kgpu_config *cfg, const double *uu, double *pp,
+                          const double *g, const double *G, int *status, int *fixup);
+const char *kgpu_u2p_cells_static_error(void);
+
 /* Instrumentation. ------------------------------------------------------- */
 /* The context's CUDA stream (cudaStream_t), for events and copies that must
  * be ordered with the operators. */

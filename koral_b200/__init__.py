@@ -118,6 +118,9 @@ def lib():
         L.kgpu_profile_reset.argtypes = [vp]
         L.kgpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
         L.kgpu_last_error.restype = ctypes.c_char_p
+        L.kgpu_u2p_cells_static.argtypes = sig["kgpu_u2p_cells"]
+        L.kgpu_u2p_cells_static.restype = ctypes.c_int
+        L.kgpu_u2p_cells_static_error.restype = ctypes.c_char_p
         L.kgpu_abi_version.restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -349,6 +352,30 @@ def u2p_cells(cfg, uu, pp, g, G):
     ip = ctypes.POINTER(ctypes.c_int)
     _check(lib().kgpu_u2p_cells(n, ctypes.byref(cfg), _ptr(uu), _ptr(pp), _ptr(g), _ptr(G),
                                 st.ctypes.data_as(ip), fx.ctypes.data_as(ip)), "kgpu_u2p_cells")
+    return pp, st, fx
+
+
+STATIC_MAX_CELLS = 8192   # KGPU_STATIC_MAX_CELLS
+
+
+def u2p_cells_static(cfg, uu, pp, g, G):
+    """u2p_cells through kgpu_u2p_cells_static, which allocates no device
+    memory: at most STATIC_MAX_CELLS cells per call, calls share one device
+    array and must not overlap on the GPU."""
+    uu = np.ascontiguousarray(uu, dtype=np.float64)
+    pp = np.ascontiguousarray(pp, dtype=np.float64).copy()
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    n = uu.shape[0]
+    st = np.zeros(n, dtype=np.int32)
+    fx = np.zeros(n, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    L = lib()
+    rc = L.kgpu_u2p_cells_static(n, ctypes.byref(cfg), _ptr(uu), _ptr(pp), _ptr(g), _ptr(G),
+                                 st.ctypes.data_as(ip), fx.ctypes.data_as(ip))
+    if rc != 0:
+        msg = L.kgpu_u2p_cells_static_error().decode(errors="replace")
+        raise KgpuError(f"kgpu_u2p_cells_static failed with code {rc}: {msg}")
     return pp, st, fx
 
 
