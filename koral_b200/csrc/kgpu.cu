@@ -77,11 +77,14 @@ __device__ inline bool outside_gc(const Grid &G, int ix, int iy, int iz) {
   return !((!inx && iny && inz) || (inx && !iny && inz) || (inx && iny && !inz) || (inx && iny && inz));
 }
 
-__device__ inline void load_cell(const double *arr, long ncell, long c, int nv, double *v) {
-  for (int iv = 0; iv < nv; iv++) v[iv] = arr[iv * ncell + c];
+// every kernel carries the NVMAX MHD variables (kgpu_create rejects others)
+__device__ inline void load_cell(const double *arr, long ncell, long c, double *v) {
+#pragma unroll
+  for (int iv = 0; iv < NVMAX; iv++) v[iv] = arr[iv * ncell + c];
 }
-__device__ inline void store_cell(double *arr, long ncell, long c, int nv, const double *v) {
-  for (int iv = 0; iv < nv; iv++) arr[iv * ncell + c] = v[iv];
+__device__ inline void store_cell(double *arr, long ncell, long c, const double *v) {
+#pragma unroll
+  for (int iv = 0; iv < NVMAX; iv++) arr[iv * ncell + c] = v[iv];
 }
 
 // ---------------------------------------------------------------------------
@@ -109,21 +112,21 @@ __global__ void k_bc_faces(Grid G, Box b) {
   }
   long c = cell_index(G, ix, iy, iz), s = cell_index(G, s3[0], s3[1], s3[2]);
   double pp[NVMAX], uu[NVMAX];
-  load_cell(G.p, G.ncell, s, G.nv, pp);
+  load_cell(G.p, G.ncell, s, pp);
   if (flip) {
     // the component normal to the boundary: VX/B1 for x, VY/B2 for y, VZ/B3 for z
     pp[VX + d] = -pp[VX + d];
     pp[B1 + d] = -pp[B1 + d];
   }
   if (kind == KGPU_BC_PERIODIC_COPY) {
-    load_cell(G.u, G.ncell, s, G.nv, uu);
+    load_cell(G.u, G.ncell, s, uu);
   } else {
     Geom g;
     geom_centre(G, ix, iy, iz, g);
     p2u_full(G, pp, uu, g);
   }
-  store_cell(G.p, G.ncell, c, G.nv, pp);
-  store_cell(G.u, G.ncell, c, G.nv, uu);
+  store_cell(G.p, G.ncell, c, pp);
+  store_cell(G.u, G.ncell, c, uu);
 }
 
 // Corners of a 2D periodic domain, filled as the reference does
@@ -174,15 +177,15 @@ __global__ void k_bc_corners2d(Grid G) {
   bool avg = k >= 2 * (G.ng - 1);
   long ca = cell_index(G, ax, ay, 0), cb = cell_index(G, bx, by, 0), c = cell_index(G, tx, ty, 0);
   double pp[NVMAX], uu[NVMAX];
-  for (int iv = 0; iv < G.nv; iv++) {
+  for (int iv = 0; iv < NVMAX; iv++) {
     double a = G.p[iv * G.ncell + ca];
     pp[iv] = avg ? .5 * (a + G.p[iv * G.ncell + cb]) : a;
   }
   Geom g;
   geom_centre(G, tx, ty, 0, g);
   p2u_full(G, pp, uu, g);
-  store_cell(G.p, G.ncell, c, G.nv, pp);
-  store_cell(G.u, G.ncell, c, G.nv, uu);
+  store_cell(G.p, G.ncell, c, pp);
+  store_cell(G.u, G.ncell, c, uu);
 }
 
 // Edges and corners of a 3D domain with physical boundaries, in the
@@ -196,15 +199,15 @@ __device__ inline void set_from(const Grid &G, int tx, int ty, int tz, int s1x, 
                                 int s2z, bool avg) {
   long c = cell_index(G, tx, ty, tz), a = cell_index(G, s1x, s1y, s1z), b = cell_index(G, s2x, s2y, s2z);
   double pp[NVMAX], uu[NVMAX];
-  for (int iv = 0; iv < G.nv; iv++) {
+  for (int iv = 0; iv < NVMAX; iv++) {
     double va = G.p[iv * G.ncell + a];
     pp[iv] = avg ? .5 * (va + G.p[iv * G.ncell + b]) : va;
   }
   Geom g;
   geom_centre(G, tx, ty, tz, g);
   p2u_full(G, pp, uu, g);
-  store_cell(G.p, G.ncell, c, G.nv, pp);
-  store_cell(G.u, G.ncell, c, G.nv, uu);
+  store_cell(G.p, G.ncell, c, pp);
+  store_cell(G.u, G.ncell, c, uu);
 }
 // one line of one elongated-edge pass.  Edge axis c, the two other axes
 // (a, b); corner k: bit 1 = high end of a, bit 0 = high end of b; position t
@@ -301,7 +304,7 @@ __global__ void k_wavespeeds(Grid G, Box b) {
   if (box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) {
     long c = cell_index(G, ix, iy, iz);
     double pp[NVMAX];
-    load_cell(G.p, G.ncell, c, G.nv, pp);
+    load_cell(G.p, G.ncell, c, pp);
     Geom g;
     geom_centre(G, ix, iy, iz, g);
     double al[3], ar[3];
@@ -335,56 +338,66 @@ __global__ void k_wavespeeds(Grid G, Box b) {
 // ---------------------------------------------------------------------------
 // fused face flux (finite.c:694-1014 and 1297-1624)
 // ---------------------------------------------------------------------------
+// Two threads per face, one per side: lane pair (2k, 2k+1) handles face k,
+// the even lane the left state (right-face value of cell i-1), the odd lane
+// the right state (left-face value of cell i).  Each lane reconstructs,
+// floors and evaluates its own state; the pair then swaps fluxes and
+// conserved values with shuffles and each lane stores every other variable.
+// Per face the arithmetic is exactly that of the one-thread form.
 template <int D>
-__global__ void __launch_bounds__(128) k_flux(Grid G, Box b) {
+__global__ void __launch_bounds__(128, 3) k_flux(Grid G, Box b) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int side = (int)(t & 1);
   int ix, iy, iz;
-  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
-  const int nv = G.nv;
+  const bool valid = box_coord(b, t >> 1, ix, iy, iz);
+  const unsigned pairmask = __ballot_sync(0xffffffffu, valid);
+  if (!valid) return;
+  constexpr int nv = NVMAX;
   const int i = D == 0 ? ix : (D == 1 ? iy : iz);
   const long stride = D == 0 ? 1 : (D == 1 ? (long)G.sx : (long)G.sx * G.sy);
   const long cR = cell_index(G, ix, iy, iz);     // cell i (right of the face)
   const long cL = cR - stride;                   // cell i-1
-  double dx[6];
-#pragma unroll
-  for (int k = 0; k < 6; k++) dx[k] = size_x(G, i - 3 + k, D);
 
-  // face states: left = right-face value of cell i-1, right = left-face
-  // value of cell i (avg2point of each cell, finite.c:89-289)
-  double pL[NVMAX], pR[NVMAX];
-  for (int iv = 0; iv < nv; iv++) {
-    const double *pv = G.p + iv * G.ncell + cR;
-    double v0 = pv[-3 * stride], v1 = pv[-2 * stride], v2 = pv[-stride], v3 = pv[0], v4 = pv[stride], v5 = pv[2 * stride];
-    if (G.int_order == 4) {
-      pL[iv] = mp5_face(v0, v1, v2, v3, v4);
-      pR[iv] = mp5_face(v5, v4, v3, v2, v1);
-    } else {
+  // reconstruction (avg2point, finite.c:89-289) of this lane's side
+  double ps[NVMAX];
+  if (G.int_order == 4) {
+    // left: MP5 centred on i-1 over cells i-3..i+1; right: centred on i,
+    // stencil mirrored, cells i+2..i-2
+    const long c0 = side ? cR + 2 * stride : cR - 3 * stride;
+    const long st = side ? -stride : stride;
+#pragma unroll
+    for (int iv = 0; iv < nv; iv++) {
+      const double *pv = G.p + iv * G.ncell + c0;
+      ps[iv] = mp5_face(pv[0], pv[st], pv[2 * st], pv[3 * st], pv[4 * st]);
+    }
+  } else {
+    // PPM of cell i-1 (its right value) or of cell i (its left value)
+    const int i0 = i - 3 + side;
+    double dx[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) dx[k] = size_x(G, i0 + k, D);
+    const long c0 = cR + (side - 3) * stride;
+#pragma unroll
+    for (int iv = 0; iv < nv; iv++) {
+      const double *pv = G.p + iv * G.ncell + c0;
       double ul, ur;
-      ppm(v0, v1, v2, v3, v4, dx[0], dx[1], dx[2], dx[3], dx[4], ul, ur);
-      pL[iv] = ur;
-      ppm(v1, v2, v3, v4, v5, dx[1], dx[2], dx[3], dx[4], dx[5], ul, ur);
-      pR[iv] = ul;
+      ppm(pv[0], pv[stride], pv[2 * stride], pv[3 * stride], pv[4 * stride], dx[0], dx[1], dx[2], dx[3], dx[4], ul,
+          ur);
+      ps[iv] = side ? ul : ur;
     }
   }
 
   Geom g;
   geom_face(G, ix, iy, iz, D, g);
-  const bool magn = nv > B3;
-  double fL[NVMAX], uL[NVMAX], fR[NVMAX], uR[NVMAX];
   // density floor of this face: x-faces sit at xb[ix], the others at x[ix]
   const double rfl = G.rhofl_c ? (D == 0 ? G.rhofl_f[ix + G.ng] : G.rhofl_c[ix + G.ng]) : -1.;
+  double fs[NVMAX], us[NVMAX];
   {
-    check_floors_mhd(G, pL, g, rfl);
+    check_floors_mhd(G, ps, g, rfl);
     Kin k;
-    kinematics(pL, g, magn, k);
-    flux_prime(G, pL, D, g, k, fL);
-    p2u_mhd(G, pL, uL, g, k);
-  }
-  {
-    check_floors_mhd(G, pR, g, rfl);
-    Kin k;
-    kinematics(pR, g, magn, k);
-    flux_prime(G, pR, D, g, k, fR);
-    p2u_mhd(G, pR, uR, g, k);
+    kinematics(ps, g, kMagn, k);
+    flux_prime(G, ps, D, g, k, fs);
+    p2u_mhd(G, ps, us, g, k);
   }
   double ap1l = G.al[D][cR], ap1r = G.ar[D][cR], am1l = G.al[D][cL], am1r = G.ar[D][cL];
   double ap1 = dmax(fabs(ap1l), fabs(ap1r)), am1 = dmax(fabs(am1l), fabs(am1r));
@@ -394,16 +407,22 @@ __global__ void __launch_bounds__(128) k_flux(Grid G, Box b) {
   const long f = face_index(G, ix, iy, iz, D);
   double *out = G.flb[D] + f;
   const long nf = G.nface[D];
+#pragma unroll
   for (int iv = 0; iv < nv; iv++) {
-    double fs;
+    const double fo = __shfl_xor_sync(pairmask, fs[iv], 1);
+    const double uo = __shfl_xor_sync(pairmask, us[iv], 1);
+    const double fL = side ? fo : fs[iv], fR = side ? fs[iv] : fo;
+    const double uL = side ? uo : us[iv], uR = side ? us[iv] : uo;
+    if ((iv & 1) != side) continue;
+    double fl;
     if (G.fluxmethod == 0) {
-      fs = .5 * (fR[iv] + fL[iv] - ag * (uR[iv] - uL[iv]));
+      fl = .5 * (fR + fL - ag * (uR - uL));
     } else {
-      if (al > 0.) fs = fL[iv];
-      else if (ar < 0.) fs = fL[iv];   // the reference takes the left flux here too (finite.c:1410)
-      else fs = (-al * fR[iv] + ar * fL[iv] + al * ar * (uR[iv] - uL[iv])) / (ar - al);
+      if (al > 0.) fl = fL;
+      else if (ar < 0.) fl = fL;   // the reference takes the left flux here too (finite.c:1410)
+      else fl = (-al * fR + ar * fL + al * ar * (uR - uL)) / (ar - al);
     }
-    out[iv * nf] = fs;
+    out[iv * nf] = fl;
   }
 }
 
@@ -472,11 +491,11 @@ __global__ void k_emf(Grid G, Box b) {
 __global__ void __launch_bounds__(128) k_update(Grid G, Box b, const double *dtp, double fac, double *save) {
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
-  const int nv = G.nv;
+  constexpr int nv = NVMAX;
   const long c = cell_index(G, ix, iy, iz);
   const double dt = fac * dtp[0];
   double pp[NVMAX];
-  load_cell(G.p, G.ncell, c, nv, pp);
+  load_cell(G.p, G.ncell, c, pp);
   Geom g;
   geom_centre(G, ix, iy, iz, g);
   Kin k;
@@ -581,26 +600,97 @@ __global__ void __launch_bounds__(128) k_update(Grid G, Box b, const double *dtp
 // calc_primitives u2p.c:13-133) and neighbour-average fixups
 // (cell_fixup finite.c:4467-4631)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_u2p(Grid G, Box b) {
-  int ix, iy, iz;
-  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
-  const long c = cell_index(G, ix, iy, iz);
-  double uu[NVMAX], pp[NVMAX];
-  load_cell(G.u, G.ncell, c, G.nv, uu);
-  load_cell(G.p, G.ncell, c, G.nv, pp);
-  Geom g;
-  geom_centre(G, ix, iy, iz, g);
-  int fix = 0;
-  int ret = u2p(G, uu, pp, g, fix);
-  if (uu[0] / g.gdet < 0.) atomicAdd(&G.cnt[C_NEGRHO], 1ull);
-  if (ret == -1) atomicAdd(&G.cnt[C_ENTROPY], 1ull);
-  if (ret == -3) atomicAdd(&G.cnt[C_FAIL], 1ull);
-  if (fix) atomicAdd(&G.cnt[C_FIXUP], 1ull);
+// Warp-aggregated counter increment: one atomic per converged group of lanes.
+__device__ inline void count_lanes(unsigned long long *ctr, bool pred) {
+  const unsigned m = __activemask();
+  const unsigned bits = __ballot_sync(m, pred);
+  if (bits && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(ctr, (unsigned long long)__popc(bits));
+}
+
+// Floors, conserved from primitives and the stores that end a cell's
+// inversion (calc_primitives u2p.c:82-127).
+__device__ inline void u2p_finish(const Grid &G, long c, int ix, double *pp, double *uu, const Geom &g, int fix) {
   check_floors_mhd(G, pp, g, G.rhofl_c ? G.rhofl_c[ix + G.ng] : -1.);
   p2u_full(G, pp, uu, g);
-  store_cell(G.p, G.ncell, c, G.nv, pp);
-  store_cell(G.u, G.ncell, c, G.nv, uu);
+  store_cell(G.p, G.ncell, c, pp);
+  store_cell(G.u, G.ncell, c, uu);
   G.flag[c] = fix;
+}
+
+// u2p (u2p.c:176-485) split in two launches so that the few cells whose
+// energy-equation inversion fails do not hold back whole warps.  Phase one
+// inverts every cell with the energy equation; a failing cell is queued
+// (its box index) together with the initial guess as the solver left it,
+// in pfix, which is free until the fixup pass.  Phase two runs the entropy
+// inversion on the queued cells only.  Per cell the sequence of operations
+// is exactly u2p's.
+__global__ void __launch_bounds__(128, 3) k_u2p(Grid G, Box b, int *queue, int *qcount) {
+  int ix, iy, iz;
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (!box_coord(b, t, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+  double uu[NVMAX], pp[NVMAX];
+  load_cell(G.u, G.ncell, c, uu);
+  load_cell(G.p, G.ncell, c, pp);
+  Geom g;
+  geom_centre(G, ix, iy, iz, g);
+  double uc[NVMAX];
+#pragma unroll
+  for (int iv = 0; iv < NVMAX; iv++) uc[iv] = uu[iv];
+  int ret = 0;
+  const bool negrho = uu[0] / g.gdet < 0.;
+  if (negrho) {
+    pp[0] = G.rhofloor;
+    uc[0] = G.rhofloor * g.gdet;
+    ret = -2;
+  }
+  count_lanes(&G.cnt[C_NEGRHO], negrho);
+  const bool failed = u2p_solver_W(G, uc, pp, g, 0) < 0;
+  {
+    const unsigned m = __activemask();
+    const unsigned bits = __ballot_sync(m, failed);
+    if (bits) {
+      const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(qcount, __popc(bits));
+      base = __shfl_sync(m, base, leader);
+      if (failed) queue[base + __popc(bits & ((1u << lane) - 1u))] = (int)t;
+    }
+  }
+  if (failed) {
+    store_cell(G.pfix, G.ncell, c, pp);
+    return;
+  }
+  const int fix = ret < -1 ? 1 : 0;
+  count_lanes(&G.cnt[C_FIXUP], fix != 0);
+  u2p_finish(G, c, ix, pp, uu, g, fix);
+}
+
+__global__ void __launch_bounds__(128) k_u2p_entropy(Grid G, Box b, const int *queue, const int *qcount) {
+  const int n = *qcount;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    box_coord(b, queue[q], ix, iy, iz);
+    const long c = cell_index(G, ix, iy, iz);
+    double uu[NVMAX], pp[NVMAX], uc[NVMAX];
+    load_cell(G.u, G.ncell, c, uu);
+    load_cell(G.pfix, G.ncell, c, pp);
+    Geom g;
+    geom_centre(G, ix, iy, iz, g);
+#pragma unroll
+    for (int iv = 0; iv < NVMAX; iv++) uc[iv] = uu[iv];
+    if (uu[0] / g.gdet < 0.) uc[0] = G.rhofloor * g.gdet;
+    int ret = -1;
+    if (u2p_solver_W(G, uc, pp, g, 1) < 0) {
+      ret = -3;   // -2 from the entropy failure, then -3: old primitives kept
+      load_cell(G.p, G.ncell, c, pp);
+    }
+    count_lanes(&G.cnt[C_ENTROPY], ret == -1);
+    count_lanes(&G.cnt[C_FAIL], ret == -3);
+    const int fix = ret < -1 ? 1 : 0;
+    count_lanes(&G.cnt[C_FIXUP], fix != 0);
+    u2p_finish(G, c, ix, pp, uu, g, fix);
+  }
 }
 
 // The reference visits cells in loop_0 order (x outer, z inner) and clears
@@ -612,7 +702,8 @@ __global__ void k_fixup(Grid G, Box b, int *fixmark) {
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
   const long c = cell_index(G, ix, iy, iz);
   if (G.flag[c] == 0) return;
-  const int NX = G.nx, NY = G.ny, NZ = G.nz, nv = G.nv;
+  const int NX = G.nx, NY = G.ny, NZ = G.nz;
+  constexpr int nv = NVMAX;
   int nb[6][3] = {{ix - 1, iy, iz}, {ix + 1, iy, iz}, {ix, iy - 1, iz}, {ix, iy + 1, iz}, {ix, iy, iz - 1}, {ix, iy, iz + 1}};
   bool inr[6] = {ix - 1 >= 0, ix + 1 < NX, iy - 1 >= 0, iy + 1 < NY, iz - 1 >= 0, iz + 1 < NZ};
   bool before[6] = {true, false, true, false, true, false};
@@ -639,18 +730,19 @@ __global__ void k_fixup(Grid G, Box b, int *fixmark) {
   Geom g;
   geom_centre(G, ix, iy, iz, g);
   p2u_full(G, pp, uu, g);
-  store_cell(G.pfix, G.ncell, c, nv, pp);
-  store_cell(G.ufix, G.ncell, c, nv, uu);
+  store_cell(G.pfix, G.ncell, c, pp);
+  store_cell(G.ufix, G.ncell, c, uu);
   fixmark[c] = 1;
 }
 
 // apply fixups; optionally finish an RK2 step: u = ut0 + (u - ut1)
 // (addi_u pair of ko.c:614-615)
-__global__ void k_commit(Grid G, Box b, const int *fixmark, int combine) {
+__global__ void k_commit(Grid G, Box b, const int *fixmark, int combine, int *qcount) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *qcount = 0;   // the inversion queue of this stage is spent
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
   const long c = cell_index(G, ix, iy, iz);
-  const int nv = G.nv;
+  constexpr int nv = NVMAX;
   if (G.flag[c] != 0) {
     if (fixmark[c]) {
       for (int iv = 0; iv < nv; iv++) {
@@ -678,13 +770,13 @@ __global__ void k_copy_domain(Grid G, Box b, double f, const double *src, double
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
   long c = cell_index(G, ix, iy, iz);
-  for (int iv = 0; iv < G.nv; iv++) dst[iv * G.ncell + c] = f * src[iv * G.ncell + c];
+  for (int iv = 0; iv < NVMAX; iv++) dst[iv * G.ncell + c] = f * src[iv * G.ncell + c];
 }
 __global__ void k_add_domain(Grid G, Box b, double f1, const double *a, double f2, const double *bb, double *c3) {
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
   long c = cell_index(G, ix, iy, iz);
-  for (int iv = 0; iv < G.nv; iv++) c3[iv * G.ncell + c] = f1 * a[iv * G.ncell + c] + f2 * bb[iv * G.ncell + c];
+  for (int iv = 0; iv < NVMAX; iv++) c3[iv * G.ncell + c] = f1 * a[iv * G.ncell + c] + f2 * bb[iv * G.ncell + c];
 }
 
 // KORAL layout [cell][var] <-> device [var][cell]
@@ -724,10 +816,11 @@ __global__ void k_fill(double *a, long n, double v) {
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------
-enum KernelId { K_BC = 0, K_WAVESPEEDS, K_FLUX0, K_FLUX1, K_FLUX2, K_EMF, K_UPDATE, K_U2P, K_FIXUP, K_COMMIT,
-                K_BEGIN, K_NKERNELS };
+enum KernelId { K_BC = 0, K_WAVESPEEDS, K_FLUX0, K_FLUX1, K_FLUX2, K_EMF, K_UPDATE, K_U2P, K_U2P_ENT, K_FIXUP,
+                K_COMMIT, K_BEGIN, K_NKERNELS };
 static const char *kKernelNames[K_NKERNELS] = {"k_bc", "k_wavespeeds", "k_flux_x", "k_flux_y", "k_flux_z", "k_emf",
-                                               "k_update", "k_u2p", "k_fixup", "k_commit", "k_begin_step"};
+                                               "k_update", "k_u2p", "k_u2p_entropy", "k_fixup", "k_commit",
+                                               "k_begin_step"};
 
 struct ProfRec {
   int id;
@@ -748,6 +841,8 @@ struct kgpu_ctx {
   std::vector<void *> allocs;
   double *stage;        // AoS staging for uploads / downloads
   int *fixmark;
+  int *u2p_queue, *u2p_qcount;   // cells left to the entropy inversion
+  int sm_count;
   double *rhofl_c = nullptr, *rhofl_f = nullptr;
   double min_dx, min_dy, min_dz;
   bool have_grid, have_metric;
@@ -876,6 +971,12 @@ extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
     delete c;
     return set_err("cudaStreamCreate", e);
   }
+  {
+    int dev = 0;
+    c->sm_count = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, dev);
+  }
   const size_t d8 = sizeof(double);
   const long ncv = G.ncell * G.nv;
   void *p;
@@ -907,6 +1008,8 @@ extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
   AL(G.emf, 3L * (G.nx + 1) * (G.ny + 1) * (G.nz + 1) * d8);
   AL(G.flag, G.ncell * sizeof(int));
   AL(c->fixmark, G.ncell * sizeof(int));
+  AL(c->u2p_queue, G.ncell * sizeof(int));
+  AL(c->u2p_qcount, sizeof(int));
   AL(G.scal, S_NSCAL * d8);
   AL(G.cnt, C_NCNT * sizeof(unsigned long long));
 #undef AL
@@ -922,6 +1025,7 @@ extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
   CK(cudaMemsetAsync(G.emf, 0, 3L * (G.nx + 1) * (G.ny + 1) * (G.nz + 1) * d8, c->stream));
   CK(cudaMemsetAsync(G.flag, 0, G.ncell * sizeof(int), c->stream));
   CK(cudaMemsetAsync(c->fixmark, 0, G.ncell * sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->u2p_qcount, 0, sizeof(int), c->stream));
   CK(cudaMemsetAsync(G.scal, 0, S_NSCAL * d8, c->stream));
   CK(cudaMemsetAsync(G.cnt, 0, C_NCNT * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync((void *)G.gkr, 0, G.nmet * 64 * d8, c->stream));
@@ -1151,19 +1255,19 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
   if (G.nx > 1) {
     Box b{0, ey0, ez0, G.nx + 1, eny, enz};
     LaunchScope ls(c, K_FLUX0);
-    k_flux<0><<<nblocks(b.n(), 128), 128, 0, c->stream>>>(G, b);
+    k_flux<0><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);
     CKL("k_flux<0>");
   }
   if (G.ny > 1) {
     Box b{ex0, 0, ez0, enx, G.ny + 1, enz};
     LaunchScope ls(c, K_FLUX1);
-    k_flux<1><<<nblocks(b.n(), 128), 128, 0, c->stream>>>(G, b);
+    k_flux<1><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);
     CKL("k_flux<1>");
   }
   if (G.nz > 1) {
     Box b{ex0, ey0, 0, enx, eny, G.nz + 1};
     LaunchScope ls(c, K_FLUX2);
-    k_flux<2><<<nblocks(b.n(), 128), 128, 0, c->stream>>>(G, b);
+    k_flux<2><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);
     CKL("k_flux<2>");
   }
   Box eb{0, 0, 0, G.nx + 1, G.ny + 1, G.nz + 1};
@@ -1178,11 +1282,16 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
 static int launch_u2p(kgpu_ctx *c, int combine) {
   Grid &G = c->G;
   Box db = domain_box(G);
-  { LaunchScope ls(c, K_U2P); k_u2p<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db); }
+  { LaunchScope ls(c, K_U2P); k_u2p<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, c->u2p_queue, c->u2p_qcount); }
   CKL("k_u2p");
+  {
+    LaunchScope ls(c, K_U2P_ENT);
+    k_u2p_entropy<<<c->sm_count * 4, 128, 0, c->stream>>>(G, db, c->u2p_queue, c->u2p_qcount);
+  }
+  CKL("k_u2p_entropy");
   { LaunchScope ls(c, K_FIXUP); k_fixup<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, c->fixmark); }
   CKL("k_fixup");
-  { LaunchScope ls(c, K_COMMIT); k_commit<<<nblocks(db.n(), 256), 256, 0, c->stream>>>(G, db, c->fixmark, combine); }
+  { LaunchScope ls(c, K_COMMIT); k_commit<<<nblocks(db.n(), 256), 256, 0, c->stream>>>(G, db, c->fixmark, combine, c->u2p_qcount); }
   CKL("k_commit");
   return launch_bc(c);
 }
@@ -1412,13 +1521,13 @@ __global__ void k_u2p_cells(Grid G, int n, const double *uu, double *pp, const d
   Geom g;
   load_geom(met, n, i, g);
   double u[NVMAX], p[NVMAX];
-  for (int iv = 0; iv < G.nv; iv++) {
+  for (int iv = 0; iv < NVMAX; iv++) {
     u[iv] = uu[(long)iv * n + i];
     p[iv] = pp[(long)iv * n + i];
   }
   int fix = 0;
   int ret = u2p(G, u, p, g, fix);
-  for (int iv = 0; iv < G.nv; iv++) pp[(long)iv * n + i] = p[iv];
+  for (int iv = 0; iv < NVMAX; iv++) pp[(long)iv * n + i] = p[iv];
   status[i] = ret;
   fixup[i] = fix;
 }
@@ -1428,9 +1537,9 @@ __global__ void k_p2u_cells(Grid G, int n, const double *pp, double *uu, const d
   Geom g;
   load_geom(met, n, i, g);
   double u[NVMAX], p[NVMAX];
-  for (int iv = 0; iv < G.nv; iv++) p[iv] = pp[(long)iv * n + i];
+  for (int iv = 0; iv < NVMAX; iv++) p[iv] = pp[(long)iv * n + i];
   p2u_full(G, p, u, g);
-  for (int iv = 0; iv < G.nv; iv++) uu[(long)iv * n + i] = u[iv];
+  for (int iv = 0; iv < NVMAX; iv++) uu[(long)iv * n + i] = u[iv];
 }
 
 static void to_soa(const double *aos, std::vector<double> &soa, int n, int m) {

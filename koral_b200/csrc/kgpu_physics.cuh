@@ -16,6 +16,7 @@ namespace kgpu {
 #define KG_HD __host__ __device__ inline
 
 constexpr int NVMAX = 9;           // MHD variables (no radiation on this path)
+constexpr bool kMagn = NVMAX > 8;  // the magnetic field is always carried
 constexpr int RHO = 0, UU = 1, VX = 2, VY = 3, VZ = 4, ENTR = 5, B1 = 6, B2 = 7, B3 = 8;
 constexpr double SMALL = 1.e-50, BIG = 1. / SMALL;
 
@@ -244,7 +245,7 @@ KG_HD void p2u_mhd(const Grid &G, const double *p, double *u, const Geom &g, con
   u[3] = gdetu * Ttth;
   u[4] = gdetu * Ttph;
   u[5] = gdetu * Sut;
-  if (G.nv > B3) {
+  if (kMagn) {
     u[B1] = gdetu * pb1;
     u[B2] = gdetu * pb2;
     u[B3] = gdetu * pb3;
@@ -252,7 +253,7 @@ KG_HD void p2u_mhd(const Grid &G, const double *p, double *u, const Geom &g, con
 }
 KG_HD void p2u_full(const Grid &G, const double *p, double *u, const Geom &g) {
   Kin k;
-  kinematics(p, g, G.nv > B3, k);
+  kinematics(p, g, kMagn, k);
   p2u_mhd(G, p, u, g, k);
 }
 
@@ -290,12 +291,12 @@ KG_HD void flux_prime(const Grid &G, const double *pp, int idim, const Geom &g, 
   double utp1 = calc_utp1(vcon, g);
   ff[0] = gdetu * rho * k.ucon[a];
   ff[1] = gdetu * (etap * k.ucon[a] * k.ucov[0] + rho * k.ucon[a] * utp1);
-  if (G.nv > B3) ff[1] += -gdetu * k.bcon[a] * k.bcov[0];
+  if (kMagn) ff[1] += -gdetu * k.bcon[a] * k.bcov[0];
   ff[2] = gdetu * (Tmix[1]);
   ff[3] = gdetu * (Tmix[2]);
   ff[4] = gdetu * (Tmix[3]);
   ff[5] = gdetu * S * k.ucon[a];
-  if (G.nv > B3) {
+  if (kMagn) {
     ff[B1] = gdetu * (k.bcon[1] * k.ucon[a] - k.bcon[a] * k.ucon[1]);
     ff[B2] = gdetu * (k.bcon[2] * k.ucon[a] - k.bcon[a] * k.ucon[2]);
     ff[B3] = gdetu * (k.bcon[3] * k.ucon[a] - k.bcon[a] * k.ucon[3]);
@@ -328,13 +329,13 @@ KG_HD void wavespeed_core(const double ucon[4], const Geom &g, double wspeed2, i
 // (calc_wavespeeds_lr_pure, physics.c:61-241, MHD part)
 KG_HD void wavespeeds(const Grid &G, const double *pp, const Geom &g, double al[3], double ar[3]) {
   Kin k;
-  kinematics(pp, g, G.nv > B3, k);
+  kinematics(pp, g, kMagn, k);
   double rho = pp[RHO], uu = pp[UU];
   double pre = (G.gamma - 1.) * uu;
   double cs2 = G.gamma * pre / (rho + uu + pre);
   if (cs2 < 0.) cs2 = 0.;
   double va2 = 0.;
-  if (G.nv > B3) {
+  if (kMagn) {
     double EF = rho + G.gamma * uu;
     double EEloc = k.bsq + EF;
     va2 = k.bsq / EEloc;
@@ -417,7 +418,7 @@ KG_HD bool u2p_bad_w(double W, double Bsq, double QdotBsq, double Qtsq, double f
 KG_HD int u2p_solver_W(const Grid &G, const double *uu, double *pp, const Geom &g, int Etype) {
   const double GAMMA = G.gamma;
   const double gdetu = g.gdet;
-  const bool magn = G.nv > B3;
+  const bool magn = kMagn;
   double alpha = sqrt(-1. / g.GG[0][0]);
   double D = uu[0] / gdetu * alpha;
   double Sc = uu[5] / gdetu * alpha;
@@ -540,7 +541,8 @@ KG_HD int u2p_solver_W(const Grid &G, const double *uu, double *pp, const Geom &
 // -2 entropy after negative density, -3 failure (old primitives kept).
 KG_HD int u2p(const Grid &G, const double *uu0, double *pp, const Geom &g, int &fixup) {
   double uu[NVMAX], ppbak[NVMAX];
-  const int nv = G.nv;
+  constexpr int nv = NVMAX;
+#pragma unroll
   for (int iv = 0; iv < nv; iv++) {
     uu[iv] = uu0[iv];
     ppbak[iv] = pp[iv];
@@ -559,6 +561,7 @@ KG_HD int u2p(const Grid &G, const double *uu0, double *pp, const Geom &g, int &
   }
   if (u2pret < 0) {
     ret = -3;
+#pragma unroll
     for (int iv = 0; iv < nv; iv++) pp[iv] = ppbak[iv];
   }
   fixup = (ret < -1) ? 1 : 0;
@@ -569,7 +572,7 @@ KG_HD int u2p(const Grid &G, const double *uu0, double *pp, const Geom &g, int &
 // (check_floors_mhd, u2p.c:492-695, B2RHOFLOORFRAME = ZAMO)
 KG_HD int check_floors_mhd(const Grid &G, double *pp, const Geom &g, double rhofloor_bh = -1.) {
   int ret = 0;
-  const bool magn = G.nv > B3;
+  const bool magn = kMagn;
   double uu[NVMAX];
   p2u_full(G, pp, uu, g);
   if (pp[0] < G.rhofloor) {
