@@ -151,6 +151,14 @@ int kgpu_rk2_steps_graph(kgpu_ctx *ctx, int nsteps);
  * out[0] cells flagged for fixup, out[1] entropy inversions,
  * out[2] failed inversions (old primitives kept), out[3] negative densities. */
 int kgpu_get_counters(kgpu_ctx *ctx, unsigned long long out[4]);
+/* All counters (up to n): the four above, then Newton steps of the energy
+ * and of the entropy solves, energy solves paused after the first pass, and
+ * cells handed to the entropy equation.  Returns how many were written. */
+int kgpu_get_counters_ex(kgpu_ctx *ctx, unsigned long long *out, int n);
+/* Tuning: Newton steps a cell may take in the first inversion pass before
+ * it is queued for the resumption pass (default 8; results do not depend
+ * on it). */
+int kgpu_set_u2p_pass_iters(kgpu_ctx *ctx, int n);
 int kgpu_reset_counters(kgpu_ctx *ctx);
 
 /* Problem set-up helpers (host-side, then uploaded). ---------------------- */

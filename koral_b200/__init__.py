@@ -95,6 +95,8 @@ def lib():
             "kgpu_rk2_steps_graph": [vp, ctypes.c_int],
             "kgpu_get_counters": [vp, ctypes.POINTER(ctypes.c_ulonglong)],
             "kgpu_reset_counters": [vp],
+            "kgpu_get_counters_ex": [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int],
+            "kgpu_set_u2p_pass_iters": [vp, ctypes.c_int],
             "kgpu_init_orszag_tang": [vp],
             "kgpu_u2p_cells": [ctypes.c_int, ctypes.POINTER(Config), _dp, _dp, _dp, _dp,
                                ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
@@ -290,9 +292,15 @@ class Subdomain:
         _check(fn(self.h, int(n)), "kgpu_rk2_steps")
 
     def counters(self):
-        a = (ctypes.c_ulonglong * 4)()
-        _check(self.L.kgpu_get_counters(self.h, a), "kgpu_get_counters")
-        return dict(fixups=a[0], entropy=a[1], failed=a[2], negrho=a[3])
+        a = (ctypes.c_ulonglong * 8)()
+        n = self.L.kgpu_get_counters_ex(self.h, a, 8)
+        if n < 0:
+            _check(n, "kgpu_get_counters_ex")
+        return dict(fixups=a[0], entropy=a[1], failed=a[2], negrho=a[3], iters_energy=a[4], iters_entropy=a[5],
+                    paused=a[6], to_entropy=a[7])
+
+    def set_u2p_pass_iters(self, n):
+        _check(self.L.kgpu_set_u2p_pass_iters(self.h, int(n)), "kgpu_set_u2p_pass_iters")
 
     @property
     def stream(self):

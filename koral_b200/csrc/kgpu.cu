@@ -49,6 +49,8 @@ static int set_err(const char *what, cudaError_t e) {
   } while (0)
 
 extern "C" const char *kgpu_last_error(void) { return g_lasterr; }
+// for the other translation units of the library
+int kgpu_report_cuda(const char *what, cudaError_t e) { return set_err(what, e); }
 extern "C" int kgpu_abi_version(void) { return KGPU_ABI_VERSION; }
 
 // ---------------------------------------------------------------------------
@@ -345,7 +347,7 @@ __global__ void k_wavespeeds(Grid G, Box b) {
 // conserved values with shuffles and each lane stores every other variable.
 // Per face the arithmetic is exactly that of the one-thread form.
 template <int D>
-__global__ void __launch_bounds__(128, 3) k_flux(Grid G, Box b) {
+__global__ void __launch_bounds__(128, 4) k_flux(Grid G, Box b) {
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const int side = (int)(t & 1);
   int ix, iy, iz;
@@ -488,7 +490,7 @@ __global__ void k_emf(Grid G, Box b) {
 // unsplit update with metric source terms (finite.c:1062-1160,
 // f_metric_source_term_arb physics.c:324-465)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_update(Grid G, Box b, const double *dtp, double fac, double *save) {
+__global__ void __launch_bounds__(128, 4) k_update(Grid G, Box b, const double *dtp, double fac, double *save) {
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
   constexpr int nv = NVMAX;
@@ -546,6 +548,7 @@ __global__ void __launch_bounds__(128) k_update(Grid G, Box b, const double *dtp
   const long fzl = face_index(G, ix, iy, iz, 2), fzr = face_index(G, ix, iy, iz + 1, 2);
   const long ne = (long)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
 #define EMFV(comp, a, b2, c2) G.emf[((comp)-1) * ne + emf_index(G, a, b2, c2)]
+#pragma unroll
   for (int iv = 0; iv < nv; iv++) {
     double flxl = G.flb[0][iv * G.nface[0] + fxl], flxr = G.flb[0][iv * G.nface[0] + fxr];
     double flyl = G.flb[1][iv * G.nface[1] + fyl], flyr = G.flb[1][iv * G.nface[1] + fyr];
@@ -617,79 +620,189 @@ __device__ inline void u2p_finish(const Grid &G, long c, int ix, double *pp, dou
   G.flag[c] = fix;
 }
 
-// u2p (u2p.c:176-485) split in two launches so that the few cells whose
-// energy-equation inversion fails do not hold back whole warps.  Phase one
-// inverts every cell with the energy equation; a failing cell is queued
-// (its box index) together with the initial guess as the solver left it,
-// in pfix, which is free until the fixup pass.  Phase two runs the entropy
-// inversion on the queued cells only.  Per cell the sequence of operations
-// is exactly u2p's.
-__global__ void __launch_bounds__(128, 3) k_u2p(Grid G, Box b, int *queue, int *qcount) {
+// Warp-aggregated append to a work queue of box indices.
+__device__ inline void queue_push(int *queue, int *qcount, bool pred, int item) {
+  const unsigned m = __activemask();
+  const unsigned bits = __ballot_sync(m, pred);
+  if (!bits) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(qcount, __popc(bits));
+  base = __shfl_sync(m, base, leader);
+  if (pred) queue[base + __popc(bits & ((1u << lane) - 1u))] = item;
+}
+
+__device__ inline void count_sum(unsigned long long *ctr, unsigned v) {
+  const unsigned m = __activemask();
+  const unsigned sum = __reduce_add_sync(m, v);
+  if (sum && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(ctr, (unsigned long long)sum);
+}
+
+// Queues of one inversion stage, reset by k_commit at the end of the stage.
+struct U2PQueues {
+  int *slow, *ent, *slow_ent;      // box indices
+  int *n;                          // counts: [0] slow, [1] ent, [2] slow_ent
+  double *w;                       // saved W of a paused solve, per cell
+  int *it;                         // saved iteration count, per cell
+};
+
+// Cell state at the start of u2p (u2p.c:187-215): the conserved variables
+// (with the negative-density fix applied by the caller), the primitive
+// guess, the metric.
+struct U2PCell {
+  long c;
+  int ix, iy, iz;
+  bool negrho;
+  double uc[NVMAX], pp[NVMAX];
+  Geom g;
+};
+
+__device__ inline void u2p_load(const Grid &G, int ix, int iy, int iz, const double *guess, U2PCell &x) {
+  x.ix = ix; x.iy = iy; x.iz = iz;
+  x.c = cell_index(G, ix, iy, iz);
+  load_cell(G.u, G.ncell, x.c, x.uc);
+  load_cell(guess, G.ncell, x.c, x.pp);
+  geom_centre(G, ix, iy, iz, x.g);
+  x.negrho = x.uc[0] / x.g.gdet < 0.;
+}
+
+// u2p (u2p.c:176-485) as a sequence of passes over work queues, so that the
+// few cells that need many Newton steps, heavy damping or the entropy
+// fallback do not hold back whole warps:
+//   k_u2p          energy equation, at most a few Newton steps and damping
+//                  halvings per cell;
+//   k_u2p_resume   continues the paused energy solves, one warp per cell;
+//   k_u2p_entropy  entropy equation for the cells whose energy solve failed,
+//                  with the same limits;
+//   k_u2p_resume   continues the paused entropy solves.
+// A paused solve keeps (W, iter) and resumes with exactly the steps it would
+// have taken, so per cell the arithmetic is that of u2p.  A cell whose
+// energy solve fails leaves its guess, as the solver left it, in pfix
+// (free until the fixup pass).
+__device__ inline void u2p_energy_done(const Grid &G, U2PQueues Q, int item, U2PCell &x, int r, int iter) {
+  count_sum(&G.cnt[C_ITERS_HOT], (unsigned)iter);
+  const bool failed = r < 0;
+  queue_push(Q.ent, Q.n + 1, failed, item);
+  count_lanes(&G.cnt[C_ENTQ], failed);
+  if (failed) {
+    store_cell(G.pfix, G.ncell, x.c, x.pp);
+    return;
+  }
+  const int fix = x.negrho ? 1 : 0;   // u2p's status stays -2 after a negative density
+  count_lanes(&G.cnt[C_FIXUP], fix != 0);
+  double uo[NVMAX];
+  u2p_finish(G, x.c, x.ix, x.pp, uo, x.g, fix);
+}
+
+__device__ inline void u2p_entropy_done(const Grid &G, U2PCell &x, int r, int iter) {
+  count_sum(&G.cnt[C_ITERS_ENT], (unsigned)iter);
+  int ret = -1;
+  if (r < 0) {
+    ret = -3;   // -2 from the entropy failure, then -3: old primitives kept
+    load_cell(G.p, G.ncell, x.c, x.pp);
+  }
+  count_lanes(&G.cnt[C_ENTROPY], ret == -1);
+  count_lanes(&G.cnt[C_FAIL], ret == -3);
+  const int fix = ret < -1 ? 1 : 0;
+  count_lanes(&G.cnt[C_FIXUP], fix != 0);
+  double uo[NVMAX];
+  u2p_finish(G, x.c, x.ix, x.pp, uo, x.g, fix);
+}
+
+// Damped-step halvings a first-pass solve may need before it is paused and
+// left to the warp-cooperative resumption pass.
+constexpr int U2P_DAMP_BUDGET = 4;
+
+// One solve of the given equation from its start (paused after `stop`
+// Newton steps or at the damping budget).  Returns U2P_PAUSED, 0
+// (primitives in x.pp) or a negative status.
+__device__ inline int u2p_run(const Grid &G, int Etype, U2PCell &x, int stop, double &W, int &iter) {
+  U2PState st;
+  u2p_setup(x.uc, x.g, st);
+  W = u2p_initial_w(G.gamma, x.pp, x.g);
+  iter = 0;
+  if (u2p_bracket(G.gamma, Etype, st.c, W)) return -150;
+  int r = u2p_newton(G.gamma, G.u2pconv, Etype, st.c, W, iter, stop, U2P_DAMP_BUDGET);
+  if (r) return r;
+  return u2p_final(G.gamma, st, W, iter, x.uc, x.pp, x.g);
+}
+
+__global__ void __launch_bounds__(128, 3) k_u2p(Grid G, Box b, U2PQueues Q, int stop) {
   int ix, iy, iz;
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (!box_coord(b, t, ix, iy, iz)) return;
-  const long c = cell_index(G, ix, iy, iz);
-  double uu[NVMAX], pp[NVMAX];
-  load_cell(G.u, G.ncell, c, uu);
-  load_cell(G.p, G.ncell, c, pp);
-  Geom g;
-  geom_centre(G, ix, iy, iz, g);
-  double uc[NVMAX];
-#pragma unroll
-  for (int iv = 0; iv < NVMAX; iv++) uc[iv] = uu[iv];
-  int ret = 0;
-  const bool negrho = uu[0] / g.gdet < 0.;
-  if (negrho) {
-    pp[0] = G.rhofloor;
-    uc[0] = G.rhofloor * g.gdet;
-    ret = -2;
+  U2PCell x;
+  u2p_load(G, ix, iy, iz, G.p, x);
+  if (x.negrho) {
+    x.pp[0] = G.rhofloor;
+    x.uc[0] = G.rhofloor * x.g.gdet;
   }
-  count_lanes(&G.cnt[C_NEGRHO], negrho);
-  const bool failed = u2p_solver_W(G, uc, pp, g, 0) < 0;
-  {
-    const unsigned m = __activemask();
-    const unsigned bits = __ballot_sync(m, failed);
-    if (bits) {
-      const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
-      int base = 0;
-      if (lane == leader) base = atomicAdd(qcount, __popc(bits));
-      base = __shfl_sync(m, base, leader);
-      if (failed) queue[base + __popc(bits & ((1u << lane) - 1u))] = (int)t;
-    }
-  }
-  if (failed) {
-    store_cell(G.pfix, G.ncell, c, pp);
+  count_lanes(&G.cnt[C_NEGRHO], x.negrho);
+  double W;
+  int iter;
+  const int r = u2p_run(G, 0, x, stop, W, iter);
+  const bool paused = r == U2P_PAUSED;
+  queue_push(Q.slow, Q.n + 0, paused, (int)t);
+  count_lanes(&G.cnt[C_SLOW], paused);
+  if (paused) {
+    Q.w[x.c] = W;
+    Q.it[x.c] = iter;
     return;
   }
-  const int fix = ret < -1 ? 1 : 0;
-  count_lanes(&G.cnt[C_FIXUP], fix != 0);
-  u2p_finish(G, c, ix, pp, uu, g, fix);
+  u2p_energy_done(G, Q, (int)t, x, r, iter);
 }
 
-__global__ void __launch_bounds__(128) k_u2p_entropy(Grid G, Box b, const int *queue, const int *qcount) {
-  const int n = *qcount;
+// Paused solves, one warp per cell (Etype 0: energy, 1: entropy).  All
+// lanes carry the cell; lane 0 writes the outcome.
+__global__ void __launch_bounds__(128) k_u2p_resume(Grid G, Box b, U2PQueues Q, int Etype) {
+  const int n = Q.n[Etype == 0 ? 0 : 2];
+  const int *queue = Etype == 0 ? Q.slow : Q.slow_ent;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n; q += nwarps) {
+    int ix, iy, iz;
+    const int item = queue[q];
+    box_coord(b, item, ix, iy, iz);
+    U2PCell x;
+    u2p_load(G, ix, iy, iz, Etype == 0 ? G.p : G.pfix, x);
+    if (x.negrho) {
+      if (Etype == 0) x.pp[0] = G.rhofloor;
+      x.uc[0] = G.rhofloor * x.g.gdet;
+    }
+    U2PState st;
+    u2p_setup(x.uc, x.g, st);
+    double W = Q.w[x.c];
+    int iter = Q.it[x.c];
+    int r = u2p_newton_warp(G.gamma, G.u2pconv, Etype, st.c, W, iter);
+    if (r == 0) r = u2p_final(G.gamma, st, W, iter, x.uc, x.pp, x.g);
+    if (lane == 0) {
+      if (Etype == 0) u2p_energy_done(G, Q, item, x, r, iter);
+      else u2p_entropy_done(G, x, r, iter);
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(128) k_u2p_entropy(Grid G, Box b, U2PQueues Q, int stop) {
+  const int n = Q.n[1];
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
     int ix, iy, iz;
-    box_coord(b, queue[q], ix, iy, iz);
-    const long c = cell_index(G, ix, iy, iz);
-    double uu[NVMAX], pp[NVMAX], uc[NVMAX];
-    load_cell(G.u, G.ncell, c, uu);
-    load_cell(G.pfix, G.ncell, c, pp);
-    Geom g;
-    geom_centre(G, ix, iy, iz, g);
-#pragma unroll
-    for (int iv = 0; iv < NVMAX; iv++) uc[iv] = uu[iv];
-    if (uu[0] / g.gdet < 0.) uc[0] = G.rhofloor * g.gdet;
-    int ret = -1;
-    if (u2p_solver_W(G, uc, pp, g, 1) < 0) {
-      ret = -3;   // -2 from the entropy failure, then -3: old primitives kept
-      load_cell(G.p, G.ncell, c, pp);
+    const int item = Q.ent[q];
+    box_coord(b, item, ix, iy, iz);
+    U2PCell x;
+    u2p_load(G, ix, iy, iz, G.pfix, x);
+    if (x.negrho) x.uc[0] = G.rhofloor * x.g.gdet;
+    double W;
+    int iter;
+    const int r = u2p_run(G, 1, x, stop, W, iter);
+    const bool paused = r == U2P_PAUSED;
+    queue_push(Q.slow_ent, Q.n + 2, paused, item);
+    if (paused) {
+      Q.w[x.c] = W;
+      Q.it[x.c] = iter;
+      continue;
     }
-    count_lanes(&G.cnt[C_ENTROPY], ret == -1);
-    count_lanes(&G.cnt[C_FAIL], ret == -3);
-    const int fix = ret < -1 ? 1 : 0;
-    count_lanes(&G.cnt[C_FIXUP], fix != 0);
-    u2p_finish(G, c, ix, pp, uu, g, fix);
+    u2p_entropy_done(G, x, r, iter);
   }
 }
 
@@ -738,7 +851,7 @@ __global__ void k_fixup(Grid G, Box b, int *fixmark) {
 // apply fixups; optionally finish an RK2 step: u = ut0 + (u - ut1)
 // (addi_u pair of ko.c:614-615)
 __global__ void k_commit(Grid G, Box b, const int *fixmark, int combine, int *qcount) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *qcount = 0;   // the inversion queue of this stage is spent
+  if (blockIdx.x == 0 && threadIdx.x < 3) qcount[threadIdx.x] = 0;   // the inversion queues of this stage are spent
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
   const long c = cell_index(G, ix, iy, iz);
@@ -816,11 +929,11 @@ __global__ void k_fill(double *a, long n, double v) {
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------
-enum KernelId { K_BC = 0, K_WAVESPEEDS, K_FLUX0, K_FLUX1, K_FLUX2, K_EMF, K_UPDATE, K_U2P, K_U2P_ENT, K_FIXUP,
-                K_COMMIT, K_BEGIN, K_NKERNELS };
+enum KernelId { K_BC = 0, K_WAVESPEEDS, K_FLUX0, K_FLUX1, K_FLUX2, K_EMF, K_UPDATE, K_U2P, K_U2P_RESUME,
+                K_U2P_ENT, K_U2P_RESUME_ENT, K_FIXUP, K_COMMIT, K_BEGIN, K_NKERNELS };
 static const char *kKernelNames[K_NKERNELS] = {"k_bc", "k_wavespeeds", "k_flux_x", "k_flux_y", "k_flux_z", "k_emf",
-                                               "k_update", "k_u2p", "k_u2p_entropy", "k_fixup", "k_commit",
-                                               "k_begin_step"};
+                                               "k_update", "k_u2p", "k_u2p_resume", "k_u2p_entropy",
+                                               "k_u2p_resume_entropy", "k_fixup", "k_commit", "k_begin_step"};
 
 struct ProfRec {
   int id;
@@ -841,7 +954,8 @@ struct kgpu_ctx {
   std::vector<void *> allocs;
   double *stage;        // AoS staging for uploads / downloads
   int *fixmark;
-  int *u2p_queue, *u2p_qcount;   // cells left to the entropy inversion
+  U2PQueues u2pq;                // work queues of the inversion passes
+  int u2p_pass_iters = 8;        // Newton steps before a solve is queued for resumption
   int sm_count;
   double *rhofl_c = nullptr, *rhofl_f = nullptr;
   double min_dx, min_dy, min_dz;
@@ -1008,8 +1122,12 @@ extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
   AL(G.emf, 3L * (G.nx + 1) * (G.ny + 1) * (G.nz + 1) * d8);
   AL(G.flag, G.ncell * sizeof(int));
   AL(c->fixmark, G.ncell * sizeof(int));
-  AL(c->u2p_queue, G.ncell * sizeof(int));
-  AL(c->u2p_qcount, sizeof(int));
+  AL(c->u2pq.slow, G.ncell * sizeof(int));
+  AL(c->u2pq.ent, G.ncell * sizeof(int));
+  AL(c->u2pq.slow_ent, G.ncell * sizeof(int));
+  AL(c->u2pq.n, 4 * sizeof(int));
+  AL(c->u2pq.w, G.ncell * d8);
+  AL(c->u2pq.it, G.ncell * sizeof(int));
   AL(G.scal, S_NSCAL * d8);
   AL(G.cnt, C_NCNT * sizeof(unsigned long long));
 #undef AL
@@ -1025,13 +1143,22 @@ extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
   CK(cudaMemsetAsync(G.emf, 0, 3L * (G.nx + 1) * (G.ny + 1) * (G.nz + 1) * d8, c->stream));
   CK(cudaMemsetAsync(G.flag, 0, G.ncell * sizeof(int), c->stream));
   CK(cudaMemsetAsync(c->fixmark, 0, G.ncell * sizeof(int), c->stream));
-  CK(cudaMemsetAsync(c->u2p_qcount, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->u2pq.n, 0, 4 * sizeof(int), c->stream));
   CK(cudaMemsetAsync(G.scal, 0, S_NSCAL * d8, c->stream));
   CK(cudaMemsetAsync(G.cnt, 0, C_NCNT * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync((void *)G.gkr, 0, G.nmet * 64 * d8, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   *out = c;
   return 0;
+}
+
+// The captured step holds kernel arguments by value: drop it when they change.
+static void drop_graph(kgpu_ctx *c) {
+  if (c->graph_ready) {
+    cudaGraphExecDestroy(c->graph_exec);
+    cudaGraphDestroy(c->graph);
+    c->graph_ready = false;
+  }
 }
 
 extern "C" int kgpu_destroy(kgpu_ctx *c) {
@@ -1148,7 +1275,7 @@ extern "C" int kgpu_set_density_floor(kgpu_ctx *c, const double *centres, const 
   CK(cudaStreamSynchronize(c->stream));
   G.rhofl_c = c->rhofl_c;
   G.rhofl_f = c->rhofl_f;
-  c->graph_ready = false;   // kernels take the Grid by value: re-capture
+  drop_graph(c);   // kernels take the Grid by value: re-capture
   return 0;
 }
 
@@ -1282,16 +1409,18 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
 static int launch_u2p(kgpu_ctx *c, int combine) {
   Grid &G = c->G;
   Box db = domain_box(G);
-  { LaunchScope ls(c, K_U2P); k_u2p<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, c->u2p_queue, c->u2p_qcount); }
+  const int sweep = c->sm_count * 4;   // grid of the queue passes (grid-stride loops)
+  { LaunchScope ls(c, K_U2P); k_u2p<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, c->u2pq, c->u2p_pass_iters); }
   CKL("k_u2p");
-  {
-    LaunchScope ls(c, K_U2P_ENT);
-    k_u2p_entropy<<<c->sm_count * 4, 128, 0, c->stream>>>(G, db, c->u2p_queue, c->u2p_qcount);
-  }
+  { LaunchScope ls(c, K_U2P_RESUME); k_u2p_resume<<<sweep, 128, 0, c->stream>>>(G, db, c->u2pq, 0); }
+  CKL("k_u2p_resume");
+  { LaunchScope ls(c, K_U2P_ENT); k_u2p_entropy<<<sweep, 128, 0, c->stream>>>(G, db, c->u2pq, c->u2p_pass_iters); }
   CKL("k_u2p_entropy");
+  { LaunchScope ls(c, K_U2P_RESUME_ENT); k_u2p_resume<<<sweep, 128, 0, c->stream>>>(G, db, c->u2pq, 1); }
+  CKL("k_u2p_resume_entropy");
   { LaunchScope ls(c, K_FIXUP); k_fixup<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, c->fixmark); }
   CKL("k_fixup");
-  { LaunchScope ls(c, K_COMMIT); k_commit<<<nblocks(db.n(), 256), 256, 0, c->stream>>>(G, db, c->fixmark, combine, c->u2p_qcount); }
+  { LaunchScope ls(c, K_COMMIT); k_commit<<<nblocks(db.n(), 256), 256, 0, c->stream>>>(G, db, c->fixmark, combine, c->u2pq.n); }
   CKL("k_commit");
   return launch_bc(c);
 }
@@ -1448,6 +1577,22 @@ extern "C" int kgpu_get_counters(kgpu_ctx *c, unsigned long long out[4]) {
   CK(cudaMemcpyAsync(h, c->G.cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   for (int i = 0; i < 4; i++) out[i] = h[i];
+  return 0;
+}
+
+extern "C" int kgpu_get_counters_ex(kgpu_ctx *c, unsigned long long *out, int n) {
+  if (!c || !out || n < 0) return KGPU_EINVAL;
+  unsigned long long h[C_NCNT];
+  CK(cudaMemcpyAsync(h, c->G.cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < n && i < C_NCNT; i++) out[i] = h[i];
+  return n < C_NCNT ? n : C_NCNT;
+}
+
+extern "C" int kgpu_set_u2p_pass_iters(kgpu_ctx *c, int n) {
+  if (!c || n < 1) return KGPU_EINVAL;
+  c->u2p_pass_iters = n;
+  drop_graph(c);
   return 0;
 }
 

@@ -51,7 +51,14 @@ struct Grid {
 };
 
 enum ScalarSlot { S_TSTEPDENMAX = 0, S_TSTEPDENMIN = 1, S_DT = 2, S_T = 3, S_NSCAL = 8 };
-enum CounterSlot { C_FIXUP = 0, C_ENTROPY = 1, C_FAIL = 2, C_NEGRHO = 3, C_NCNT = 8 };
+enum CounterSlot {
+  C_FIXUP = 0, C_ENTROPY = 1, C_FAIL = 2, C_NEGRHO = 3,
+  C_ITERS_HOT = 4,   // Newton steps of energy-equation solves
+  C_ITERS_ENT = 5,   // Newton steps of entropy-equation solves
+  C_SLOW = 6,        // energy solves paused after the first pass and resumed
+  C_ENTQ = 7,        // cells handed to the entropy equation
+  C_NCNT = 8
+};
 
 // ---------------------------------------------------------------------------
 // index helpers (ko.h:190-230 and 505-560, with the same collapse of unused
@@ -412,13 +419,17 @@ KG_HD bool u2p_bad_w(double W, double Bsq, double QdotBsq, double Qtsq, double f
          !isfinite(df);
 }
 
-// Returns 0 on success or the reference's negative status codes.
-// Iteration counts are bounded exactly as in the reference (50 bracket
-// expansions, 50 Newton steps, 100 halvings), so every call terminates.
-KG_HD int u2p_solver_W(const Grid &G, const double *uu, double *pp, const Geom &g, int Etype) {
-  const double GAMMA = G.gamma;
+// The W solver in resumable pieces.  U2PState holds everything the solver
+// derives from the conserved variables and the metric; the Newton loop's
+// only carried state is (W, iter), so a solve stopped after some iterations
+// and resumed later takes exactly the same steps as an uninterrupted one.
+struct U2PState {
+  U2PCons c;
+  double Qtcon[4], Bcon[4], QdotB;
+};
+
+KG_HD void u2p_setup(const double *uu, const Geom &g, U2PState &s) {
   const double gdetu = g.gdet;
-  const bool magn = kMagn;
   double alpha = sqrt(-1. / g.GG[0][0]);
   double D = uu[0] / gdetu * alpha;
   double Sc = uu[5] / gdetu * alpha;
@@ -428,64 +439,85 @@ KG_HD int u2p_solver_W(const Grid &G, const double *uu, double *pp, const Geom &
   Qcov[2] = uu[3] / gdetu * alpha;
   Qcov[3] = uu[4] / gdetu * alpha;
   raise(Qcov, Qcon, g.GG);
-  double Bcon[4] = {0., 0., 0., 0.}, Bcov[4], Bsq = 0., QdotB = 0., QdotBsq = 0.;
-  if (magn) {
-    Bcon[1] = uu[B1] / gdetu * alpha;
-    Bcon[2] = uu[B2] / gdetu * alpha;
-    Bcon[3] = uu[B3] / gdetu * alpha;
-    lower(Bcon, Bcov, g.gg);
-    Bsq = dot4(Bcon, Bcov);
-    QdotB = dot4(Qcov, Bcon);
+  double Bcov[4], Bsq = 0., QdotB = 0., QdotBsq = 0.;
+  s.Bcon[0] = s.Bcon[1] = s.Bcon[2] = s.Bcon[3] = 0.;
+  if (kMagn) {
+    s.Bcon[1] = uu[B1] / gdetu * alpha;
+    s.Bcon[2] = uu[B2] / gdetu * alpha;
+    s.Bcon[3] = uu[B3] / gdetu * alpha;
+    lower(s.Bcon, Bcov, g.gg);
+    Bsq = dot4(s.Bcon, Bcov);
+    QdotB = dot4(Qcov, s.Bcon);
     QdotBsq = QdotB * QdotB;
   }
   double ncov[4] = {-alpha, 0., 0., 0.}, ncon[4];
   raise(ncov, ncon, g.GG);
   double Qn = Qcon[0] * ncov[0];
-  double Qtcon[4], Qtcov[4];
+  double Qtcov[4];
 #pragma unroll
   for (int i = 0; i < 4; i++) {
-    double s = 0.;
+    double sum = 0.;
 #pragma unroll
-    for (int j = 0; j < 4; j++) s += ((i == j ? 1 : 0) + ncon[i] * ncov[j]) * Qcon[j];
-    Qtcon[i] = s;
+    for (int j = 0; j < 4; j++) sum += ((i == j ? 1 : 0) + ncon[i] * ncov[j]) * Qcon[j];
+    s.Qtcon[i] = sum;
   }
-  lower(Qtcon, Qtcov, g.gg);
-  double Qt2 = dot4(Qtcon, Qtcov);
-  double Qtsq = Qt2;
+  lower(s.Qtcon, Qtcov, g.gg);
+  double Qt2 = dot4(s.Qtcon, Qtcov);
+  s.QdotB = QdotB;
+  s.c = U2PCons{Qn, Qt2, D, QdotBsq, Bsq, Sc};
+}
 
+// initial W from the primitive guess (u2p.c:2100-2110)
+KG_HD double u2p_initial_w(double GAMMA, const double *pp, const Geom &g) {
   double qsq = 0.;
 #pragma unroll
   for (int i = 1; i < 4; i++)
 #pragma unroll
     for (int j = 1; j < 4; j++) qsq += pp[1 + i] * pp[1 + j] * g.gg[i][j];
   double gamma2 = 1. + qsq;
-  double W = (pp[0] + GAMMA * pp[1]) * gamma2;
+  return (pp[0] + GAMMA * pp[1]) * gamma2;
+}
 
-  U2PCons c{Qn, Qt2, D, QdotBsq, Bsq, Sc};
+// W x 10 until the state is physical (u2p.c:2117-2135); 0 or -150
+KG_HD int u2p_bracket(double GAMMA, int Etype, const U2PCons &c, double &W) {
   double f0, dfdW, err;
   int i_increase = 0;
   while (true) {
     f0 = dfdW = 0.;
-    f_u2p(GAMMA, Etype, W - D, c, f0, dfdW, err);
-    if (u2p_bad_w(W, Bsq, QdotBsq, Qtsq, f0, dfdW) && (i_increase < 50)) {
+    f_u2p(GAMMA, Etype, W - c.D, c, f0, dfdW, err);
+    if (u2p_bad_w(W, c.Bsq, c.QdotBsq, c.Qt2, f0, dfdW) && (i_increase < 50)) {
       W *= 10.;
       i_increase++;
       continue;
     }
     break;
   }
-  if (i_increase >= 50) return -150;
+  return i_increase >= 50 ? -150 : 0;
+}
 
-  const double CONV = G.u2pconv;
-  int iter = 0;
-  do {
+constexpr int U2P_PAUSED = 1;
+
+// Newton iterations (u2p.c:2140-2200) until convergence, failure, or a
+// pause: at the top of an iteration once iter reaches `stop`, or before an
+// iteration whose damped step would need `damp_budget` or more halvings
+// (the iteration is then undone, (W, iter) as before it).  A paused solve
+// resumed with larger limits takes exactly the steps an uninterrupted one
+// takes.  Returns 0 when the loop has ended (the caller finishes with
+// u2p_final), U2P_PAUSED, or a negative reference status on failure.
+KG_HD int u2p_newton(double GAMMA, double CONV, int Etype, const U2PCons &c, double &W, int &iter, int stop,
+                     int damp_budget = 1 << 30) {
+  const double D = c.D;
+  double f0, dfdW, err;
+  while (true) {
+    if (iter >= stop && iter < 50) return U2P_PAUSED;
     double Wprev = W;
     iter++;
     f_u2p(GAMMA, Etype, W - D, c, f0, dfdW, err);
     if (err < CONV) break;
     if (dfdW == 0.) {
       W *= 1.1;
-      continue;
+      if (iter < 50) continue;
+      break;
     }
     double Wnew = W - f0 / dfdW;
     int idump = 0;
@@ -493,8 +525,13 @@ KG_HD int u2p_solver_W(const Grid &G, const double *uu, double *pp, const Geom &
     while (true) {
       double f0t = 0., dft = 0., errt;
       f_u2p(GAMMA, Etype, Wnew - D, c, f0t, dft, errt);
-      if (u2p_bad_w(Wnew, Bsq, QdotBsq, Qtsq, f0t, dft) && (idump < 100)) {
+      if (u2p_bad_w(Wnew, c.Bsq, c.QdotBsq, c.Qt2, f0t, dft) && (idump < 100)) {
         idump++;
+        if (idump >= damp_budget) {
+          W = Wprev;
+          iter--;
+          return U2P_PAUSED;
+        }
         dumpfac /= 2.;
         Wnew = W - dumpfac * f0 / dfdW;
         continue;
@@ -505,20 +542,84 @@ KG_HD int u2p_solver_W(const Grid &G, const double *uu, double *pp, const Geom &
     W = Wnew;
     if (fabs(W) > BIG) return -103;
     if (fabs((W - Wprev) / Wprev) < CONV && err < 1.e-1) break;
-  } while (iter < 50);
+    if (!(iter < 50)) break;
+  }
+  return 0;
+}
+
+#ifdef __CUDACC__
+// The same iterations carried out by a whole warp on one cell (all lanes
+// hold the same state): the damped step's trial points, which the scalar
+// loop tries one after another, are tried 32 at a time and the first
+// acceptable one is taken.  Trial k is W - 2^-k f/f' as in the scalar loop
+// (2^-k is the exact result of its repeated halving), so the result is the
+// same bit for bit.  Every lane returns the same values.
+__device__ inline int u2p_newton_warp(double GAMMA, double CONV, int Etype, const U2PCons &c, double &W, int &iter) {
+  const int lane = threadIdx.x & 31;
+  const double D = c.D;
+  double f0, dfdW, err;
+  while (true) {
+    double Wprev = W;
+    iter++;
+    f_u2p(GAMMA, Etype, W - D, c, f0, dfdW, err);
+    if (err < CONV) break;
+    if (dfdW == 0.) {
+      W *= 1.1;
+      if (iter < 50) continue;
+      break;
+    }
+    double Wnew = 0.;
+    int found = -1;
+    for (int base = 0; base <= 100 && found < 0; base += 32) {
+      const int k = base + lane;
+      double Wk = 0.;
+      bool accept = false;
+      if (k == 0) {
+        Wk = W - f0 / dfdW;
+      } else if (k <= 100) {
+        const double dumpfac = ldexp(1.0, -k);
+        Wk = W - dumpfac * f0 / dfdW;
+      }
+      if (k == 100) {
+        accept = true;   // the scalar loop stops here whatever the state
+      } else if (k < 100) {
+        double f0t = 0., dft = 0., errt;
+        f_u2p(GAMMA, Etype, Wk - D, c, f0t, dft, errt);
+        accept = !u2p_bad_w(Wk, c.Bsq, c.QdotBsq, c.Qt2, f0t, dft);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, accept);
+      if (m) {
+        const int L = __ffs(m) - 1;
+        found = base + L;
+        Wnew = __shfl_sync(0xffffffffu, Wk, L);
+      }
+    }
+    if (found >= 100) return -101;
+    W = Wnew;
+    if (fabs(W) > BIG) return -103;
+    if (fabs((W - Wprev) / Wprev) < CONV && err < 1.e-1) break;
+    if (!(iter < 50)) break;
+  }
+  return 0;
+}
+#endif
+
+// checks and primitives from the converged W (u2p.c:2205-2292)
+KG_HD int u2p_final(double GAMMA, const U2PState &s, double W, int iter, const double *uu, double *pp, const Geom &g) {
   if (iter >= 50) return -102;
   if (!isfinite(W)) return -103;
-
+  const double gdetu = g.gdet;
+  const double Bsq = s.c.Bsq, QdotBsq = s.c.QdotBsq, Qtsq = s.c.Qt2, D = s.c.D, QdotB = s.QdotB;
   double Wsq = W * W;
   double Xsq = (Bsq + W) * (Bsq + W);
   double v2 = (Wsq * Qtsq + QdotBsq * (Bsq + 2. * W)) / (Wsq * Xsq);
-  gamma2 = 1. / (1. - v2);
+  double gamma2 = 1. / (1. - v2);
   double gamma = sqrt(gamma2);
   double rho = D / gamma;
   double uint = 1. / GAMMA * (W / gamma2 - rho);
-  double ut1 = gamma / (W + Bsq) * (Qtcon[1] + QdotB * Bcon[1] / W);
-  double ut2 = gamma / (W + Bsq) * (Qtcon[2] + QdotB * Bcon[2] / W);
-  double ut3 = gamma / (W + Bsq) * (Qtcon[3] + QdotB * Bcon[3] / W);
+  double ut1 = gamma / (W + Bsq) * (s.Qtcon[1] + QdotB * s.Bcon[1] / W);
+  double ut2 = gamma / (W + Bsq) * (s.Qtcon[2] + QdotB * s.Bcon[2] / W);
+  double ut3 = gamma / (W + Bsq) * (s.Qtcon[3] + QdotB * s.Bcon[3] / W);
   if (!isfinite(ut1)) return -120;
   if (uint < 0. || gamma2 < 0. || isnan(W) || !isfinite(W)) return -104;
   pp[0] = rho;
@@ -527,13 +628,27 @@ KG_HD int u2p_solver_W(const Grid &G, const double *uu, double *pp, const Geom &
   pp[3] = ut2;
   pp[4] = ut3;
   if (rho < 0.) return -105;
-  pp[5] = calc_Sfromu(G.gamma, rho, uint);
-  if (magn) {
+  pp[5] = calc_Sfromu(GAMMA, rho, uint);
+  if (kMagn) {
     pp[B1] = uu[B1] / gdetu;
     pp[B2] = uu[B2] / gdetu;
     pp[B3] = uu[B3] / gdetu;
   }
   return 0;
+}
+
+// Returns 0 on success or the reference's negative status codes.
+// Iteration counts are bounded exactly as in the reference (50 bracket
+// expansions, 50 Newton steps, 100 halvings), so every call terminates.
+KG_HD int u2p_solver_W(const Grid &G, const double *uu, double *pp, const Geom &g, int Etype) {
+  U2PState s;
+  u2p_setup(uu, g, s);
+  double W = u2p_initial_w(G.gamma, pp, g);
+  if (u2p_bracket(G.gamma, Etype, s.c, W)) return -150;
+  int iter = 0;
+  int r = u2p_newton(G.gamma, G.u2pconv, Etype, s.c, W, iter, 1 << 30);
+  if (r < 0) return r;
+  return u2p_final(G.gamma, s, W, iter, uu, pp, g);
 }
 
 // high-level inversion with entropy fallback and "keep old" last resort

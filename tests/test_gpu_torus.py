@@ -157,3 +157,26 @@ def test_u2p_at_kerr_points_matches_oracle(kgpu, oracle):
     hot = so == 0
     assert hot.mean() > 0.9
     assert np.array_equal(pg[hot][:, [0, 1, 2, 3, 4, 6, 7, 8]], po[hot][:, [0, 1, 2, 3, 4, 6, 7, 8]])
+
+
+def test_u2p_pause_and_resume_is_exact(kgpu, oracle):
+    """The inversion runs as passes over work queues: a cell whose Newton
+    solve is not done after a few steps, or needs many damping halvings, is
+    paused and resumed in a later pass (one warp per cell).  Where the pause
+    falls must not change any bit of the result."""
+    R, s = make_pair(kgpu, oracle)
+    u0, p0 = R.array("u").copy(), R.array("p").copy()
+    tsd = R.scalar("tstepdenmax")
+    states = []
+    for n in (8, 1, 3, 1000):
+        s.upload_state(u0.copy(), p0.copy())
+        s.tstepdenmax = tsd
+        s.set_u2p_pass_iters(n)
+        s.reset_counters()
+        s.rk2_steps(20)
+        states.append(s.download_state())
+        cnt = s.counters()
+        if n == 1:
+            assert cnt["paused"] > 0
+    for u, p in states[1:]:
+        assert np.array_equal(u, states[0][0]) and np.array_equal(p, states[0][1])
