@@ -249,6 +249,78 @@ int kgpu_launch_count(kgpu_ctx *ctx, long long *out);
 int kgpu_download_flux(kgpu_ctx *ctx, int d, double *out);
 int kgpu_download_emf(kgpu_ctx *ctx, double *out);
 
+/* Radiation: per-cell implicit gas-radiation source solve. ----------------
+ * A cell carries 13 doubles: the nine MHD variables followed by the M1
+ * radiation variables (primitives: rest-frame energy density and the
+ * relative four-velocity of the radiation frame; conserved: R^t_t, R^t_i),
+ * KORAL's order with RADIATION and MAGNFIELD (mnemonics.h:29-55).  Metric
+ * points are 20 + 20 doubles as elsewhere.  Opacities: Kramers-type
+ * absorption kappa = kramers rho T^-3.5 cm^2/g plus electron scattering kes
+ * cm^2/g, converted to code units with the black-hole mass. */
+typedef struct {
+  double gamma;                        /* adiabatic index                         */
+  double kb, mp, sigma, mu;            /* K_BOLTZ, M_PROTON, SIGMA_RAD, MU_GAS    */
+  double ggg, ccc, masscm;             /* G, c (cgs) and GM/c^2 (cm)              */
+  double kramers, kes;                 /* opacity law coefficients (cgs)          */
+  double kes_gu;                       /* kes in code units                       */
+  double gammamaxrad, eradfloor;       /* GAMMAMAXRAD, ERADFLOOR                  */
+  double gammasmalllimit, numepsilon;  /* GAMMASMALLLIMIT, NUMEPSILON             */
+  double eps, conv, entrconv, maxiter; /* RADIMPEPS, RADIMPCONV, RADIMPENTRCONV,  */
+                                       /* RADIMPMAXITER                           */
+  double dampfac, maxdown, maxup;      /* RADIMPLICITDAMPINGFACTOR,               */
+                                       /* RADIMPLICITMAXENCHANGEDOWN/UP           */
+  double maxdamping, threshold;        /* MAXRADIMPDAMPING, RADIMPLICITTHRESHOLD  */
+  double u2pconv;                      /* U2PCONV of the nested MHD inversion     */
+} kgpu_rad_params;
+
+/* KORAL's defaults (choices.h:320-597, ko.h:17-48) for a black hole of
+ * `mass` solar masses, adiabatic index gamma and the given opacity law. */
+int kgpu_rad_default_params(kgpu_rad_params *rp, double mass, double gamma, double kramers, double kes);
+
+/* Solver variants of kgpu_rad_implicit_cells. */
+#define KGPU_RAD_PLAIN 0    /* one thread runs a cell's whole cascade        */
+#define KGPU_RAD_BATCHED 1  /* passes over a work queue of unfinished cells  */
+
+/* Batched solve_implicit_lab (rad.c:1225-1570): for each of n cells, the
+ * conserved state uu after the explicit update, the primitive guess pp,
+ * its metric point and time step dt; the cascade of 4D Newton solves
+ * (energy equation on the dominant then the other component, lab then
+ * fluid frame, then the entropy equation) runs until one converges to the
+ * residual RADIMPCONV.  Outputs: primitives and conserved variables
+ * (unchanged inputs where all attempts fail), status (0 or -1 as
+ * solve_implicit_lab returns), the attempt that succeeded (0..5, -1) and
+ * its Newton iterations.  Host pointers. */
+int kgpu_rad_implicit_cells(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
+                            const double *G, const double *dt, double *pp_out, double *uu_out, int *status,
+                            int *attempt, int *iters, int mode);
+/* The same on device pointers, asynchronously on `stream` (a cudaStream_t,
+ * or null for the default stream).  stats, when not null, receives after
+ * completion: [0] Newton iterations over all attempts, [1] passes run.
+ * Temporary device memory of the batched variant is taken from `work`,
+ * which must hold kgpu_rad_work_bytes(n) bytes (null for the plain one). */
+size_t kgpu_rad_work_bytes(int n);
+int kgpu_rad_implicit_cells_device(int n, const kgpu_rad_params *rp, const double *uu, const double *pp,
+                                   const double *g, const double *G, const double *dt, double *pp_out,
+                                   double *uu_out, int *status, int *attempt, int *iters, int mode, void *work,
+                                   void *stream, unsigned long long *stats);
+/* Tuning of the batched form: Newton iterations a cell may take per pass
+ * (default 8; results do not depend on it).  Process-wide. */
+int kgpu_rad_set_pass_iters(int k);
+/* M1 closure u2p_rad (u2prad.c:485) and p2u (p2u.c:40) of n cells, host
+ * pointers; corrected[i] is u2p_rad's corrected flag. */
+int kgpu_rad_u2p_cells(int n, const kgpu_rad_params *rp, const double *uu, double *pp, const double *g,
+                       const double *G, int *status, int *corrected);
+int kgpu_rad_p2u_cells(int n, const kgpu_rad_params *rp, const double *pp, double *uu, const double *g,
+                       const double *G);
+/* Kerr-Schild metric point (r, theta) of spin a in the 20 + 20 layout
+ * (g_{mu nu}, d ln sqrt(-g)/dx^i, sqrt(-g); g^{mu nu}, g_tt + 1).  Host. */
+int kgpu_ks_metric(double a, double r, double th, double *g20, double *G20);
+int kgpu_ks_metric_batch(double a, int n, const double *r, const double *th, double *g20, double *G20);
+/* Measured FP64 issue rate of this GPU (DMUL + DADD per second, no FMA
+ * contraction, as the library's kernels are built): the denominator of the
+ * FP64 roofline of the solver kernels. */
+int kgpu_fp64_peak(double *ops_per_s);
+
 /* Last CUDA error string of this thread's most recent failing call. */
 const char *kgpu_last_error(void);
 int kgpu_abi_version(void);

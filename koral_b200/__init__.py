@@ -25,6 +25,14 @@ ARR_U, ARR_P, ARR_UT0, ARR_UT1 = 0, 1, 2, 3
 _dp = ctypes.POINTER(ctypes.c_double)
 
 
+class RadParams(ctypes.Structure):
+    """kgpu_rad_params (include/koral_b200.h)."""
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "gamma", "kb", "mp", "sigma", "mu", "ggg", "ccc", "masscm", "kramers", "kes", "kes_gu", "gammamaxrad",
+        "eradfloor", "gammasmalllimit", "numepsilon", "eps", "conv", "entrconv", "maxiter", "dampfac", "maxdown",
+        "maxup", "maxdamping", "threshold", "u2pconv")]
+
+
 class KgpuError(RuntimeError):
     pass
 
@@ -120,6 +128,20 @@ def lib():
         L.kgpu_profile_reset.argtypes = [vp]
         L.kgpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
         L.kgpu_last_error.restype = ctypes.c_char_p
+        ip_ = ctypes.POINTER(ctypes.c_int)
+        rpp = ctypes.POINTER(RadParams)
+        L.kgpu_rad_default_params.argtypes = [rpp] + [ctypes.c_double] * 4
+        L.kgpu_rad_implicit_cells.argtypes = [ctypes.c_int, rpp] + [_dp] * 7 + [ip_] * 3 + [ctypes.c_int]
+        L.kgpu_rad_implicit_cells_device.argtypes = [ctypes.c_int, rpp] + [vp] * 10 + [ctypes.c_int, vp, vp,
+                                                     ctypes.POINTER(ctypes.c_ulonglong)]
+        L.kgpu_rad_work_bytes.argtypes = [ctypes.c_int]
+        L.kgpu_rad_work_bytes.restype = ctypes.c_size_t
+        L.kgpu_rad_u2p_cells.argtypes = [ctypes.c_int, rpp] + [_dp] * 4 + [ip_] * 2
+        L.kgpu_rad_p2u_cells.argtypes = [ctypes.c_int, rpp] + [_dp] * 4
+        L.kgpu_rad_set_pass_iters.argtypes = [ctypes.c_int]
+        L.kgpu_ks_metric.argtypes = [ctypes.c_double] * 3 + [_dp] * 2
+        L.kgpu_ks_metric_batch.argtypes = [ctypes.c_double, ctypes.c_int] + [_dp] * 4
+        L.kgpu_fp64_peak.argtypes = [_dp]
         L.kgpu_u2p_cells_static.argtypes = sig["kgpu_u2p_cells"]
         L.kgpu_u2p_cells_static.restype = ctypes.c_int
         L.kgpu_u2p_cells_static_error.restype = ctypes.c_char_p
@@ -449,3 +471,125 @@ def fm_torus_state(tp, cfg, xb, g, G):
                                      _ptr(np.ascontiguousarray(g)), _ptr(np.ascontiguousarray(G)), _ptr(u), _ptr(p)),
            "kgpu_fm_torus_state")
     return u, p
+
+
+# ---------------------------------------------------------------------------
+# radiation: per-cell implicit gas-radiation source solve
+# ---------------------------------------------------------------------------
+RAD_PLAIN, RAD_BATCHED = 0, 1
+NVR = 13
+
+
+def rad_params(mass=10.0, gamma=13.0 / 9.0, kramers=6.4e22, kes=0.34):
+    """Constants and solver controls (KORAL's defaults) for a black hole of
+    `mass` solar masses and a Kramers + electron-scattering opacity law."""
+    rp = RadParams()
+    _check(lib().kgpu_rad_default_params(ctypes.byref(rp), mass, gamma, kramers, kes), "kgpu_rad_default_params")
+    return rp
+
+
+def _cells(*arrs):
+    return [np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
+
+
+def rad_implicit_cells(rp, uu, pp, g, G, dt, mode=RAD_BATCHED):
+    """solve_implicit_lab (rad.c:1225) on n independent cells; returns
+    (pp, uu, status, attempt, iters)."""
+    uu, pp, g, G, dt = _cells(uu, pp, g, G, dt)
+    n = uu.shape[0]
+    po, uo = np.zeros_like(pp), np.zeros_like(uu)
+    st, at, it = (np.zeros(n, dtype=np.int32) for _ in range(3))
+    ip = ctypes.POINTER(ctypes.c_int)
+    _check(lib().kgpu_rad_implicit_cells(n, ctypes.byref(rp), _ptr(uu), _ptr(pp), _ptr(g), _ptr(G), _ptr(dt),
+                                         _ptr(po), _ptr(uo), st.ctypes.data_as(ip), at.ctypes.data_as(ip),
+                                         it.ctypes.data_as(ip), mode), "kgpu_rad_implicit_cells")
+    return po, uo, st, at, it
+
+
+def rad_u2p_cells(rp, uu, pp, g, G):
+    """u2p_rad (u2prad.c:485) on n cells; returns (pp, status, corrected)."""
+    uu, pp, g, G = _cells(uu, pp, g, G)
+    pp = pp.copy()
+    n = uu.shape[0]
+    st, co = np.zeros(n, dtype=np.int32), np.zeros(n, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    _check(lib().kgpu_rad_u2p_cells(n, ctypes.byref(rp), _ptr(uu), _ptr(pp), _ptr(g), _ptr(G),
+                                    st.ctypes.data_as(ip), co.ctypes.data_as(ip)), "kgpu_rad_u2p_cells")
+    return pp, st, co
+
+
+def rad_p2u_cells(rp, pp, g, G):
+    """p2u (p2u.c:40) of the 13-variable state on n cells."""
+    pp, g, G = _cells(pp, g, G)
+    uu = np.zeros_like(pp)
+    _check(lib().kgpu_rad_p2u_cells(pp.shape[0], ctypes.byref(rp), _ptr(pp), _ptr(uu), _ptr(g), _ptr(G)),
+           "kgpu_rad_p2u_cells")
+    return uu
+
+
+def ks_metric(a, r, th):
+    """Kerr-Schild metric point in the 20 + 20 layout."""
+    g20, G20 = np.zeros(20), np.zeros(20)
+    _check(lib().kgpu_ks_metric(a, r, th, _ptr(g20), _ptr(G20)), "kgpu_ks_metric")
+    return g20, G20
+
+
+def rad_cell_draws(n, seed, rp, metric=None, spin=0.9):
+    """Random radiating cells around a Kerr black hole: r log-uniform in
+    [2, 100] M, theta uniform in [0.1, pi - 0.1]; log-uniform rho in
+    [1e-8, 1], gas temperature in [1e4, 1e12] K, E_rad/rho in [1e-10, 1e2]
+    and optical depth per cell in [1e-3, 1e5]; gas Lorentz factor
+    log-uniform in [1, 20] and radiation flux fraction uniform in [0, 0.99],
+    each in an isotropic direction.  Returns (pp, g, G, tau) with the entropy
+    slot of pp left for the caller (it goes with the conserved variables).
+    `metric(r, th)` gives the metric point (default: the product's
+    Kerr-Schild metric)."""
+    rng = np.random.default_rng(seed)
+    r = np.exp(rng.uniform(np.log(2.), np.log(100.), n))
+    th = rng.uniform(0.1, np.pi - 0.1, n)
+    g20, G20 = np.zeros((n, 20)), np.zeros((n, 20))
+    if metric is None:
+        _check(lib().kgpu_ks_metric_batch(spin, n, _ptr(r), _ptr(th), _ptr(g20), _ptr(G20)), "kgpu_ks_metric_batch")
+    else:
+        for k in range(n):
+            g20[k], G20[k] = metric(r[k], th[k])
+    rho = 10 ** rng.uniform(-8, 0, n)
+    T = 10 ** rng.uniform(4, 12, n)
+    u = rp.kb * rho * T / rp.mu / rp.mp / (rp.gamma - 1.)
+    Erf = 10 ** rng.uniform(-10, 2, n) * rho
+
+    def direction(norm2):
+        d = rng.normal(size=(n, 3))
+        d /= np.linalg.norm(d, axis=1)[:, None]
+        v = d / np.sqrt(np.stack([g20[:, 6], g20[:, 12], g20[:, 18]], 1))
+        vgv = np.einsum('ni,nij,nj->n', v, g20.reshape(n, 4, 5)[:, 1:4, 1:4], v)
+        return v * np.sqrt(norm2 / vgv)[:, None]
+
+    gam = np.exp(rng.uniform(0., np.log(20.), n))
+    ug = direction(gam ** 2 - 1.)
+    f = rng.uniform(0., 0.99, n)
+    vr = np.where(f > 0, (4. - np.sqrt(16. - 12. * f * f)) / (2. * np.maximum(f, 1e-300)), 0.)
+    ur = direction(vr * vr / (1. - vr * vr))
+    pp = np.zeros((n, NVR))
+    pp[:, 0], pp[:, 1], pp[:, 2:5], pp[:, 9], pp[:, 10:13] = rho, u, ug, Erf, ur
+    tau = 10 ** rng.uniform(-3, 5, n)
+    return pp, g20, G20, tau
+
+
+def rad_cells(n, seed, rp, spin=0.9, metric=None):
+    """rad_cell_draws completed with the product's own p2u: entropy, conserved
+    variables, and dt = 0.5 dx with dx = tau / (kappa_abs + kappa_es) (the
+    light-crossing CFL step of a cell of that optical depth).  Returns
+    (uu, pp, g, G, dt)."""
+    pp, g20, G20, tau = rad_cell_draws(n, seed, rp, metric=metric, spin=spin)
+    gm1 = rp.gamma - 1.
+    idx = 1. / gm1
+    pp[:, 5] = pp[:, 0] * np.log((gm1 * pp[:, 1]) ** idx / pp[:, 0] ** (idx + 1.))
+    uu = rad_p2u_cells(rp, pp, g20, G20)
+    T = pp[:, 1] * gm1 / (rp.kb * pp[:, 0] / rp.mu / rp.mp)
+    rhocgs = pp[:, 0] / rp.ggg * rp.ccc * rp.ccc / rp.masscm / rp.masscm
+    kabs = rp.kramers * rhocgs * T ** -3.5 / rp.ggg * rp.ccc * rp.ccc / rp.masscm * pp[:, 0]
+    kes = rp.kes_gu * pp[:, 0]
+    dt = 0.5 * tau / (kabs + kes)
+    return uu, pp, g20, G20, dt
+

@@ -427,3 +427,32 @@ extern "C" int kgpu_default_torus_params(kgpu_torus_params *tp) {
   tp->maxbeta = 0.01;
   return 0;
 }
+
+extern "C" int kgpu_ks_metric(double a, double r, double th, double *g20, double *G20) {
+  if (!g20 || !G20 || !(r > 0.)) return KGPU_EINVAL;
+  KSPoint k;
+  ks_point(a, r, th, k);
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      g20[i * 5 + j] = k.g[i][j];
+      G20[i * 5 + j] = k.G[i][j];
+    }
+  double s = sin(th), c = cos(th), Sig = r * r + a * a * c * c;
+  g20[0 * 5 + 4] = 2. * r / Sig;                          // d ln(Sigma sin) / dr
+  g20[1 * 5 + 4] = -2. * a * a * c * s / Sig + c / s;     // d ln(Sigma sin) / dtheta
+  g20[2 * 5 + 4] = 0.;
+  g20[3 * 5 + 4] = k.gdet;
+  G20[0 * 5 + 4] = G20[1 * 5 + 4] = G20[2 * 5 + 4] = 0.;
+  G20[3 * 5 + 4] = 2. * r / Sig;                          // g_tt + 1
+  return 0;
+}
+
+extern "C" int kgpu_ks_metric_batch(double a, int n, const double *r, const double *th, double *g20, double *G20) {
+  if (n < 0 || (n > 0 && (!r || !th || !g20 || !G20))) return KGPU_EINVAL;
+  for (int k = 0; k < n; k++) {
+    int e = kgpu_ks_metric(a, r[k], th[k], g20 + 20L * k, G20 + 20L * k);
+    if (e) return e;
+  }
+  return 0;
+}
+

@@ -6,7 +6,10 @@ Two CPU implementations of KORAL's hot path are reachable from here:
   size and scheme), built by ``oracle/Makefile`` into
   ``oracle/_ref/libkoral_oracle.so``;
 * ``RefKoral`` drives the reference KORAL sources themselves, compiled per
-  problem by ``oracle/ref/build_ref.sh`` into ``oracle/_ref/libkref_*.so``.
+  problem by ``oracle/ref/build_ref.sh`` into ``oracle/_ref/libkref_*.so``;
+* ``RefRadCells`` calls the reference's per-cell radiation routines (M1
+  closure, implicit source solve) on independent cells of the radiating-cells
+  build.
 
 Only the tests, the smoke check and the CPU-baseline leg of the benchmark use
 this module; the product never imports it.
@@ -21,6 +24,17 @@ REF_DIR = os.path.join(HERE, "_ref")
 ORACLE_LIB = os.path.join(REF_DIR, "libkoral_oracle.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def _p(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_ip)
 
 
 def _lib(path):
@@ -208,3 +222,54 @@ class RefKoral:
 
     def set_scalar(self, name, v):
         ctypes.c_double.in_dll(self.L, name).value = v
+
+
+class RefRadCells:
+    """The reference's per-cell radiation routines on independent cells
+    (RADCELLS build, oracle/ref/harness.c): metric points, conserved
+    variables and opacities of given primitives, u2p_rad and the implicit
+    source solve solve_implicit_lab (rad.c:1225-1570)."""
+
+    def __init__(self, libname="libkref_radcells.so"):
+        self.L = _lib(os.path.join(REF_DIR, libname))
+        self.L.kref_init()
+        c = np.zeros(32)
+        self.L.kref_rad_consts(_p(c))
+        self.consts = c
+        self.batch = int(c[24])
+
+    def metric(self, r, th):
+        g20, G20 = np.zeros(20), np.zeros(20)
+        xx = np.array([0., r, th, 0.])
+        self.L.kref_metric_at(_p(xx), _p(g20), _p(G20))
+        return g20, G20
+
+    def prepare(self, pp, g, G):
+        """Sets the entropy slot of pp (in place); returns (uu, kappa_abs, kappa_es)."""
+        n = pp.shape[0]
+        uu, kap = np.zeros_like(pp), np.zeros((n, 2))
+        self.L.kref_rad_prepare(n, _p(pp), _p(g), _p(G), _p(uu), _p(kap))
+        return uu, kap[:, 0], kap[:, 1]
+
+    def u2p(self, uu, pp, g, G):
+        n = uu.shape[0]
+        pp = pp.copy()
+        st, co = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        self.L.kref_rad_u2p(n, _p(uu), _p(pp), _p(g), _p(G), _i(st), _i(co))
+        return pp, st, co
+
+    # counter slot of the successful attempt -> (primitives, equation, frame)
+    SLOTS = {0: ("RAD", "energy", "lab"), 13: ("RAD", "energy", "ff"), 2: ("MHD", "energy", "lab"),
+             14: ("MHD", "energy", "ff"), 4: ("RAD", "entropy", "lab"), 6: ("MHD", "entropy", "lab")}
+
+    def implicit(self, uu, pp, g, G, dt):
+        """Returns (pp, uu, status, slot, iters); slot keys SLOTS (-1: all failed)."""
+        n = uu.shape[0]
+        po, uo = np.zeros_like(pp), np.zeros_like(uu)
+        st, wh, it = (np.zeros(n, np.int32) for _ in range(3))
+        for s in range(0, n, self.batch):
+            m = min(self.batch, n - s)
+            self.L.kref_rad_implicit(m, _p(uu[s:]), _p(pp[s:]), _p(g[s:]), _p(G[s:]), _p(dt[s:]), _p(po[s:]),
+                                     _p(uo[s:]), _i(st[s:]), _i(wh[s:]), _i(it[s:]))
+        return po, uo, st, wh, it
+

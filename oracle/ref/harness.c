@@ -260,3 +260,178 @@ int kref_physics(double *out)
 #endif
   return 10;
 }
+
+#ifdef RADIATION
+/* ---------------------------------------------------------------------
+ * Per-cell radiation entry points (RADCELLS build).  Independent cells are
+ * stored in the domain (cell k at ix = k % NX, iy = k / NX, iz = 0), each
+ * with its own metric written into the reference's metric tables, and the
+ * reference's solve_implicit_lab (rad.c:1225-1570) is called on each.
+ * --------------------------------------------------------------------- */
+
+/* Unit constants and solver parameters of this build, in code units. */
+int kref_rad_consts(double *out)
+{
+  out[0] = K_BOLTZ;
+  out[1] = M_PROTON;
+  out[2] = SIGMA_RAD;
+  out[3] = MU_GAS;
+  out[4] = GGG;
+  out[5] = CCC;
+  out[6] = MASSCM;
+  out[7] = GAMMAMAXRAD;
+  out[8] = ERADFLOOR;
+  out[9] = RADIMPEPS;
+  out[10] = RADIMPCONV;
+  out[11] = RADIMPENTRCONV;
+  out[12] = RADIMPMAXITER;
+  out[13] = RADIMPLICITDAMPINGFACTOR;
+  out[14] = RADIMPLICITMAXENCHANGEDOWN;
+  out[15] = RADIMPLICIMAXENCHANGEUP;
+  out[16] = MAXRADIMPDAMPING;
+  out[17] = RADIMPLICITTHRESHOLD;
+  out[18] = GAMMASMALLLIMIT;
+  out[19] = NUMEPSILON;
+  out[20] = EERHORATIOMIN;
+  out[21] = EERHORATIOMAX;
+  out[22] = EEUURATIOMIN;
+  out[23] = EEUURATIOMAX;
+  out[24] = NX * NY;
+  return 25;
+}
+
+/* The metric of the build's coordinates at xx[4], laid out as one cell of
+ * the metric tables (calc_metric, metric.c:3900-3920). */
+int kref_metric_at(const double *xx, double *g20, double *G20)
+{
+  ldouble x[4] = {xx[0], xx[1], xx[2], xx[3]}, gl[4][5];
+  int i, j;
+  calc_g(x, gl);
+  for (i = 0; i < 4; i++)
+    for (j = 0; j < 4; j++) g20[i * 5 + j] = gl[i][j];
+  for (j = 0; j < 3; j++) g20[j * 5 + 4] = calc_dlgdet(x, j);
+  g20[3 * 5 + 4] = calc_gdet(x);
+  calc_G(x, gl);
+  for (i = 0; i < 4; i++)
+    for (j = 0; j < 4; j++) G20[i * 5 + j] = gl[i][j];
+  for (j = 0; j < 3; j++) G20[j * 5 + 4] = 0.;
+  G20[3 * 5 + 4] = calc_gttpert(x);
+  return 0;
+}
+
+static void kref_geom_from(const double *g20, const double *G20, struct geometry *geom)
+{
+  int i, j;
+  memset(geom, 0, sizeof(*geom));
+  for (i = 0; i < 4; i++)
+    for (j = 0; j < 5; j++) {
+      geom->gg[i][j] = g20[i * 5 + j];
+      geom->GG[i][j] = G20[i * 5 + j];
+    }
+  geom->alpha = sqrt(-1. / geom->GG[0][0]);
+  geom->gdet = geom->gg[3][4];
+  geom->gttpert = geom->GG[3][4];
+  geom->ifacedim = -1;
+  geom->par = -1;
+  geom->coords = MYCOORDS;
+}
+
+/* Entropy primitive from (rho, u) and the conserved variables (p2u.c:40),
+ * n cells of NV primitives each; opacities (calc_kappa, calc_kappaes) of
+ * each cell go to kap[2k], kap[2k+1]. */
+int kref_rad_prepare(int n, double *pp, const double *g20, const double *G20, double *uu, double *kap)
+{
+  int k;
+  for (k = 0; k < n; k++) {
+    struct geometry geom;
+    kref_geom_from(g20 + 20 * k, G20 + 20 * k, &geom);
+    double *p1 = pp + (long)k * NV;
+    p1[ENTR] = calc_Sfromu(p1[RHO], p1[UU]);
+    p2u(p1, uu + (long)k * NV, &geom);
+    ldouble k1, k2, k3, k4;
+    kap[2 * k] = calc_kappa(p1, &geom, &k1, &k2, &k3, &k4);
+    kap[2 * k + 1] = calc_kappaes(p1, &geom);
+  }
+  return 0;
+}
+
+static void kref_rad_load(int k, const double *uu, const double *pp, const double *g20, const double *G20)
+{
+  int ix = k % NX, iy = k / NX, i, j, iv;
+  for (i = 0; i < 4; i++)
+    for (j = 0; j < 5; j++) {
+      set_g(g, i, j, ix, iy, 0, g20[20 * k + i * 5 + j]);
+      set_g(G, i, j, ix, iy, 0, G20[20 * k + i * 5 + j]);
+    }
+  for (iv = 0; iv < NV; iv++) {
+    set_u(u, iv, ix, iy, 0, uu[(long)k * NV + iv]);
+    set_u(p, iv, ix, iy, 0, pp[(long)k * NV + iv]);
+  }
+}
+
+/* solve_implicit_lab on n <= NX*NY cells, one after another.  Outputs per
+ * cell: the primitives and conserved left in the reference's arrays, the
+ * return value, which attempt succeeded (the index of the global counter
+ * slot it incremented: 0 RAD energy lab, 13 RAD energy fluid frame, 2 MHD
+ * energy lab, 14 MHD energy fluid frame, 4 RAD entropy, 6 MHD entropy; -1
+ * when all failed) and the Newton iterations of the successful attempt. */
+int kref_rad_implicit(int n, const double *uu, const double *pp, const double *g20, const double *G20,
+                      const double *dtc, double *pp_out, double *uu_out, int *status, int *which, int *iters)
+{
+  int k, s, iv;
+  if (n > NX * NY) return -1;
+  for (k = 0; k < n; k++) {
+    int ix = k % NX, iy = k / NX;
+    int before[NGLOBALINTSLOT];
+    ldouble deltas[5];
+    kref_rad_load(k, uu, pp, g20, G20);
+    for (s = 0; s < NGLOBALINTSLOT; s++) before[s] = global_int_slot[s];
+    status[k] = solve_implicit_lab(ix, iy, 0, dtc[k], deltas, 0);
+    which[k] = -1;
+    iters[k] = 0;
+    const int succ[6] = {GLOBALINTSLOT_NIMPENERRAD, GLOBALINTSLOT_NIMPENERRADFF, GLOBALINTSLOT_NIMPENERMHD,
+                         GLOBALINTSLOT_NIMPENERMHDFF, GLOBALINTSLOT_NIMPENTRRAD, GLOBALINTSLOT_NIMPENTRMHD};
+    for (s = 0; s < 6; s++)
+      if (global_int_slot[succ[s]] != before[succ[s]]) which[k] = succ[s];
+    const int its[4] = {GLOBALINTSLOT_ITERIMPENERRAD, GLOBALINTSLOT_ITERIMPENERMHD, GLOBALINTSLOT_ITERIMPENTRRAD,
+                        GLOBALINTSLOT_ITERIMPENTRMHD};
+    for (s = 0; s < 4; s++) iters[k] += global_int_slot[its[s]] - before[its[s]];
+    for (iv = 0; iv < NV; iv++) {
+      pp_out[(long)k * NV + iv] = get_u(p, iv, ix, iy, 0);
+      uu_out[(long)k * NV + iv] = get_u(u, iv, ix, iy, 0);
+    }
+  }
+  return 0;
+}
+
+/* u2p_rad (u2prad.c:485) on n cells with their own metric points. */
+int kref_rad_u2p(int n, const double *uu, double *pp, const double *g20, const double *G20, int *status, int *corr)
+{
+  int k;
+  for (k = 0; k < n; k++) {
+    struct geometry geom;
+    int c[3] = {0, 0, 0};
+    kref_geom_from(g20 + 20 * k, G20 + 20 * k, &geom);
+    status[k] = u2p_rad((double *)uu + (long)k * NV, pp + (long)k * NV, &geom, c);
+    corr[k] = c[0];
+  }
+  return 0;
+}
+
+/* The same solves for CPU timing: all cells loaded first, then solved in an
+ * OpenMP loop when the build has OpenMP (the reference's counters are then
+ * updated without synchronisation, as in its own parallel loops). */
+int kref_rad_implicit_timed(int n, const double *uu, const double *pp, const double *g20, const double *G20,
+                            const double *dtc, int *status)
+{
+  int k;
+  if (n > NX * NY) return -1;
+  for (k = 0; k < n; k++) kref_rad_load(k, uu, pp, g20, G20);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (k = 0; k < n; k++) {
+    ldouble deltas[5];
+    status[k] = solve_implicit_lab(k % NX, k / NX, 0, dtc[k], deltas, 0);
+  }
+  return 0;
+}
+#endif
