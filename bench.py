@@ -47,7 +47,15 @@ WORKLOADS = {
     "ot128": dict(desc="relativistic Orszag-Tang vortex 128x128 (Minkowski, PPM+LLF+flux-CT, RK2, CFL 0.5, Gamma 5/3)",
                   shape=(128, 128, 1), ref_lib="libkref_orszagrel_128_omp.so", ref_serial="libkref_orszagrel_128.so",
                   ref_sample_steps=40),
+    "radcells": dict(desc="batched implicit gas-radiation source solve, 2^22 independent cells (Kerr-Schild a=0.9, "
+                          "r log-U[2,100] M, theta U[0.1,pi-0.1], log-U rho [1e-8,1], T [1e4,1e12] K, "
+                          "E_rad/rho [1e-10,1e2], tau [1e-3,1e5], gas Lorentz factor [1,20], flux fraction [0,0.99], "
+                          "Kramers + electron scattering, M = 10 Msun, Gamma 13/9, Newton to 1e-10, seed 2026)",
+                     ncells=1 << 22, ref_lib="libkref_radcells_omp.so", ref_serial="libkref_radcells.so",
+                     ref_sample_cells=1 << 17),
 }
+RAD_METRIC = "implicit solves/s (1 B200)"
+RAD_UNIT = "solves/s"
 
 
 def make_subdomain(kgpu, name):
@@ -147,15 +155,73 @@ def run_reference_cpu(wl, steps, warm, threads):
     return d["cells"] * d["steps"] / d["seconds"], None
 
 
+RAD_REF_CHILD = r"""
+import json, sys, time
+import numpy as np
+sys.path.insert(0, {root!r})
+import koral_b200 as k
+from oracle.koral_oracle import RefRadCells, _p, _i
+R = RefRadCells({lib!r})
+rp = k.rad_params()
+pp, g, G, tau = k.rad_cell_draws({n}, 2026, rp)
+uu, kabs, kes = R.prepare(pp, g, G)
+dt = 0.5 * tau / (kabs + kes)
+st = np.zeros({n}, np.int32)
+B = R.batch
+t0 = time.perf_counter()
+for s in range(0, {n}, B):
+    m = min(B, {n} - s)
+    R.L.kref_rad_implicit_timed(m, _p(uu[s:]), _p(pp[s:]), _p(g[s:]), _p(G[s:]), _p(dt[s:]), _i(st[s:]))
+t1 = time.perf_counter()
+print(json.dumps({{"seconds": t1 - t0, "cells": {n}, "ok": float(np.mean(st == 0))}}))
+"""
+
+
+def run_reference_radcells(wl, ncells, threads):
+    lib = wl["ref_lib"] if threads > 1 else wl["ref_serial"]
+    path = os.path.join(ROOT, "oracle", "_ref", lib)
+    if not os.path.exists(path):
+        return None, f"{lib} not built (needs the reference tree at build time)"
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    code = RAD_REF_CHILD.format(root=ROOT, lib=lib, n=ncells)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=1800)
+    line = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    if r.returncode != 0 or not line:
+        return None, (r.stderr or r.stdout)[-300:]
+    d = json.loads(line[-1])
+    return d["cells"] / d["seconds"], None
+
+
 def cells_of(wl):
     nx, ny, nz = wl["shape"]
     return nx * ny * nz
+
+
+def reference_arm_radcells(args, wl, threads):
+    n = wl["ref_sample_cells"]
+    val, err = run_reference_radcells(wl, n, threads)
+    if val is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    line = {
+        "metric": RAD_METRIC, "value": val, "unit": RAD_UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wl["ncells"] / val * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["desc"], "parallelism": "openmp host threads"},
+        "cpu_baseline": {"value": val, "unit": RAD_UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{n} cells of the same distribution, one solve_implicit_lab each"},
+        "e2e": {"value": val, "unit": RAD_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
 
 
 def reference_arm(args, wl, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    if "ncells" in wl:
+        reference_arm_radcells(args, wl, threads)
+        return
     # one full RK2 step of the reference on all host cores per step, at most
     # ref_sample_steps of them (a full-size CPU step takes seconds)
     nsteps = max(1, min(args.steps, wl["ref_sample_steps"]))
@@ -322,6 +388,133 @@ def our_arm(args, wl, rank, world, local_rank):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------------------
+# our arm, batched implicit solve
+# ---------------------------------------------------------------------------
+def our_arm_radcells(args, wl, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import koral_b200 as k
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    from koral_b200 import build
+    build.build()
+    L = k.lib()
+    n = wl["ncells"]
+    rp = k.rad_params()
+    uu, pp, g, G, dt = k.rad_cells(n, 2026 + rank, rp)
+    # inputs resident in HBM (2.2 GB, larger than L2)
+    d_in = [torch.from_numpy(a).to(dev) for a in (uu, pp, g, G, dt)]
+    d_po = torch.empty((n, 13), dtype=torch.float64, device=dev)
+    d_uo = torch.empty((n, 13), dtype=torch.float64, device=dev)
+    d_st, d_at, d_it = (torch.empty(n, dtype=torch.int32, device=dev) for _ in range(3))
+    work = torch.empty(int(L.kgpu_rad_work_bytes(n)), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    vp = ctypes.c_void_p
+
+    def solve(mode, stats=None):
+        ptrs = [vp(t.data_ptr()) for t in d_in] + [vp(d_po.data_ptr()), vp(d_uo.data_ptr()), vp(d_st.data_ptr()),
+                                                   vp(d_at.data_ptr()), vp(d_it.data_ptr())]
+        k._check(L.kgpu_rad_implicit_cells_device(n, ctypes.byref(rp), *ptrs, mode, vp(work.data_ptr()),
+                                                  vp(stream.cuda_stream), stats), "kgpu_rad_implicit_cells_device")
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        dist = dist_
+
+    def timed(mode, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in ev:
+            a.record(stream)
+            solve(mode)
+            b.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = sum(a.elapsed_time(b) for a, b in ev)
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        solve(k.RAD_BATCHED)
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    with ClockSampler(local_rank) as clk:
+        ms = timed(k.RAD_BATCHED, args.steps)
+    value = n * args.steps * world / (ms / 1e3)
+    # the plain one-thread-per-cell form on the same cells, for comparison
+    steps_plain = max(1, min(3, args.steps))
+    ms_plain = timed(k.RAD_PLAIN, steps_plain)
+    plain_value = n * steps_plain * world / (ms_plain / 1e3)
+    # iteration statistics of one batched solve
+    stats = (ctypes.c_ulonglong * 2)()
+    solve(k.RAD_BATCHED, stats)
+    st = d_st.cpu().numpy()
+    it = d_it.cpu().numpy()
+    at = d_at.cpu().numpy()
+    peak = ctypes.c_double()
+    k._check(L.kgpu_fp64_peak(ctypes.byref(peak)), "kgpu_fp64_peak")
+
+    # e2e: the host-pointer entry point with pinned buffers, copies included
+    hin = []
+    for a in (uu, pp, g, G, dt):
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        hin.append(t)
+    hpo = torch.empty((n, 13), dtype=torch.float64, pin_memory=True)
+    huo = torch.empty((n, 13), dtype=torch.float64, pin_memory=True)
+    hst, hat, hit = (torch.empty(n, dtype=torch.int32, pin_memory=True) for _ in range(3))
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    ke = max(1, min(2, args.steps))
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        k._check(L.kgpu_rad_implicit_cells(n, ctypes.byref(rp), *[ctypes.cast(t.data_ptr(), dp) for t in hin],
+                                           ctypes.cast(hpo.data_ptr(), dp), ctypes.cast(huo.data_ptr(), dp),
+                                           ctypes.cast(hst.data_ptr(), ip), ctypes.cast(hat.data_ptr(), ip),
+                                           ctypes.cast(hit.data_ptr(), ip), k.RAD_BATCHED), "kgpu_rad_implicit_cells")
+    torch.cuda.synchronize(dev)
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = n * ke * world / float(t.item())
+    if rank != 0:
+        return
+    ok = st == 0
+    passes = (6 * 51 + 7) // 8 + 1   # pass launches of one batched solve at 8 iterations per pass
+    line = {
+        "metric": RAD_METRIC, "value": value, "unit": RAD_UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["desc"], "cells_per_gpu": n, "l2": "inputs 2.2 GB > L2, no flush",
+                   "parallelism": "replicas" if world > 1 else "one batch", "solver": "batched work queue"},
+        "plain": {"value": plain_value, "unit": RAD_UNIT, "ms_per_step": ms_plain / steps_plain},
+        "newton": {"mean_iterations_successful_attempt": float(it[ok].mean()),
+                   "mean_iterations_all_attempts": stats[0] / n, "passes_with_work": int(stats[1]),
+                   "success_rate": float(ok.mean()),
+                   "attempt_histogram": {int(a): int((at == a).sum()) for a in np.unique(at)}},
+        "roofline": {"kernel": "k_rad_pass", "bound": "fp64", "peak": peak.value / 1e12, "unit": "TFLOP/s",
+                     "peak_source": "measured live (DMUL+DADD chains, no FMA)", "achieved": None, "frac": None,
+                     "traffic": None},
+        "e2e": {"value": e2e_value, "unit": RAD_UNIT, "h2d_bytes_per_step": n * (13 + 13 + 20 + 20 + 1) * 8,
+                "d2h_bytes_per_step": n * (26 * 8 + 12)},
+        "gpu_launches": passes * args.steps,
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        val, err = run_reference_radcells(wl, wl["ref_sample_cells"], threads)
+        line["cpu_baseline"] = {"value": val, "unit": RAD_UNIT, "cores": threads, "kind": "reference",
+                                "sample": (f"{wl['ref_sample_cells']} cells of the same distribution"
+                                           if val is not None else f"unavailable: {err}")}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     wl = WORKLOADS[args.workload]
@@ -340,7 +533,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        our_arm(args, wl, rank, world, local_rank)
+        if "ncells" in wl:
+            our_arm_radcells(args, wl, rank, world, local_rank)
+        else:
+            our_arm(args, wl, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist
