@@ -11,12 +11,10 @@ transcendental functions besides sqrt).  u2p_rad uses pow(x, 2) in its
 closed forms; CUDA's pow and the host library's differ in the last place
 now and then, so the recovered primitives agree to 1e-12 relative.  The
 implicit solve iterates a Newton method whose residual calls pow (the
-Planck function, the Kramers law) and log (the entropy): last-place
-differences move the iterates slightly, so the attempt that succeeds, the
-iteration count and the converged state agree per cell except where a
-decision (convergence test, damping acceptance) sits on a knife edge.
-Compiled for the host with the host's libm, the same device code matches
-the reference bit for bit in every cell.
+Planck function, the Kramers law) and log (the entropy); it is held to the
+reference's own sensitivity to a one-ulp nudge of its input (see that
+test).  Compiled for the host with the host's libm, the same device code
+matches the reference bit for bit in every cell.
 """
 import numpy as np
 import pytest
@@ -65,22 +63,48 @@ def test_rad_u2p_matches_reference(kgpu, ref, cells):
     assert rel.max() <= 1e-12
 
 
+def scaled_difference(p, q):
+    """Per cell, the largest difference of the primitives of p from those of
+    q, each on the scale the solve controls it to: the densities relative to
+    themselves, the two energy densities relative to their sum (the residual
+    of the energy equation is normalised by both), each velocity relative to
+    its largest component."""
+    etot = np.abs(q[:, 1]) + np.abs(q[:, 9])
+    d = [np.abs(p[:, 0] - q[:, 0]) / np.abs(q[:, 0]),
+         np.abs(p[:, 1] - q[:, 1]) / etot,
+         np.abs(p[:, 9] - q[:, 9]) / etot,
+         np.abs(p[:, 2:5] - q[:, 2:5]).max(1) / np.maximum(np.abs(q[:, 2:5]).max(1), 1e-300),
+         np.abs(p[:, 10:13] - q[:, 10:13]).max(1) / np.maximum(np.abs(q[:, 10:13]).max(1), 1e-300)]
+    return np.max(d, axis=0)
+
+
 def test_rad_implicit_matches_reference(kgpu, ref, cells):
+    """The GPU agrees with the reference at least as well as the reference
+    agrees with itself when the gas energy of every cell is nudged by one
+    ulp: the implicit solve is ill-conditioned in part of this distribution
+    (a converged residual of 1e-10 leaves a small component, such as a cold
+    radiation field beside a hot gas, loosely pinned), so last-place
+    differences in pow and log move individual solutions by as much as the
+    nudge does.  Compared: success status, Newton iteration counts, and the
+    50/90/99% quantiles of the scaled difference of the primitives."""
     rp, uu, pp, g, G, dt = cells
     pr, ur, sr, wr, ir = ref.implicit(uu, pp, g, G, dt)
+    un = uu.copy()
+    un[:, 1] = np.nextafter(un[:, 1], np.inf)
+    pn, _, sn, _, inn = ref.implicit(un, pp, g, G, dt)
     pg, ug, sg, ag, ig = kgpu.rad_implicit_cells(rp, uu, pp, g, G, dt, mode=kgpu.RAD_BATCHED)
-    same = sg == sr
-    both = (sg == 0) & (sr == 0)
-    relmax = (np.abs(pg - pr) / (np.abs(pr) + 1e-300))[:, NONENT].max(axis=1)
-    print(f"status agree {same.mean():.5f}, both succeeded {both.sum()} of {len(sr)}, "
-          f"iterations agree {np.mean(ig[both] == ir[both]):.5f}, mean iterations reference "
-          f"{ir[sr == 0].mean():.3f} gpu {ig[sg == 0].mean():.3f}")
-    print("max relative difference of primitives, quantiles 50/90/99/99.9/100%:",
-          np.quantile(relmax[both], [0.5, 0.9, 0.99, 0.999, 1.0]), "bit-identical cells",
-          np.mean(relmax[both] == 0))
-    assert same.mean() >= 0.995
-    assert np.mean(ig[both] == ir[both]) >= 0.98
-    assert np.quantile(relmax[both], 0.99) <= 1e-8
+    q = [0.5, 0.9, 0.99]
+    bg, bn = (sg == 0) & (sr == 0), (sn == 0) & (sr == 0)
+    dg, dn = np.quantile(scaled_difference(pg[bg], pr[bg]), q), np.quantile(scaled_difference(pn[bn], pr[bn]), q)
+    agree = lambda a, b, m: np.mean(a[m] == b[m])
+    print(f"GPU vs reference: status agree {np.mean(sg == sr):.5f}, iterations agree {agree(ig, ir, bg):.4f}, "
+          f"difference quantiles 50/90/99% {dg}")
+    print(f"nudged reference: status agree {np.mean(sn == sr):.5f}, iterations agree {agree(inn, ir, bn):.4f}, "
+          f"difference quantiles 50/90/99% {dn}")
+    print(f"mean iterations: reference {ir[sr == 0].mean():.3f}, GPU {ig[sg == 0].mean():.3f}")
+    assert np.mean(sg == sr) >= np.mean(sn == sr) - 0.005
+    assert agree(ig, ir, bg) >= agree(inn, ir, bn) - 0.05
+    assert np.all(dg <= 10 * dn + 1e-12), (dg, dn)
     assert abs(ig[sg == 0].mean() - ir[sr == 0].mean()) <= 0.02 * ir[sr == 0].mean()
 
 
