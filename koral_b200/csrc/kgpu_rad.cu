@@ -11,6 +11,9 @@
 //    that finish leave the queue, so warps stay full of live work.  The
 //    iterations a cell takes are the same in both forms (the solve resumes
 //    exactly where it stopped), so both give the same results.
+// Both run the cascade as the one-evaluation state machine of
+// kgpu_rad.cuh (imp_advance), so the lanes of a warp perform their
+// expensive evaluations together whatever phase each cell is in.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -146,26 +149,21 @@ __global__ void __launch_bounds__(128) k_rad_plain(RadParams R, Cell C, int n, u
   RadGeom rg;
   rad_geom(C.g + 20L * k, C.G + 20L * k, rg);
   const double *u0 = C.uu + (long)k * NVR, *p0 = C.pp + (long)k * NVR;
-  const int sw = imp_startwith(R, p0, rg.g);
-  unsigned total = 0;
-  bool done = false;
-  for (int a = 0; a < IMP_NATTEMPTS && !done; a++) {
-    double pw[NVR], uw[NVR];
-    for (int i = 0; i < NVR; i++) pw[i] = p0[i];
-    int it = 0;
-    const int r = imp_solve(R, imp_attempt(a, sw), u0, p0, C.dt[k], rg, pw, uw, it, 1 << 30);
-    total += it;
-    if (r == 0) {
-      cell_success(R, C, k, rg, pw, a, it);
-      done = true;
-    }
+  const double dt = C.dt[k];
+  ImpState s;
+  imp_begin(R, p0, rg.g, s);
+  int budget = 1 << 30;
+  int r;
+  while ((r = imp_advance(R, u0, p0, dt, rg, s, budget)) == IMP_RUNNING) {
   }
-  if (!done) cell_failure(C, k);
-  if (stats) warp_add(stats, total);
+  if (r == IMP_DONE_OK) cell_success(R, C, k, rg, s.pp, s.att, s.iter);
+  else cell_failure(C, k);
+  if (stats) warp_add(stats, (unsigned)((1 << 30) - budget));
 }
 
-// Pass p of the batched form: cells of queue p (all cells in pass 0) get up
-// to K Newton iterations; unfinished ones go to queue p+1.
+// Pass p of the batched form: cells of queue p (all cells in pass 0) may
+// start up to K Newton iterations; unfinished ones keep their state (the
+// iterate, its iteration count, the attempt) and go to queue p+1.
 __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, int n, int p, int K) {
   const int nin = p == 0 ? n : W.count[p];
   const int *qin = W.q[p & 1];
@@ -175,51 +173,37 @@ __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, i
     RadGeom rg;
     rad_geom(C.g + 20L * k, C.G + 20L * k, rg);
     const double *u0 = C.uu + (long)k * NVR, *p0 = C.pp + (long)k * NVR;
-    double pw[NVR], uw[NVR];
-    int att, it, sw;
+    const double dt = C.dt[k];
+    ImpState s;
     if (p == 0) {
-      sw = imp_startwith(R, p0, rg.g);
-      W.wsw[k] = sw;
-      att = 0;
-      it = 0;
-      for (int i = 0; i < NVR; i++) pw[i] = p0[i];
+      imp_begin(R, p0, rg.g, s);
     } else {
-      sw = W.wsw[k];
-      att = W.watt[k];
-      it = W.wit[k];
-      for (int i = 0; i < NVR; i++) pw[i] = W.wpp[(long)k * NVR + i];
+      s.phase = PH_BASE;
+      s.j = 0;
+      s.sign = -1.;
+      s.xiapp = 1.;
+      s.evals = 0;
+      s.sw = W.wsw[k];
+      s.att = W.watt[k];
+      s.iter = W.wit[k];
+      for (int i = 0; i < NVR; i++) s.pp[i] = W.wpp[(long)k * NVR + i];
     }
     int budget = K;
-    unsigned used = 0;
-    bool finished = false;
-    while (budget > 0) {
-      const int before = it;
-      const int r = imp_solve(R, imp_attempt(att, sw), u0, p0, C.dt[k], rg, pw, uw, it, it + budget);
-      const int spent = it - before;
-      used += spent;
-      budget -= spent;
-      if (r == IMP_PAUSED) break;
-      if (r == 0) {
-        cell_success(R, C, k, rg, pw, att, it);
-        finished = true;
-        break;
-      }
-      // this attempt failed: the next one starts afresh from the guess
-      att++;
-      it = 0;
-      for (int i = 0; i < NVR; i++) pw[i] = p0[i];
-      if (att >= IMP_NATTEMPTS) {
-        cell_failure(C, k);
-        finished = true;
-        break;
-      }
+    int r;
+    while ((r = imp_advance(R, u0, p0, dt, rg, s, budget)) == IMP_RUNNING) {
     }
-    warp_add(W.stats, used);
-    warp_push(qout, W.count + p + 1, !finished, k);
-    if (!finished) {
-      W.watt[k] = att;
-      W.wit[k] = it;
-      for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = pw[i];
+    warp_add(W.stats, (unsigned)(K - budget));
+    const bool paused = r == IMP_PAUSE;
+    warp_push(qout, W.count + p + 1, paused, k);
+    if (paused) {
+      W.wsw[k] = s.sw;
+      W.watt[k] = s.att;
+      W.wit[k] = s.iter;
+      for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = s.pp[i];
+    } else if (r == IMP_DONE_OK) {
+      cell_success(R, C, k, rg, s.pp, s.att, s.iter);
+    } else {
+      cell_failure(C, k);
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && nin > 0) atomicAdd(W.stats + 1, 1ull);

@@ -419,26 +419,28 @@ KG_HD void imp_rho_from_velocity(const double *uu0, double *pp, const Geom &g) {
   pp[RHO] = (uu0[RHO]) / g.gdet / ucon[0];
 }
 
-// residual f[4] and its relative size (f_implicit_lab_4dprim, rad.c:110-351)
-KG_HD int f_implicit(const RadParams &R, const ImpParams &P, const double *ppin, const double *uu0, double *pp0,
-                     double dt, const RadGeom &rg, double f[4], double &err0) {
+// The part of every evaluation that precedes the residual (rad.c:130-198,
+// 880-960): the density that follows the gas velocity when iterating MHD
+// primitives, the entropy, the conserved state that goes with pp, and the
+// inversion of the other component (which updates pp in place).
+KG_HD int imp_prepare(const RadParams &R, const ImpParams &P, const double *uu0, double *pp, double *uu,
+                      const RadGeom &rg, int &corr) {
+  if (P.prim == IMP_MHD) imp_rho_from_velocity(uu0, pp, rg.g);
+  pp[ENTR] = rad_Sfromu(R, pp[RHO], pp[UU]);
+  return imp_counterpart(R, P.prim, uu0, pp, uu, rg, corr);
+}
+
+// residual f[4] and its relative size from a prepared state (the rest of
+// f_implicit_lab_4dprim, rad.c:199-351).  Returns -1 on failure, 1 when the
+// closure was corrected, else 0.
+KG_HD int imp_residual(const RadParams &R, const ImpParams &P, double *pp, const double *uu, const double *uu0,
+                       const double *pp00, double dt, const RadGeom &rg, int u2pret, int corr, double f[4],
+                       double &err0) {
   const Geom &g = rg.g;
   const double gdetu = g.gdet;
-  int ret = 0;
-  double uu[NVR], pp[NVR], err[4] = {0., 0., 0., 0.};
-  for (int i = 0; i < NVR; i++) pp[i] = ppin[i];
-  double ut[4] = {0., pp[2], pp[3], pp[4]}, ucon[4], ucov[4];
-  velr_to_vel4(ut, ucon, ucov, g);
-  if (P.prim == IMP_MHD) {
-    double rho = (uu0[RHO]) / gdetu / ucon[0];
-    pp[RHO] = rho;
-  }
-  pp[ENTR] = rad_Sfromu(R, pp[RHO], pp[UU]);
-  int corr = 0;
-  int u2pret = imp_counterpart(R, P.prim, uu0, pp, uu, rg, corr);
-  if (corr != 0) ret = 1;
+  int ret = corr != 0 ? 1 : 0;
   if (u2pret < -1) return -1;
-
+  double err[4] = {0., 0., 0., 0.};
   double Gi[4];
   calc_Gi(R, pp, g, Gi, 1);
   lower(Gi, Gi, g.gg);
@@ -476,6 +478,8 @@ KG_HD int f_implicit(const RadParams &R, const ImpParams &P, const double *ppin,
     else
       err[0] = 0.;
   } else {
+    double pp0[NVR];
+    for (int i = 0; i < NVR; i++) pp0[i] = pp00[i];
     calc_Gi(R, pp, g, Gi, 0);
     double uconf[4], Rtt0, Rtt;
     calc_ff_Rtt(pp0, g, Rtt0, uconf);
@@ -511,122 +515,6 @@ KG_HD int f_implicit(const RadParams &R, const ImpParams &P, const double *ppin,
   return ret;
 }
 
-constexpr int IMP_PAUSED = 1;
-
-// One Newton iteration of solve_implicit_lab_4dprim (rad.c:611-1000).
-// pp is the iterate.  Returns 0 to continue, 2 on convergence, -1 on
-// failure.
-KG_HD int imp_iteration(const RadParams &R, const ImpParams &P, double *pp, const double *uu0, double *pp0, double dt,
-                        const RadGeom &rg, double CONV) {
-  const int sh = P.prim == IMP_MHD ? UU : EE0;
-  const Geom &g = rg.g;
-  double ppp[NVR], f1[4], f2[4], J[4][4], iJ[4][4], err;
-  for (int i = 0; i < NVR; i++) ppp[i] = pp[i];
-  if (f_implicit(R, P, pp, uu0, pp0, dt, rg, f1, err) < 0) return -1;
-  if (err < CONV) return 2;
-  // one-sided finite-difference Jacobian, the other side on trouble
-  for (int j = 0; j < 4; j++) {
-    double sign = -1.;
-    for (;;) {
-      double del;
-      if (j == 0) {
-        del = sign * R.eps * ppp[sh];
-      } else {
-        double x = ppp[j + sh];
-        double sg = x > 0. ? 1. : (x < 0. ? -1. : (x == 0. ? 1. : 0.));
-        double lim = 1.e-6 / sqrt(g.gg[j][j]);
-        double ax = fabs(x);
-        double veleps = R.eps * sg * (lim > ax ? lim : ax);
-        del = x >= 0. ? sign * veleps : -sign * veleps;
-      }
-      pp[j + sh] = ppp[j + sh] + del;
-      double e2;
-      int fret = f_implicit(R, P, pp, uu0, pp0, dt, rg, f2, e2);
-      if (fret < 0) {
-        if (sign > 0.) return -1;
-        pp[j + sh] = ppp[j + sh];
-        sign *= -1.;
-        continue;
-      }
-      for (int i = 0; i < 4; i++) J[i][j] = (f2[i] - f1[i]) / (pp[j + sh] - ppp[j + sh]);
-      pp[j + sh] = ppp[j + sh];
-      break;
-    }
-  }
-  if (inverse_44(J, iJ) < 0) return -1;
-  // damped update until the energy density stays positive and bounded and
-  // the other component inverts
-  double xiapp = 1.;
-  for (;;) {
-    double xxx[4];
-    for (int i = 0; i < 4; i++) xxx[i] = ppp[i + sh];
-    for (int i = 0; i < 4; i++)
-      for (int j = 0; j < 4; j++) xxx[i] -= xiapp * iJ[i][j] * f1[j];
-    for (int i = 0; i < 4; i++) pp[i + sh] = xxx[i];
-    if (P.prim == IMP_MHD) imp_rho_from_velocity(uu0, pp, g);
-    pp[ENTR] = rad_Sfromu(R, pp[RHO], pp[UU]);
-    double uu[NVR];
-    int corr = 0;
-    int u2pret = imp_counterpart(R, P.prim, uu0, pp, uu, rg, corr);
-    if (P.prim == IMP_MHD && corr > 0) u2pret = -1;
-    double edenmin = ppp[sh] / R.maxdown;
-    double edenmax = ppp[sh] * R.maxup;
-    if (xxx[0] > edenmin && xxx[0] < edenmax && u2pret >= -1) break;
-    if (xxx[0] <= 0.) {
-      xiapp *= ppp[sh] / (ppp[sh] + fabs(xxx[0]));
-      xiapp *= 1.e-1;
-    } else {
-      xiapp /= R.dampfac;
-    }
-    if (xiapp < R.maxdamping) return -1;
-  }
-  return 0;
-}
-
-// solve_implicit_lab_4dprim (rad.c:376-1218) from iteration `iter`
-// (0 for a fresh start with pp = pp0) until convergence, failure, or iter
-// reaching `stop` (IMP_PAUSED; the iterate pp and iter carry the state).
-// On success (0) pp holds the primitives and uu the conserved variables.
-KG_HD int imp_solve(const RadParams &R, const ImpParams &P, const double *uu0, const double *pp00, double dt,
-                    const RadGeom &rg, double *pp, double *uu, int &iter, int stop) {
-  double pp0[NVR];
-  for (int i = 0; i < NVR; i++) pp0[i] = pp00[i];
-  const double CONV = P.eq == IMP_ENTROPY ? R.entrconv : R.conv;
-  for (;;) {
-    if (iter >= stop) return IMP_PAUSED;
-    iter++;
-    int r = imp_iteration(R, P, pp, uu0, pp0, dt, rg, CONV);
-    if (r == 2) break;
-    if (r < 0) return -1;
-    if (iter > R.maxiter) return -1;
-  }
-  // convergence found on the step past the limit still fails (rad.c:1051)
-  if (iter > R.maxiter) return -1;
-  // the converged state and its conserved counterpart (rad.c:1088-1150)
-  if (P.prim == IMP_MHD) imp_rho_from_velocity(uu0, pp, rg.g);
-  pp[ENTR] = rad_Sfromu(R, pp[RHO], pp[UU]);
-  int corr = 0;
-  int u2pret;
-  if (P.prim == IMP_RAD) {
-    Grid G;
-    G.gamma = R.gamma;
-    G.nv = NVMAX;
-    p2u_rad_full(G, pp, uu, rg.g);
-    uu[RHO] = uu0[RHO];
-    uu[1] = uu0[1] - (uu[EE0] - uu0[EE0]);
-    uu[2] = uu0[2] - (uu[FX0] - uu0[FX0]);
-    uu[3] = uu0[3] - (uu[FY0] - uu0[FY0]);
-    uu[4] = uu0[4] - (uu[FZ0] - uu0[FZ0]);
-    uu[ENTR] = uu0[ENTR];
-    u2pret = imp_u2p_hot(R, uu, pp, rg.g) < 0 ? -2 : 0;
-  } else {
-    u2pret = imp_counterpart(R, IMP_MHD, uu0, pp, uu, rg, corr);
-    if (corr > 0) u2pret = -2;
-  }
-  if (u2pret < -1) return -1;
-  return 0;
-}
-
 // The attempts solve_implicit_lab makes (rad.c:1404-1505), in order.  The
 // primitive set of attempts 0, 1, 4 is `startwith`, of 2, 3, 5 the other.
 constexpr int IMP_NATTEMPTS = 6;
@@ -648,6 +536,170 @@ KG_HD int imp_startwith(const RadParams &R, const double *pp0, const Geom &g) {
   calc_ff_Rtt(pp0, g, Rtt0, ugas0);
   double Ehat = -Rtt0;
   return Ehat < R.threshold * pp0[UU] ? IMP_RAD : IMP_MHD;
+}
+
+// ---------------------------------------------------------------------------
+// The cascade as a state machine that advances one evaluation at a time.
+//
+// solve_implicit_lab_4dprim (rad.c:376-1218) evaluates, per Newton
+// iteration, the residual at the iterate (base), at four perturbed iterates
+// (Jacobian columns, a column tried with the other sign after a failure),
+// and the inversion of the other component at damped trial points until
+// one is accepted; after convergence the final state is inverted once more.
+// Written as nested loops, the threads of a warp sit in different loops
+// and take turns.  Here every call of imp_advance performs exactly one of
+// those evaluations — the preparation and inversion of the other component
+// are common to all of them, the residual is added for base and Jacobian
+// evaluations — and then moves the cell's state to the next one, so all
+// lanes of a warp run the expensive part together whatever phase their cell
+// is in.  The sequence of operations per cell is the reference's.
+// ---------------------------------------------------------------------------
+enum ImpPhase { PH_BASE = 0, PH_JAC = 1, PH_DAMP = 2, PH_FINAL = 3 };
+enum ImpAdvance { IMP_RUNNING = 0, IMP_DONE_OK = 1, IMP_DONE_FAIL = 2, IMP_PAUSE = 3 };
+
+struct ImpState {
+  double pp[NVR];      // the iterate
+  double ppp[NVR];     // the iterate at the start of the iteration
+  double f1[4];        // residual at ppp
+  double J[4][4];      // Jacobian; its inverse once complete
+  double xiapp;        // damping factor of the update
+  double sign;         // side of the finite difference of column j
+  int iter;            // Newton iterations of the running attempt
+  int att, sw;         // running attempt (0..5), primitives the cascade starts with
+  int phase, j;
+  unsigned evals;      // evaluations performed (statistics)
+};
+
+KG_HD void imp_begin(const RadParams &R, const double *pp00, const Geom &g, ImpState &s) {
+  for (int i = 0; i < NVR; i++) s.pp[i] = pp00[i];
+  s.iter = 0;
+  s.att = 0;
+  s.sw = imp_startwith(R, pp00, g);
+  s.phase = PH_BASE;
+  s.j = 0;
+  s.sign = -1.;
+  s.xiapp = 1.;
+  s.evals = 0;
+}
+
+// The attempt failed: the next one starts afresh from the guess.
+KG_HD int imp_next_attempt(const double *pp00, ImpState &s) {
+  s.att++;
+  if (s.att >= IMP_NATTEMPTS) return IMP_DONE_FAIL;
+  for (int i = 0; i < NVR; i++) s.pp[i] = pp00[i];
+  s.iter = 0;
+  s.phase = PH_BASE;
+  return IMP_RUNNING;
+}
+
+// One evaluation and the transition that follows it.  `budget` counts the
+// Newton iterations the cell may still start in this call sequence; at the
+// start of an iteration with no budget left the cell pauses (IMP_PAUSE)
+// with its state intact.
+KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00, double dt, const RadGeom &rg,
+                      ImpState &s, int &budget) {
+  const ImpParams P = imp_attempt(s.att, s.sw);
+  const int sh = P.prim == IMP_MHD ? UU : EE0;
+  const double CONV = P.eq == IMP_ENTROPY ? R.entrconv : R.conv;
+  double pin[NVR], uu[NVR], f[4] = {0., 0., 0., 0.}, err = 0., xxx0 = 0.;
+  // input of this evaluation
+  if (s.phase == PH_BASE) {
+    if (budget <= 0) return IMP_PAUSE;
+    budget--;
+    s.iter++;
+    for (int i = 0; i < NVR; i++) s.ppp[i] = s.pp[i];
+    for (int i = 0; i < NVR; i++) pin[i] = s.pp[i];
+  } else if (s.phase == PH_JAC) {
+    for (int i = 0; i < NVR; i++) pin[i] = s.ppp[i];
+    const int j = s.j;
+    double del;
+    if (j == 0) {
+      del = s.sign * R.eps * s.ppp[sh];
+    } else {
+      double x = s.ppp[j + sh];
+      double sg = x > 0. ? 1. : (x < 0. ? -1. : (x == 0. ? 1. : 0.));
+      double lim = 1.e-6 / sqrt(rg.g.gg[j][j]);
+      double ax = fabs(x);
+      double veleps = R.eps * sg * (lim > ax ? lim : ax);
+      del = x >= 0. ? s.sign * veleps : -s.sign * veleps;
+    }
+    pin[j + sh] = s.ppp[j + sh] + del;
+  } else if (s.phase == PH_DAMP) {
+    double xxx[4];
+    for (int i = 0; i < 4; i++) xxx[i] = s.ppp[i + sh];
+    for (int i = 0; i < 4; i++)
+      for (int k = 0; k < 4; k++) xxx[i] -= s.xiapp * s.J[i][k] * s.f1[k];
+    for (int i = 0; i < NVR; i++) pin[i] = s.pp[i];
+    for (int i = 0; i < 4; i++) pin[i + sh] = xxx[i];
+    xxx0 = xxx[0];
+  } else {
+    for (int i = 0; i < NVR; i++) pin[i] = s.pp[i];
+  }
+  // the evaluation: other component's inversion, residual where needed
+  s.evals++;
+  int corr = 0;
+  int u2pret = imp_prepare(R, P, uu0, pin, uu, rg, corr);
+  int fret = 0;
+  if (s.phase == PH_BASE || s.phase == PH_JAC)
+    fret = imp_residual(R, P, pin, uu, uu0, pp00, dt, rg, u2pret, corr, f, err);
+  // transition
+  if (s.phase == PH_BASE) {
+    if (fret < 0) return imp_next_attempt(pp00, s);
+    if (err < CONV) {
+      if (s.iter > R.maxiter) return imp_next_attempt(pp00, s);   // converged past the limit (rad.c:1051)
+      s.phase = PH_FINAL;
+      return IMP_RUNNING;
+    }
+    for (int i = 0; i < 4; i++) s.f1[i] = f[i];
+    s.j = 0;
+    s.sign = -1.;
+    s.phase = PH_JAC;
+    return IMP_RUNNING;
+  }
+  if (s.phase == PH_JAC) {
+    const int j = s.j;
+    if (fret < 0) {
+      if (s.sign > 0.) return imp_next_attempt(pp00, s);
+      s.sign = 1.;
+      return IMP_RUNNING;
+    }
+    for (int i = 0; i < 4; i++) s.J[i][j] = (f[i] - s.f1[i]) / (pin[j + sh] - s.ppp[j + sh]);
+    s.j = j + 1;
+    s.sign = -1.;
+    if (s.j == 4) {
+      double iJ[4][4];
+      if (inverse_44(s.J, iJ) < 0) return imp_next_attempt(pp00, s);
+      for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++) s.J[a][b] = iJ[a][b];
+      s.xiapp = 1.;
+      s.phase = PH_DAMP;
+    }
+    return IMP_RUNNING;
+  }
+  if (s.phase == PH_DAMP) {
+    for (int i = 0; i < NVR; i++) s.pp[i] = pin[i];   // the trial and its inversion stay in the iterate
+    if (P.prim == IMP_MHD && corr > 0) u2pret = -1;
+    const double edenmin = s.ppp[sh] / R.maxdown;
+    const double edenmax = s.ppp[sh] * R.maxup;
+    if (xxx0 > edenmin && xxx0 < edenmax && u2pret >= -1) {
+      if (s.iter > R.maxiter) return imp_next_attempt(pp00, s);
+      s.phase = PH_BASE;
+      return IMP_RUNNING;
+    }
+    if (xxx0 <= 0.) {
+      s.xiapp *= s.ppp[sh] / (s.ppp[sh] + fabs(xxx0));
+      s.xiapp *= 1.e-1;
+    } else {
+      s.xiapp /= R.dampfac;
+    }
+    if (s.xiapp < R.maxdamping) return imp_next_attempt(pp00, s);
+    return IMP_RUNNING;
+  }
+  // final inversion of the converged state (rad.c:1088-1150)
+  for (int i = 0; i < NVR; i++) s.pp[i] = pin[i];
+  if (P.prim == IMP_MHD && corr > 0) u2pret = -2;
+  if (u2pret < -1) return imp_next_attempt(pp00, s);
+  return IMP_DONE_OK;
 }
 
 }  // namespace kgpu
