@@ -72,8 +72,8 @@ struct Work {
   int *wit;         // [n] its iteration count
   int *watt;        // [n] the running attempt (0..5)
   int *wsw;         // [n] which primitives the cascade starts with
-  int *q[2];        // queues of cell indices
-  int *count;       // [passes + 2] queue lengths
+  int *q[2][2];     // queues of cell indices [pass parity][primitives of the running attempt]
+  int *count;       // [passes + 2][2] queue lengths
   unsigned long long *stats;  // [0] Newton iterations, [1] passes
 };
 
@@ -90,9 +90,12 @@ size_t work_layout(int n, int passes, Work *w, char *base) {
   p = take((size_t)n * 4); if (w) w->wit = (int *)p;
   p = take((size_t)n * 4); if (w) w->watt = (int *)p;
   p = take((size_t)n * 4); if (w) w->wsw = (int *)p;
-  p = take((size_t)n * 4); if (w) w->q[0] = (int *)p;
-  p = take((size_t)n * 4); if (w) w->q[1] = (int *)p;
-  p = take((size_t)(passes + 2) * 4); if (w) w->count = (int *)p;
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++) {
+      p = take((size_t)n * 4);
+      if (w) w->q[a][b] = (int *)p;
+    }
+  p = take((size_t)(passes + 2) * 2 * 4); if (w) w->count = (int *)p;
   p = take(2 * sizeof(unsigned long long)); if (w) w->stats = (unsigned long long *)p;
   return off;
 }
@@ -161,42 +164,57 @@ __global__ void __launch_bounds__(128) k_rad_plain(RadParams R, Cell C, int n, u
   if (stats) warp_add(stats, (unsigned)((1 << 30) - budget));
 }
 
-// Pass p of the batched form: cells of queue p (all cells in pass 0) may
-// start up to K Newton iterations; unfinished ones keep their state (the
-// iterate, its iteration count, the attempt) and go to queue p+1.
+// Start of the batched form: every cell's cascade state (first attempt,
+// no iteration yet, the guess as iterate), queued by the primitives its
+// first attempt works on, so that warps of a pass run one kind of inversion.
+__global__ void k_rad_start(RadParams R, Cell C, Work W, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  RadGeom rg;
+  rad_geom(C.g + 20L * k, C.G + 20L * k, rg);
+  const double *p0 = C.pp + (long)k * NVR;
+  const int sw = imp_startwith(R, p0, rg.g);
+  W.wsw[k] = sw;
+  W.watt[k] = 0;
+  W.wit[k] = 0;
+  for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = p0[i];
+  const int type = imp_attempt(0, sw).prim;
+  warp_push(W.q[0][type], W.count + 0 * 2 + type, true, k);
+}
+
+// Pass p: the cells of queue p may start up to K Newton iterations;
+// unfinished ones keep their state (the iterate, its iteration count, the
+// attempt) and go to queue p+1, by the primitives of their running attempt.
 __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, int n, int p, int K) {
-  const int nin = p == 0 ? n : W.count[p];
-  const int *qin = W.q[p & 1];
-  int *qout = W.q[(p + 1) & 1];
+  const int n0 = W.count[p * 2 + 0], n1 = W.count[p * 2 + 1];
+  const int nin = n0 + n1;
+  const int par = p & 1;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nin; q += gridDim.x * blockDim.x) {
-    const int k = p == 0 ? q : qin[q];
+    const int k = q < n0 ? W.q[par][0][q] : W.q[par][1][q - n0];
     RadGeom rg;
     rad_geom(C.g + 20L * k, C.G + 20L * k, rg);
     const double *u0 = C.uu + (long)k * NVR, *p0 = C.pp + (long)k * NVR;
     const double dt = C.dt[k];
     ImpState s;
-    if (p == 0) {
-      imp_begin(R, p0, rg.g, s);
-    } else {
-      s.phase = PH_BASE;
-      s.j = 0;
-      s.sign = -1.;
-      s.xiapp = 1.;
-      s.evals = 0;
-      s.sw = W.wsw[k];
-      s.att = W.watt[k];
-      s.iter = W.wit[k];
-      for (int i = 0; i < NVR; i++) s.pp[i] = W.wpp[(long)k * NVR + i];
-    }
+    s.phase = PH_BASE;
+    s.j = 0;
+    s.sign = -1.;
+    s.xiapp = 1.;
+    s.evals = 0;
+    s.sw = W.wsw[k];
+    s.att = W.watt[k];
+    s.iter = W.wit[k];
+    for (int i = 0; i < NVR; i++) s.pp[i] = W.wpp[(long)k * NVR + i];
     int budget = K;
     int r;
     while ((r = imp_advance(R, u0, p0, dt, rg, s, budget)) == IMP_RUNNING) {
     }
     warp_add(W.stats, (unsigned)(K - budget));
     const bool paused = r == IMP_PAUSE;
-    warp_push(qout, W.count + p + 1, paused, k);
+    const int type = paused ? imp_attempt(s.att, s.sw).prim : 0;
+    warp_push(W.q[par ^ 1][0], W.count + (p + 1) * 2 + 0, paused && type == 0, k);
+    warp_push(W.q[par ^ 1][1], W.count + (p + 1) * 2 + 1, paused && type == 1, k);
     if (paused) {
-      W.wsw[k] = s.sw;
       W.watt[k] = s.att;
       W.wit[k] = s.iter;
       for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = s.pp[i];
@@ -346,9 +364,11 @@ extern "C" int kgpu_rad_implicit_cells_device(int n, const kgpu_rad_params *rp, 
   char *base = (char *)(((uintptr_t)work + 255) & ~(uintptr_t)255);
   Work W;
   work_layout(n, passes, &W, base);   // fits: the area is sized for kMaxPasses >= passes
-  RCK(cudaMemsetAsync(W.count, 0, (size_t)(passes + 2) * 4, st));
+  RCK(cudaMemsetAsync(W.count, 0, (size_t)(passes + 2) * 2 * 4, st));
   RCK(cudaMemsetAsync(W.stats, 0, 2 * sizeof(unsigned long long), st));
   const int grid = sm_count() * 8;
+  k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n);
+  RCK(cudaGetLastError());
   for (int p = 0; p < passes; p++) {
     const int Kp = p == passes - 1 ? (1 << 30) : K;   // the last pass finishes whatever is left
     const int blocks = p == 0 ? (n + 127) / 128 : grid;
