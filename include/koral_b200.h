@@ -303,6 +303,47 @@ int kgpu_rad_implicit_cells_device(int n, const kgpu_rad_params *rp, const doubl
                                    const double *g, const double *G, const double *dt, double *pp_out,
                                    double *uu_out, int *status, int *attempt, int *iters, int mode, void *work,
                                    void *stream, unsigned long long *stats);
+/* Learned warm start.  kgpu_rad_implicit_cells_warm_device is the batched
+ * form whose first attempt starts from the iterate predicted by the warm-
+ * start network (ypred, float [n][8], the output of kgpu_mlp_forward on
+ * the cells' features); where that attempt fails it is repeated from the
+ * cell's own guess and the reference cascade follows, so every cell still
+ * converges to RADIMPCONV or fails as the reference would.  stats: [0]
+ * Newton iterations over all attempts, [1] passes, [2] cells whose warm
+ * attempt failed (fallbacks). */
+int kgpu_rad_implicit_cells_warm_device(int n, const kgpu_rad_params *rp, const double *uu, const double *pp,
+                                        const double *g, const double *G, const double *dt, const float *ypred,
+                                        double *pp_out, double *uu_out, int *status, int *attempt, int *iters,
+                                        void *work, void *stream, unsigned long long *stats);
+/* Network inputs (float [n][16]) of cells before a solve, and training
+ * targets (float [n][5]: ln of the gas and radiation energy ratios, change
+ * of the iterated velocity) from the states before and after; NaN where
+ * status is not 0.  Device pointers, asynchronous on stream. */
+int kgpu_rad_features_device(int n, const kgpu_rad_params *rp, const double *pp, const double *g, const double *G,
+                             const double *dt, float *X, void *stream);
+int kgpu_rad_targets_device(int n, const kgpu_rad_params *rp, const double *pp, const double *pp1,
+                            const double *g, const double *G, const int *status, float *T, void *stream);
+
+/* The warm-start network: 16 -> 128 -> 128 -> 5, SiLU, BF16 weights and
+ * activations with FP32 accumulation on the tensor cores; trained and run on
+ * the device.  The parameter blob (kgpu_mlp_blob_size() floats) holds
+ * W1[16][128], b1[128], W2[128][128], b2[128], W3[128][8], b3[8] (outputs
+ * 5..7 unused), then the output standardisation mean[8] and scale[8]. */
+typedef struct kgpu_mlp kgpu_mlp;
+int kgpu_mlp_blob_size(void);
+int kgpu_mlp_create(kgpu_mlp **mlp, unsigned long long seed);
+int kgpu_mlp_destroy(kgpu_mlp *mlp);
+int kgpu_mlp_get(kgpu_mlp *mlp, float *blob);
+int kgpu_mlp_set(kgpu_mlp *mlp, const float *blob);
+/* Y[n][8] (unstandardised outputs) from X[n][16]; device pointers. */
+int kgpu_mlp_forward(kgpu_mlp *mlp, const float *X, int n, float *Y, void *stream);
+/* Gradient (the blob's first part) and mean loss of one batch of n samples
+ * at the current weights, without an update; device X, T, host outputs. */
+int kgpu_mlp_gradient(kgpu_mlp *mlp, const float *X, const float *T, int n, float *grad, double *loss);
+/* One shuffled epoch of Adam over n samples in batches of `batch`. */
+int kgpu_mlp_train_epoch(kgpu_mlp *mlp, const float *X, const float *T, int n, int batch, float lr,
+                         unsigned long long seed, double *mean_loss);
+
 /* Tuning of the batched form: Newton iterations a cell may take per pass
  * (default 8; results do not depend on it).  Process-wide. */
 int kgpu_rad_set_pass_iters(int k);

@@ -142,6 +142,19 @@ def lib():
         L.kgpu_ks_metric.argtypes = [ctypes.c_double] * 3 + [_dp] * 2
         L.kgpu_ks_metric_batch.argtypes = [ctypes.c_double, ctypes.c_int] + [_dp] * 4
         L.kgpu_fp64_peak.argtypes = [_dp]
+        L.kgpu_rad_implicit_cells_warm_device.argtypes = [ctypes.c_int, rpp] + [vp] * 13 + [
+            ctypes.POINTER(ctypes.c_ulonglong)]
+        L.kgpu_rad_features_device.argtypes = [ctypes.c_int, rpp] + [vp] * 6
+        L.kgpu_rad_targets_device.argtypes = [ctypes.c_int, rpp] + [vp] * 7
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.kgpu_mlp_create.argtypes = [ctypes.POINTER(vp), ctypes.c_ulonglong]
+        L.kgpu_mlp_destroy.argtypes = [vp]
+        L.kgpu_mlp_get.argtypes = [vp, fp]
+        L.kgpu_mlp_set.argtypes = [vp, fp]
+        L.kgpu_mlp_forward.argtypes = [vp, vp, ctypes.c_int, vp, vp]
+        L.kgpu_mlp_gradient.argtypes = [vp, vp, vp, ctypes.c_int, fp, _dp]
+        L.kgpu_mlp_train_epoch.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                           ctypes.c_ulonglong, _dp]
         L.kgpu_u2p_cells_static.argtypes = sig["kgpu_u2p_cells"]
         L.kgpu_u2p_cells_static.restype = ctypes.c_int
         L.kgpu_u2p_cells_static_error.restype = ctypes.c_char_p
@@ -534,13 +547,15 @@ def ks_metric(a, r, th):
     return g20, G20
 
 
-def rad_cell_draws(n, seed, rp, metric=None, spin=0.9):
+def rad_cell_draws(n, seed, rp, metric=None, spin=0.9, sigma=None):
     """Random radiating cells around a Kerr black hole: r log-uniform in
     [2, 100] M, theta uniform in [0.1, pi - 0.1]; log-uniform rho in
     [1e-8, 1], gas temperature in [1e4, 1e12] K, E_rad/rho in [1e-10, 1e2]
     and optical depth per cell in [1e-3, 1e5]; gas Lorentz factor
     log-uniform in [1, 20] and radiation flux fraction uniform in [0, 0.99],
-    each in an isotropic direction.  Returns (pp, g, G, tau) with the entropy
+    each in an isotropic direction; with sigma = (lo, hi), a magnetic field
+    in an isotropic direction with B^i g_ij B^j / rho log-uniform in
+    [lo, hi].  Returns (pp, g, G, tau) with the entropy
     slot of pp left for the caller (it goes with the conserved variables).
     `metric(r, th)` gives the metric point (default: the product's
     Kerr-Schild metric)."""
@@ -573,15 +588,18 @@ def rad_cell_draws(n, seed, rp, metric=None, spin=0.9):
     pp = np.zeros((n, NVR))
     pp[:, 0], pp[:, 1], pp[:, 2:5], pp[:, 9], pp[:, 10:13] = rho, u, ug, Erf, ur
     tau = 10 ** rng.uniform(-3, 5, n)
+    if sigma is not None:
+        sg = 10 ** rng.uniform(np.log10(sigma[0]), np.log10(sigma[1]), n)
+        pp[:, 6:9] = direction(sg * rho)
     return pp, g20, G20, tau
 
 
-def rad_cells(n, seed, rp, spin=0.9, metric=None):
+def rad_cells(n, seed, rp, spin=0.9, metric=None, sigma=None):
     """rad_cell_draws completed with the product's own p2u: entropy, conserved
     variables, and dt = 0.5 dx with dx = tau / (kappa_abs + kappa_es) (the
     light-crossing CFL step of a cell of that optical depth).  Returns
     (uu, pp, g, G, dt)."""
-    pp, g20, G20, tau = rad_cell_draws(n, seed, rp, metric=metric, spin=spin)
+    pp, g20, G20, tau = rad_cell_draws(n, seed, rp, metric=metric, spin=spin, sigma=sigma)
     gm1 = rp.gamma - 1.
     idx = 1. / gm1
     pp[:, 5] = pp[:, 0] * np.log((gm1 * pp[:, 1]) ** idx / pp[:, 0] ** (idx + 1.))
@@ -592,4 +610,109 @@ def rad_cells(n, seed, rp, spin=0.9, metric=None):
     kes = rp.kes_gu * pp[:, 0]
     dt = 0.5 * tau / (kabs + kes)
     return uu, pp, g20, G20, dt
+
+
+# ---------------------------------------------------------------------------
+# learned warm start (device tensors from torch: plumbing only)
+# ---------------------------------------------------------------------------
+def _vp(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p()
+
+
+def _stream():
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class Mlp:
+    """The warm-start network (kgpu_mlp_*): 16 -> 128 -> 128 -> 5, SiLU,
+    BF16 tensor-core kernels with FP32 accumulation."""
+
+    def __init__(self, seed=1):
+        self.L = lib()
+        self.h = ctypes.c_void_p()
+        _check(self.L.kgpu_mlp_create(ctypes.byref(self.h), seed), "kgpu_mlp_create")
+        self.size = self.L.kgpu_mlp_blob_size()
+
+    def close(self):
+        if self.h:
+            self.L.kgpu_mlp_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get(self):
+        b = np.zeros(self.size, dtype=np.float32)
+        _check(self.L.kgpu_mlp_get(self.h, b.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), "kgpu_mlp_get")
+        return b
+
+    def set(self, blob):
+        b = np.ascontiguousarray(blob, dtype=np.float32)
+        assert b.size == self.size
+        _check(self.L.kgpu_mlp_set(self.h, b.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), "kgpu_mlp_set")
+
+    def forward(self, X):
+        import torch
+        Y = torch.empty((X.shape[0], 8), dtype=torch.float32, device=X.device)
+        _check(self.L.kgpu_mlp_forward(self.h, _vp(X), X.shape[0], _vp(Y), _stream()), "kgpu_mlp_forward")
+        return Y
+
+    def gradient(self, X, T):
+        g = np.zeros(self.size - 16, dtype=np.float32)
+        loss = ctypes.c_double()
+        _check(self.L.kgpu_mlp_gradient(self.h, _vp(X), _vp(T), X.shape[0],
+                                        g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(loss)),
+               "kgpu_mlp_gradient")
+        return g, loss.value
+
+    def train_epoch(self, X, T, batch=8192, lr=1e-3, seed=0):
+        loss = ctypes.c_double()
+        _check(self.L.kgpu_mlp_train_epoch(self.h, _vp(X), _vp(T), X.shape[0], batch, lr, seed,
+                                           ctypes.byref(loss)), "kgpu_mlp_train_epoch")
+        return loss.value
+
+
+def rad_features_device(rp, pp, g, G, dt):
+    import torch
+    X = torch.empty((pp.shape[0], 16), dtype=torch.float32, device=pp.device)
+    _check(lib().kgpu_rad_features_device(pp.shape[0], ctypes.byref(rp), _vp(pp), _vp(g), _vp(G), _vp(dt), _vp(X),
+                                          _stream()), "kgpu_rad_features_device")
+    return X
+
+
+def rad_targets_device(rp, pp, pp1, g, G, status):
+    import torch
+    T = torch.empty((pp.shape[0], 5), dtype=torch.float32, device=pp.device)
+    _check(lib().kgpu_rad_targets_device(pp.shape[0], ctypes.byref(rp), _vp(pp), _vp(pp1), _vp(g), _vp(G),
+                                         _vp(status), _vp(T), _stream()), "kgpu_rad_targets_device")
+    return T
+
+
+def rad_solve_device(rp, uu, pp, g, G, dt, mode=RAD_BATCHED, ypred=None, work=None):
+    """Batched implicit solve on device tensors; with ypred, the learned warm
+    start.  Returns (pp, uu, status, attempt, iters, stats)."""
+    import torch
+    n = uu.shape[0]
+    dev = uu.device
+    po = torch.empty_like(pp)
+    uo = torch.empty_like(uu)
+    st, at, it = (torch.empty(n, dtype=torch.int32, device=dev) for _ in range(3))
+    L = lib()
+    if work is None and (mode == RAD_BATCHED or ypred is not None):
+        work = torch.empty(int(L.kgpu_rad_work_bytes(n)), dtype=torch.uint8, device=dev)
+    stats = (ctypes.c_ulonglong * 3)()
+    if ypred is None:
+        _check(L.kgpu_rad_implicit_cells_device(n, ctypes.byref(rp), _vp(uu), _vp(pp), _vp(g), _vp(G), _vp(dt),
+                                                _vp(po), _vp(uo), _vp(st), _vp(at), _vp(it), mode, _vp(work),
+                                                _stream(), stats), "kgpu_rad_implicit_cells_device")
+    else:
+        _check(L.kgpu_rad_implicit_cells_warm_device(n, ctypes.byref(rp), _vp(uu), _vp(pp), _vp(g), _vp(G),
+                                                     _vp(dt), _vp(ypred), _vp(po), _vp(uo), _vp(st), _vp(at),
+                                                     _vp(it), _vp(work), _stream(), stats),
+               "kgpu_rad_implicit_cells_warm_device")
+    return po, uo, st, at, it, list(stats)
 

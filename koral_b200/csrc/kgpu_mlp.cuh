@@ -1,0 +1,69 @@
+// Learned warm start of the implicit radiation source solve: the network's
+// inputs (16 features of a cell's state before the solve) and outputs (5
+// numbers from which the initial iterate is built), host and device
+// callable.
+//
+// Features (each brought to order one):
+//   0  log10 rho / 4 + 1           1  log10(u_gas / rho) / 4
+//   2  log10(E_rad / rho) / 6      3-5  gas relative 4-velocity x sqrt(g_ii), asinh
+//   6-8  radiation-frame relative 4-velocity x sqrt(g_ii), asinh
+//   9  log10(kappa_abs dt) / 5     10  log10(kappa_es dt) / 5
+//   11 lapse                       12  g_tt + 1
+//   13 log10 sqrt(g_33) / 2        14  1 when the cascade starts on gas primitives, else 0
+//   15 log10(E_rad / u_gas) / 6
+// Outputs, the change from the state before the solve to the converged one:
+//   0  ln(u_gas' / u_gas)          1  ln(E_rad' / E_rad)
+//   2-4  change of the velocity the first attempt iterates (the gas's when
+//        it works on gas primitives, the radiation frame's otherwise),
+//        x sqrt(g_ii)
+// Each output is standardised with a mean and a scale kept with the weights.
+#pragma once
+
+#include "kgpu_rad.cuh"
+
+namespace kgpu {
+
+constexpr int MLP_IN = 16, MLP_H = 128, MLP_OUT = 5, MLP_OUTP = 8;
+
+KG_HD double mlp_safe_log10(double x) { return log10(x > 1e-300 ? x : 1e-300); }
+
+KG_HD void mlp_features(const RadParams &R, const double *pp, const RadGeom &rg, double dt, int startwith,
+                        float x[MLP_IN]) {
+  const auto &gg = rg.g.gg;
+  const double rho = pp[RHO], ug = pp[UU], Er = pp[EE0];
+  x[0] = (float)(mlp_safe_log10(rho) / 4. + 1.);
+  x[1] = (float)(mlp_safe_log10(ug / rho) / 4.);
+  x[2] = (float)(mlp_safe_log10(Er / rho) / 6.);
+  for (int i = 0; i < 3; i++) {
+    x[3 + i] = (float)asinh(pp[VX + i] * sqrt(gg[i + 1][i + 1]));
+    x[6 + i] = (float)asinh(pp[FX0 + i] * sqrt(gg[i + 1][i + 1]));
+  }
+  x[9] = (float)(mlp_safe_log10(rad_kappa_abs(R, pp) * dt) / 5.);
+  x[10] = (float)(mlp_safe_log10(rad_kappa_es(R, pp) * dt) / 5.);
+  x[11] = (float)rg.alpha;
+  x[12] = (float)rg.g.gttpert;
+  x[13] = (float)(mlp_safe_log10(sqrt(gg[3][3])) / 2.);
+  x[14] = startwith == IMP_MHD ? 1.f : 0.f;
+  x[15] = (float)(mlp_safe_log10(Er / ug) / 6.);
+}
+
+// raw (unstandardised) targets from the state before and after the solve
+KG_HD void mlp_targets(const double *pp0, const double *pp1, const RadGeom &rg, int startwith, double t[MLP_OUT]) {
+  const auto &gg = rg.g.gg;
+  t[0] = log(pp1[UU] / pp0[UU]);
+  t[1] = log(pp1[EE0] / pp0[EE0]);
+  const int v = startwith == IMP_MHD ? VX : FX0;
+  for (int i = 0; i < 3; i++) t[2 + i] = (pp1[v + i] - pp0[v + i]) * sqrt(gg[i + 1][i + 1]);
+}
+
+// initial iterate from the (unstandardised) prediction
+KG_HD void mlp_guess(const double *pp0, const RadGeom &rg, int startwith, const double t[MLP_OUT], double *guess) {
+  const auto &gg = rg.g.gg;
+  for (int i = 0; i < NVR; i++) guess[i] = pp0[i];
+  guess[UU] = pp0[UU] * exp(t[0]);
+  guess[EE0] = pp0[EE0] * exp(t[1]);
+  const int v = startwith == IMP_MHD ? VX : FX0;
+  for (int i = 0; i < 3; i++) guess[v + i] = pp0[v + i] + t[2 + i] / sqrt(gg[i + 1][i + 1]);
+}
+
+}  // namespace kgpu

@@ -20,7 +20,7 @@
 #include <string.h>
 
 #include "../../include/koral_b200.h"
-#include "kgpu_rad.cuh"
+#include "kgpu_mlp.cuh"
 
 using namespace kgpu;
 
@@ -72,9 +72,10 @@ struct Work {
   int *wit;         // [n] its iteration count
   int *watt;        // [n] the running attempt (0..5)
   int *wsw;         // [n] which primitives the cascade starts with
+  int *wwarm;       // [n] the first attempt still runs from a predicted iterate
   int *q[2][2];     // queues of cell indices [pass parity][primitives of the running attempt]
   int *count;       // [passes + 2][2] queue lengths
-  unsigned long long *stats;  // [0] Newton iterations, [1] passes
+  unsigned long long *stats;  // [0] Newton iterations, [1] passes, [2] fallbacks of the warm start
 };
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -90,13 +91,14 @@ size_t work_layout(int n, int passes, Work *w, char *base) {
   p = take((size_t)n * 4); if (w) w->wit = (int *)p;
   p = take((size_t)n * 4); if (w) w->watt = (int *)p;
   p = take((size_t)n * 4); if (w) w->wsw = (int *)p;
+  p = take((size_t)n * 4); if (w) w->wwarm = (int *)p;
   for (int a = 0; a < 2; a++)
     for (int b = 0; b < 2; b++) {
       p = take((size_t)n * 4);
       if (w) w->q[a][b] = (int *)p;
     }
   p = take((size_t)(passes + 2) * 2 * 4); if (w) w->count = (int *)p;
-  p = take(2 * sizeof(unsigned long long)); if (w) w->stats = (unsigned long long *)p;
+  p = take(4 * sizeof(unsigned long long)); if (w) w->stats = (unsigned long long *)p;
   return off;
 }
 
@@ -167,7 +169,7 @@ __global__ void __launch_bounds__(128) k_rad_plain(RadParams R, Cell C, int n, u
 // Start of the batched form: every cell's cascade state (first attempt,
 // no iteration yet, the guess as iterate), queued by the primitives its
 // first attempt works on, so that warps of a pass run one kind of inversion.
-__global__ void k_rad_start(RadParams R, Cell C, Work W, int n) {
+__global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypred) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   RadGeom rg;
@@ -177,7 +179,17 @@ __global__ void k_rad_start(RadParams R, Cell C, Work W, int n) {
   W.wsw[k] = sw;
   W.watt[k] = 0;
   W.wit[k] = 0;
-  for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = p0[i];
+  if (ypred) {
+    // learned warm start: the first attempt begins at the predicted state
+    double t[MLP_OUT], guess[NVR];
+    for (int o = 0; o < MLP_OUT; o++) t[o] = ypred[(long)k * MLP_OUTP + o];
+    mlp_guess(p0, rg, sw, t, guess);
+    for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = guess[i];
+    W.wwarm[k] = 1;
+  } else {
+    for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = p0[i];
+    W.wwarm[k] = 0;
+  }
   const int type = imp_attempt(0, sw).prim;
   warp_push(W.q[0][type], W.count + 0 * 2 + type, true, k);
 }
@@ -204,12 +216,15 @@ __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, i
     s.sw = W.wsw[k];
     s.att = W.watt[k];
     s.iter = W.wit[k];
+    s.warm = W.wwarm[k];
     for (int i = 0; i < NVR; i++) s.pp[i] = W.wpp[(long)k * NVR + i];
+    const int warm0 = s.warm;
     int budget = K;
     int r;
     while ((r = imp_advance(R, u0, p0, dt, rg, s, budget)) == IMP_RUNNING) {
     }
     warp_add(W.stats, (unsigned)(K - budget));
+    warp_add(W.stats + 2, (unsigned)(warm0 && !s.warm));
     const bool paused = r == IMP_PAUSE;
     const int type = paused ? imp_attempt(s.att, s.sw).prim : 0;
     warp_push(W.q[par ^ 1][0], W.count + (p + 1) * 2 + 0, paused && type == 0, k);
@@ -217,6 +232,7 @@ __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, i
     if (paused) {
       W.watt[k] = s.att;
       W.wit[k] = s.iter;
+      W.wwarm[k] = s.warm;
       for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = s.pp[i];
     } else if (r == IMP_DONE_OK) {
       cell_success(R, C, k, rg, s.pp, s.att, s.iter);
@@ -329,15 +345,16 @@ extern "C" size_t kgpu_rad_work_bytes(int n) {
   return work_layout(n, kMaxPasses, nullptr, nullptr) + 256;
 }
 
-extern "C" int kgpu_rad_implicit_cells_device(int n, const kgpu_rad_params *rp, const double *uu, const double *pp,
-                                              const double *g, const double *G, const double *dt, double *pp_out,
-                                              double *uu_out, int *status, int *attempt, int *iters, int mode,
-                                              void *work, void *stream, unsigned long long *stats) {
+static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
+                            const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
+                            int *status, int *attempt, int *iters, int mode, void *work, void *stream,
+                            unsigned long long *stats, int nstats) {
   if (n < 0 || !rp || (mode != KGPU_RAD_PLAIN && mode != KGPU_RAD_BATCHED)) return KGPU_EINVAL;
   if (n > 0 && (!uu || !pp || !g || !G || !dt || !pp_out || !uu_out || !status || !attempt || !iters))
     return KGPU_EINVAL;
   if (mode == KGPU_RAD_BATCHED && n > 0 && !work) return KGPU_EINVAL;
-  if (stats) stats[0] = stats[1] = 0;
+  if (stats)
+    for (int i = 0; i < nstats; i++) stats[i] = 0;
   if (n == 0) return 0;
   cudaStream_t st = (cudaStream_t)stream;
   RadParams R = to_dev(*rp);
@@ -365,9 +382,9 @@ extern "C" int kgpu_rad_implicit_cells_device(int n, const kgpu_rad_params *rp, 
   Work W;
   work_layout(n, passes, &W, base);   // fits: the area is sized for kMaxPasses >= passes
   RCK(cudaMemsetAsync(W.count, 0, (size_t)(passes + 2) * 2 * 4, st));
-  RCK(cudaMemsetAsync(W.stats, 0, 2 * sizeof(unsigned long long), st));
+  RCK(cudaMemsetAsync(W.stats, 0, 4 * sizeof(unsigned long long), st));
   const int grid = sm_count() * 8;
-  k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n);
+  k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n, ypred);
   RCK(cudaGetLastError());
   for (int p = 0; p < passes; p++) {
     const int Kp = p == passes - 1 ? (1 << 30) : K;   // the last pass finishes whatever is left
@@ -376,9 +393,73 @@ extern "C" int kgpu_rad_implicit_cells_device(int n, const kgpu_rad_params *rp, 
     RCK(cudaGetLastError());
   }
   if (stats) {
-    RCK(cudaMemcpyAsync(stats, W.stats, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    RCK(cudaMemcpyAsync(stats, W.stats, nstats * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     RCK(cudaStreamSynchronize(st));
   }
+  return 0;
+}
+
+extern "C" int kgpu_rad_implicit_cells_device(int n, const kgpu_rad_params *rp, const double *uu, const double *pp,
+                                              const double *g, const double *G, const double *dt, double *pp_out,
+                                              double *uu_out, int *status, int *attempt, int *iters, int mode,
+                                              void *work, void *stream, unsigned long long *stats) {
+  return rad_solve_device(n, rp, uu, pp, g, G, dt, nullptr, pp_out, uu_out, status, attempt, iters, mode, work,
+                          stream, stats, 2);
+}
+
+extern "C" int kgpu_rad_implicit_cells_warm_device(int n, const kgpu_rad_params *rp, const double *uu,
+                                                   const double *pp, const double *g, const double *G,
+                                                   const double *dt, const float *ypred, double *pp_out,
+                                                   double *uu_out, int *status, int *attempt, int *iters,
+                                                   void *work, void *stream, unsigned long long *stats) {
+  if (n > 0 && !ypred) return KGPU_EINVAL;
+  return rad_solve_device(n, rp, uu, pp, g, G, dt, ypred, pp_out, uu_out, status, attempt, iters,
+                          KGPU_RAD_BATCHED, work, stream, stats, 3);
+}
+
+// network inputs of n cells (float [n][16])
+__global__ void k_rad_features(RadParams R, int n, const double *pp, const double *g, const double *G,
+                               const double *dt, float *X) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  RadGeom rg;
+  rad_geom(g + 20L * k, G + 20L * k, rg);
+  const double *p0 = pp + (long)k * NVR;
+  float x[MLP_IN];
+  mlp_features(R, p0, rg, dt[k], imp_startwith(R, p0, rg.g), x);
+  for (int f = 0; f < MLP_IN; f++) X[(long)k * MLP_IN + f] = x[f];
+}
+
+// training targets (float [n][5]) from the states before and after a solve;
+// cells whose solve failed get NaN
+__global__ void k_rad_targets(RadParams R, int n, const double *pp, const double *pp1, const double *g,
+                              const double *G, const int *status, float *T) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  RadGeom rg;
+  rad_geom(g + 20L * k, G + 20L * k, rg);
+  const double *p0 = pp + (long)k * NVR;
+  double t[MLP_OUT];
+  mlp_targets(p0, pp1 + (long)k * NVR, rg, imp_startwith(R, p0, rg.g), t);
+  for (int o = 0; o < MLP_OUT; o++) T[(long)k * MLP_OUT + o] = status[k] == 0 ? (float)t[o] : __int_as_float(0x7fc00000);
+}
+
+extern "C" int kgpu_rad_features_device(int n, const kgpu_rad_params *rp, const double *pp, const double *g,
+                                        const double *G, const double *dt, float *X, void *stream) {
+  if (n < 0 || !rp || (n > 0 && (!pp || !g || !G || !dt || !X))) return KGPU_EINVAL;
+  if (n == 0) return 0;
+  k_rad_features<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(to_dev(*rp), n, pp, g, G, dt, X);
+  RCK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int kgpu_rad_targets_device(int n, const kgpu_rad_params *rp, const double *pp, const double *pp1,
+                                       const double *g, const double *G, const int *status, float *T,
+                                       void *stream) {
+  if (n < 0 || !rp || (n > 0 && (!pp || !pp1 || !g || !G || !status || !T))) return KGPU_EINVAL;
+  if (n == 0) return 0;
+  k_rad_targets<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(to_dev(*rp), n, pp, pp1, g, G, status, T);
+  RCK(cudaGetLastError());
   return 0;
 }
 

@@ -567,6 +567,7 @@ struct ImpState {
   int iter;            // Newton iterations of the running attempt
   int att, sw;         // running attempt (0..5), primitives the cascade starts with
   int phase, j;
+  int warm;            // the first attempt runs from a predicted iterate
   unsigned evals;      // evaluations performed (statistics)
 };
 
@@ -579,11 +580,22 @@ KG_HD void imp_begin(const RadParams &R, const double *pp00, const Geom &g, ImpS
   s.j = 0;
   s.sign = -1.;
   s.xiapp = 1.;
+  s.warm = 0;
   s.evals = 0;
 }
 
-// The attempt failed: the next one starts afresh from the guess.
+// The attempt failed: the next one starts afresh from the guess.  A first
+// attempt started from a predicted iterate is first repeated from the
+// guess itself (the fallback of the learned warm start), so the cascade
+// that follows is exactly the reference's.
 KG_HD int imp_next_attempt(const double *pp00, ImpState &s) {
+  if (s.warm) {
+    s.warm = 0;
+    for (int i = 0; i < NVR; i++) s.pp[i] = pp00[i];
+    s.iter = 0;
+    s.phase = PH_BASE;
+    return IMP_RUNNING;
+  }
   s.att++;
   if (s.att >= IMP_NATTEMPTS) return IMP_DONE_FAIL;
   for (int i = 0; i < NVR; i++) s.pp[i] = pp00[i];
