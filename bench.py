@@ -391,6 +391,66 @@ def our_arm(args, wl, rank, world, local_rank):
 # ---------------------------------------------------------------------------
 # our arm, batched implicit solve
 # ---------------------------------------------------------------------------
+def learned_leg(k, rp, d_in, work, stream, n, st_plain, it_plain, args, dev):
+    """The same solve with the learned warm start (features, network on the
+    tensor cores, warm batched solve), timed as a whole, against the plain
+    batched solve's iterations on the same cells."""
+    import numpy as np
+    import torch
+    from koral_b200 import train_warmstart
+    path = train_warmstart.DEFAULT_OUT
+    if not os.path.exists(path):
+        return {"unavailable": "no trained weights (python -m koral_b200.train_warmstart)"}
+    mlp = train_warmstart.load(k, path)
+    uu, pp, g, G, dt = d_in
+
+    def run():
+        X = k.rad_features_device(rp, pp, g, G, dt)
+        Y = mlp.forward(X)
+        return k.rad_solve_device(rp, uu, pp, g, G, dt, ypred=Y, work=work), X, Y
+
+    run()
+    torch.cuda.synchronize(dev)
+    steps = max(1, min(3, args.steps))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        out, X, Y = run()
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = a.elapsed_time(b) / steps
+    # the network alone (tensor-core roofline: 2 (16 128 + 128 128 + 128 5) flop per sample)
+    a.record(stream)
+    for _ in range(10):
+        mlp.forward(X)
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_mlp = a.elapsed_time(b) / 10
+    flop = 2 * (16 * 128 + 128 * 128 + 128 * 5) * n
+    po, uo, st, at, it, stats = out
+    st, it = st.cpu().numpy(), it.cpu().numpy()
+    ok = (st == 0) & (st_plain == 0)
+    # error of the BF16 prediction against the converged FP64 state
+    pred = torch.exp(Y[:, :2].double()).cpu().numpy()
+    true = (po[:, [1, 9]] / pp[:, [1, 9]]).cpu().numpy()
+    gerr = np.abs(pred - true) / np.abs(true)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    return {"value": n / (ms / 1e3), "unit": RAD_UNIT, "ms_per_step": ms,
+            "mean_iterations_successful_attempt": float(it[ok].mean()),
+            "plain_mean_iterations_successful_attempt": float(it_plain[ok].mean()),
+            "iteration_ratio": float(it_plain[ok].mean() / it[ok].mean()),
+            "mean_iterations_all_attempts": stats[0] / n, "fallback_rate": stats[2] / n,
+            "status_agreement": float(np.mean(st == st_plain)),
+            "guess_error_median": {"u_gas": float(np.median(gerr[ok, 0])), "E_rad": float(np.median(gerr[ok, 1]))},
+            "mlp": {"ms": ms_mlp, "achieved_tflops": flop / (ms_mlp / 1e3) / 1e12, "peak_tflops": bf16_peak,
+                    "frac": flop / (ms_mlp / 1e3) / 1e12 / bf16_peak, "bound": "tensor"}}
+
+
 def our_arm_radcells(args, wl, rank, world, local_rank):
     import numpy as np
     import torch
@@ -457,6 +517,7 @@ def our_arm_radcells(args, wl, rank, world, local_rank):
     at = d_at.cpu().numpy()
     peak = ctypes.c_double()
     k._check(L.kgpu_fp64_peak(ctypes.byref(peak)), "kgpu_fp64_peak")
+    learned = learned_leg(k, rp, d_in, work, stream, n, st, it, args, dev)
 
     # e2e: the host-pointer entry point with pinned buffers, copies included
     hin = []
@@ -494,6 +555,7 @@ def our_arm_radcells(args, wl, rank, world, local_rank):
         "config": {"workload": wl["desc"], "cells_per_gpu": n, "l2": "inputs 2.2 GB > L2, no flush",
                    "parallelism": "replicas" if world > 1 else "one batch", "solver": "batched work queue"},
         "plain": {"value": plain_value, "unit": RAD_UNIT, "ms_per_step": ms_plain / steps_plain},
+        "learned": learned,
         "newton": {"mean_iterations_successful_attempt": float(it[ok].mean()),
                    "mean_iterations_all_attempts": stats[0] / n, "passes_with_work": int(stats[1]),
                    "success_rate": float(ok.mean()),

@@ -190,8 +190,11 @@ __global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypr
     for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = p0[i];
     W.wwarm[k] = 0;
   }
+  // the queue is chosen by the predicate, never by the pointer: every lane
+  // of a warp-aggregated push must name the same queue
   const int type = imp_attempt(0, sw).prim;
-  warp_push(W.q[0][type], W.count + 0 * 2 + type, true, k);
+  warp_push(W.q[0][0], W.count + 0, type == 0, k);
+  warp_push(W.q[0][1], W.count + 1, type == 1, k);
 }
 
 // Pass p: the cells of queue p may start up to K Newton iterations;
