@@ -62,8 +62,11 @@ KG_HD void mlp_guess(const double *pp0, const RadGeom &rg, int startwith, const 
   for (int i = 0; i < NVR; i++) guess[i] = pp0[i];
   guess[UU] = pp0[UU] * exp(t[0]);
   guess[EE0] = pp0[EE0] * exp(t[1]);
-  const int v = startwith == IMP_MHD ? VX : FX0;
-  for (int i = 0; i < 3; i++) guess[v + i] = pp0[v + i] + t[2 + i] / sqrt(gg[i + 1][i + 1]);
+  // the predicted velocity is used for the radiation frame only: a gas
+  // velocity guess moved by the prediction slows the gas-primitive Newton
+  // iteration down (measured), the radiation one speeds it up
+  if (startwith == IMP_RAD)
+    for (int i = 0; i < 3; i++) guess[FX0 + i] = pp0[FX0 + i] + t[2 + i] / sqrt(gg[i + 1][i + 1]);
 }
 
 }  // namespace kgpu

@@ -72,7 +72,8 @@ struct Work {
   int *wit;         // [n] its iteration count
   int *watt;        // [n] the running attempt (0..5)
   int *wsw;         // [n] which primitives the cascade starts with
-  int *wwarm;       // [n] the first attempt still runs from a predicted iterate
+  int *wwarm;       // [n] the cascade still runs from the predicted iterate
+  double *wguess;   // [n][13] the predicted iterate (warm start only)
   int *q[2][2];     // queues of cell indices [pass parity][primitives of the running attempt]
   int *count;       // [passes + 2][2] queue lengths
   unsigned long long *stats;  // [0] Newton iterations, [1] passes, [2] fallbacks of the warm start
@@ -92,6 +93,7 @@ size_t work_layout(int n, int passes, Work *w, char *base) {
   p = take((size_t)n * 4); if (w) w->watt = (int *)p;
   p = take((size_t)n * 4); if (w) w->wsw = (int *)p;
   p = take((size_t)n * 4); if (w) w->wwarm = (int *)p;
+  p = take((size_t)n * NVR * 8); if (w) w->wguess = (double *)p;
   for (int a = 0; a < 2; a++)
     for (int b = 0; b < 2; b++) {
       p = take((size_t)n * 4);
@@ -184,7 +186,10 @@ __global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypr
     double t[MLP_OUT], guess[NVR];
     for (int o = 0; o < MLP_OUT; o++) t[o] = ypred[(long)k * MLP_OUTP + o];
     mlp_guess(p0, rg, sw, t, guess);
-    for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = guess[i];
+    for (int i = 0; i < NVR; i++) {
+      W.wpp[(long)k * NVR + i] = guess[i];
+      W.wguess[(long)k * NVR + i] = guess[i];
+    }
     W.wwarm[k] = 1;
   } else {
     for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = p0[i];
@@ -224,7 +229,8 @@ __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, i
     const int warm0 = s.warm;
     int budget = K;
     int r;
-    while ((r = imp_advance(R, u0, p0, dt, rg, s, budget)) == IMP_RUNNING) {
+    const double *wg = W.wguess + (long)k * NVR;
+    while ((r = imp_advance(R, u0, p0, dt, rg, s, budget, wg)) == IMP_RUNNING) {
     }
     warp_add(W.stats, (unsigned)(K - budget));
     warp_add(W.stats + 2, (unsigned)(warm0 && !s.warm));

@@ -584,21 +584,20 @@ KG_HD void imp_begin(const RadParams &R, const double *pp00, const Geom &g, ImpS
   s.evals = 0;
 }
 
-// The attempt failed: the next one starts afresh from the guess.  A first
-// attempt started from a predicted iterate is first repeated from the
-// guess itself (the fallback of the learned warm start), so the cascade
-// that follows is exactly the reference's.
-KG_HD int imp_next_attempt(const double *pp00, ImpState &s) {
-  if (s.warm) {
-    s.warm = 0;
-    for (int i = 0; i < NVR; i++) s.pp[i] = pp00[i];
-    s.iter = 0;
-    s.phase = PH_BASE;
-    return IMP_RUNNING;
-  }
+// The attempt failed: the next one starts afresh, from the cell's guess, or
+// from the predicted iterate while the learned warm start is on.  When the
+// warm cascade has failed in every attempt, the reference cascade runs
+// from the guess (the fallback), so a cell fails only where the reference
+// fails.
+KG_HD int imp_next_attempt(const double *pp00, const double *warm_guess, ImpState &s) {
   s.att++;
-  if (s.att >= IMP_NATTEMPTS) return IMP_DONE_FAIL;
-  for (int i = 0; i < NVR; i++) s.pp[i] = pp00[i];
+  if (s.att >= IMP_NATTEMPTS) {
+    if (!s.warm) return IMP_DONE_FAIL;
+    s.warm = 0;
+    s.att = 0;
+  }
+  const double *start = s.warm ? warm_guess : pp00;
+  for (int i = 0; i < NVR; i++) s.pp[i] = start[i];
   s.iter = 0;
   s.phase = PH_BASE;
   return IMP_RUNNING;
@@ -609,7 +608,7 @@ KG_HD int imp_next_attempt(const double *pp00, ImpState &s) {
 // start of an iteration with no budget left the cell pauses (IMP_PAUSE)
 // with its state intact.
 KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00, double dt, const RadGeom &rg,
-                      ImpState &s, int &budget) {
+                      ImpState &s, int &budget, const double *warm_guess = nullptr) {
   const ImpParams P = imp_attempt(s.att, s.sw);
   const int sh = P.prim == IMP_MHD ? UU : EE0;
   const double CONV = P.eq == IMP_ENTROPY ? R.entrconv : R.conv;
@@ -656,9 +655,9 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
     fret = imp_residual(R, P, pin, uu, uu0, pp00, dt, rg, u2pret, corr, f, err);
   // transition
   if (s.phase == PH_BASE) {
-    if (fret < 0) return imp_next_attempt(pp00, s);
+    if (fret < 0) return imp_next_attempt(pp00, warm_guess, s);
     if (err < CONV) {
-      if (s.iter > R.maxiter) return imp_next_attempt(pp00, s);   // converged past the limit (rad.c:1051)
+      if (s.iter > R.maxiter) return imp_next_attempt(pp00, warm_guess, s);   // converged past the limit (rad.c:1051)
       s.phase = PH_FINAL;
       return IMP_RUNNING;
     }
@@ -671,7 +670,7 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
   if (s.phase == PH_JAC) {
     const int j = s.j;
     if (fret < 0) {
-      if (s.sign > 0.) return imp_next_attempt(pp00, s);
+      if (s.sign > 0.) return imp_next_attempt(pp00, warm_guess, s);
       s.sign = 1.;
       return IMP_RUNNING;
     }
@@ -680,7 +679,7 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
     s.sign = -1.;
     if (s.j == 4) {
       double iJ[4][4];
-      if (inverse_44(s.J, iJ) < 0) return imp_next_attempt(pp00, s);
+      if (inverse_44(s.J, iJ) < 0) return imp_next_attempt(pp00, warm_guess, s);
       for (int a = 0; a < 4; a++)
         for (int b = 0; b < 4; b++) s.J[a][b] = iJ[a][b];
       s.xiapp = 1.;
@@ -694,7 +693,7 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
     const double edenmin = s.ppp[sh] / R.maxdown;
     const double edenmax = s.ppp[sh] * R.maxup;
     if (xxx0 > edenmin && xxx0 < edenmax && u2pret >= -1) {
-      if (s.iter > R.maxiter) return imp_next_attempt(pp00, s);
+      if (s.iter > R.maxiter) return imp_next_attempt(pp00, warm_guess, s);
       s.phase = PH_BASE;
       return IMP_RUNNING;
     }
@@ -704,13 +703,13 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
     } else {
       s.xiapp /= R.dampfac;
     }
-    if (s.xiapp < R.maxdamping) return imp_next_attempt(pp00, s);
+    if (s.xiapp < R.maxdamping) return imp_next_attempt(pp00, warm_guess, s);
     return IMP_RUNNING;
   }
   // final inversion of the converged state (rad.c:1088-1150)
   for (int i = 0; i < NVR; i++) s.pp[i] = pin[i];
   if (P.prim == IMP_MHD && corr > 0) u2pret = -2;
-  if (u2pret < -1) return imp_next_attempt(pp00, s);
+  if (u2pret < -1) return imp_next_attempt(pp00, warm_guess, s);
   return IMP_DONE_OK;
 }
 

@@ -87,7 +87,8 @@ def test_mlp_training_lowers_the_loss(kgpu, torch):
 def test_warm_start_with_the_guess_itself_is_the_plain_solve(kgpu, torch):
     """A prediction of 'no change' makes the warm iterate the cell's own
     guess: every output equals the plain batched solve's, bit for bit, and
-    the fallbacks are exactly the cells whose first attempt fails."""
+    the fallbacks (cells whose whole warm cascade fails, then rerun from the
+    guess) are exactly the cells the plain solve cannot solve."""
     rp = kgpu.rad_params()
     uu, pp, g, G, dt = kgpu.rad_cells(8192, 21, rp)
     d = [torch.from_numpy(a).cuda() for a in (uu, pp, g, G, dt)]
@@ -96,8 +97,7 @@ def test_warm_start_with_the_guess_itself_is_the_plain_solve(kgpu, torch):
     b = kgpu.rad_solve_device(rp, *d, ypred=zero)
     for x, y in zip(a[:5], b[:5]):
         assert torch.equal(x, y)
-    first_failed = int((a[3] != 0).sum())
-    assert b[5][2] == first_failed
+    assert b[5][2] == int((a[2] != 0).sum())
 
 
 WEIGHTS = os.path.join(os.path.dirname(__file__), "..", "koral_b200", "data", "warmstart_mlp.npz")
@@ -106,7 +106,7 @@ WEIGHTS = os.path.join(os.path.dirname(__file__), "..", "koral_b200", "data", "w
 @pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="no trained warm-start weights")
 def test_trained_warm_start_cuts_newton_iterations(kgpu, torch):
     """The trained network (held-out cells, seed not used in training): mean
-    Newton iterations of the succeeding attempt at least 1.5x lower than the
+    Newton iterations of the succeeding attempt at least 1.8x lower than the
     plain solve, same success on 99% of the cells."""
     from koral_b200 import train_warmstart
     m = train_warmstart.load(kgpu, WEIGHTS)
@@ -123,4 +123,4 @@ def test_trained_warm_start_cuts_newton_iterations(kgpu, torch):
     print(f"iterations plain {ip[ok].mean():.3f} learned {iw[ok].mean():.3f}; fallbacks {warm[5][2]}; "
           f"status agree {np.mean(sp == sw):.4f}")
     assert np.mean(sp == sw) >= 0.99
-    assert iw[ok].mean() * 1.5 <= ip[ok].mean()
+    assert iw[ok].mean() * 1.8 <= ip[ok].mean()
