@@ -5,7 +5,7 @@
 // give every cell of a batched implicit solve its initial iterate.
 //
 // Tile of work: a warp carries 16 samples (the M dimension of one mma);
-// a block of four warps 64.  Weights sit in shared memory as BF16, laid
+// a training block of four warps 64; an inference block has sixteen warps.  Weights sit in shared memory as BF16, laid
 // out [output][input] so that a B fragment is two 32-bit loads.  FP32
 // master weights, their gradients and Adam moments stay in global memory.
 #include <cuda_bf16.h>
@@ -141,45 +141,70 @@ __device__ void load_weights(SmemW &w, const Bf16Weights W, const float *blob) {
   for (int i = threadIdx.x; i < MLP_OUTP; i += blockDim.x) w.b3[i] = blob[OB3 + i];
 }
 
-// forward pass of one warp's 16 samples (x already in sw.x); leaves z1, z2,
-// a1, a2 and the standardised outputs y
-__device__ void warp_forward(const SmemW &w, SmemWarp &sw) {
+// forward pass of one warp's 16 samples (x already in x); leaves a1, a2,
+// the standardised outputs y and, for training, the pre-activations z1, z2.
+// Layer 2 keeps all 16 output tiles in flight (16 independent accumulator
+// chains), so the tensor-core latency of one chain is hidden by the others.
+template <bool TRAIN>
+__device__ void warp_forward_t(const SmemW &w, const bf16 *x, bf16 *a1s, bf16 *a2s, float *z1s, float *z2s,
+                               float *ys) {
   const int g = lane_id() >> 2, t = lane_id() & 3;
   uint32_t a[4], b[2];
   // layer 1: 16 x 16 . 16 x 128
-  load_a(a, sw.x, LDX, 0);
+  load_a(a, x, LDX, 0);
   for (int nt = 0; nt < MLP_H / 8; nt++) {
     const int c0 = nt * 8 + 2 * t;
     float c[4] = {w.b1[c0], w.b1[c0 + 1], w.b1[c0], w.b1[c0 + 1]};
     load_b_nk(b, w.w1t, LDX, nt * 8, 0);
     mma16816(c, a, b);
-    sw.z1[g * MLP_H + c0] = c[0];
-    sw.z1[g * MLP_H + c0 + 1] = c[1];
-    sw.z1[(g + 8) * MLP_H + c0] = c[2];
-    sw.z1[(g + 8) * MLP_H + c0 + 1] = c[3];
-    sw.a1[g * LDH + c0] = __float2bfloat16(silu(c[0]));
-    sw.a1[g * LDH + c0 + 1] = __float2bfloat16(silu(c[1]));
-    sw.a1[(g + 8) * LDH + c0] = __float2bfloat16(silu(c[2]));
-    sw.a1[(g + 8) * LDH + c0 + 1] = __float2bfloat16(silu(c[3]));
+    if (TRAIN) {
+      z1s[g * MLP_H + c0] = c[0];
+      z1s[g * MLP_H + c0 + 1] = c[1];
+      z1s[(g + 8) * MLP_H + c0] = c[2];
+      z1s[(g + 8) * MLP_H + c0 + 1] = c[3];
+    }
+    a1s[g * LDH + c0] = __float2bfloat16(silu(c[0]));
+    a1s[g * LDH + c0 + 1] = __float2bfloat16(silu(c[1]));
+    a1s[(g + 8) * LDH + c0] = __float2bfloat16(silu(c[2]));
+    a1s[(g + 8) * LDH + c0 + 1] = __float2bfloat16(silu(c[3]));
   }
   __syncwarp();
   // layer 2: 16 x 128 . 128 x 128
-  for (int nt = 0; nt < MLP_H / 8; nt++) {
-    const int c0 = nt * 8 + 2 * t;
-    float c[4] = {w.b2[c0], w.b2[c0 + 1], w.b2[c0], w.b2[c0 + 1]};
-    for (int ks = 0; ks < MLP_H / 16; ks++) {
-      load_a(a, sw.a1, LDH, ks * 16);
-      load_b_nk(b, w.w2t, LDH, nt * 8, ks * 16);
-      mma16816(c, a, b);
+  {
+    float c[MLP_H / 8][4];
+#pragma unroll
+    for (int nt = 0; nt < MLP_H / 8; nt++) {
+      const int c0 = nt * 8 + 2 * t;
+      c[nt][0] = w.b2[c0];
+      c[nt][1] = w.b2[c0 + 1];
+      c[nt][2] = w.b2[c0];
+      c[nt][3] = w.b2[c0 + 1];
     }
-    sw.z2[g * MLP_H + c0] = c[0];
-    sw.z2[g * MLP_H + c0 + 1] = c[1];
-    sw.z2[(g + 8) * MLP_H + c0] = c[2];
-    sw.z2[(g + 8) * MLP_H + c0 + 1] = c[3];
-    sw.a2[g * LDH + c0] = __float2bfloat16(silu(c[0]));
-    sw.a2[g * LDH + c0 + 1] = __float2bfloat16(silu(c[1]));
-    sw.a2[(g + 8) * LDH + c0] = __float2bfloat16(silu(c[2]));
-    sw.a2[(g + 8) * LDH + c0 + 1] = __float2bfloat16(silu(c[3]));
+#pragma unroll
+    for (int ks = 0; ks < MLP_H / 16; ks++) {
+      load_a(a, a1s, LDH, ks * 16);
+#pragma unroll
+      for (int nt = 0; nt < MLP_H / 8; nt++) {
+        load_b_nk(b, w.w2t, LDH, nt * 8, ks * 16);
+        mma16816(c[nt], a, b);
+      }
+    }
+    // every lane has read its a1 fragments: a2 may overwrite a1
+    __syncwarp();
+#pragma unroll
+    for (int nt = 0; nt < MLP_H / 8; nt++) {
+      const int c0 = nt * 8 + 2 * t;
+      if (TRAIN) {
+        z2s[g * MLP_H + c0] = c[nt][0];
+        z2s[g * MLP_H + c0 + 1] = c[nt][1];
+        z2s[(g + 8) * MLP_H + c0] = c[nt][2];
+        z2s[(g + 8) * MLP_H + c0 + 1] = c[nt][3];
+      }
+      a2s[g * LDH + c0] = __float2bfloat16(silu(c[nt][0]));
+      a2s[g * LDH + c0 + 1] = __float2bfloat16(silu(c[nt][1]));
+      a2s[(g + 8) * LDH + c0] = __float2bfloat16(silu(c[nt][2]));
+      a2s[(g + 8) * LDH + c0 + 1] = __float2bfloat16(silu(c[nt][3]));
+    }
   }
   __syncwarp();
   // layer 3: 16 x 128 . 128 x 8
@@ -187,40 +212,55 @@ __device__ void warp_forward(const SmemW &w, SmemWarp &sw) {
     const int c0 = 2 * t;
     float c[4] = {w.b3[c0], w.b3[c0 + 1], w.b3[c0], w.b3[c0 + 1]};
     for (int ks = 0; ks < MLP_H / 16; ks++) {
-      load_a(a, sw.a2, LDH, ks * 16);
+      load_a(a, a2s, LDH, ks * 16);
       load_b_nk(b, w.w3t, LDH, 0, ks * 16);
       mma16816(c, a, b);
     }
-    sw.y[g * MLP_OUTP + c0] = c[0];
-    sw.y[g * MLP_OUTP + c0 + 1] = c[1];
-    sw.y[(g + 8) * MLP_OUTP + c0] = c[2];
-    sw.y[(g + 8) * MLP_OUTP + c0 + 1] = c[3];
+    ys[g * MLP_OUTP + c0] = c[0];
+    ys[g * MLP_OUTP + c0 + 1] = c[1];
+    ys[(g + 8) * MLP_OUTP + c0] = c[2];
+    ys[(g + 8) * MLP_OUTP + c0 + 1] = c[3];
   }
   __syncwarp();
 }
 
-__device__ void load_x_tile(SmemWarp &sw, const float *X, int n, int s0) {
+__device__ inline void warp_forward(const SmemW &w, SmemWarp &sw) {
+  warp_forward_t<true>(w, sw.x, sw.a1, sw.a2, sw.z1, sw.z2, sw.y);
+}
+
+// per warp, inference only: no pre-activations are kept and the second
+// layer's activations overwrite the first's
+struct SmemWarpInfer {
+  bf16 x[16 * LDX];
+  bf16 a[16 * LDH];
+  float y[16 * MLP_OUTP];
+};
+// 16 warps of 124 registers fill the register file of an SM
+constexpr int kInferWarps = 16;
+
+__device__ void load_x_tile(bf16 *x, const float *X, int n, int s0) {
   for (int i = lane_id(); i < 16 * MLP_IN; i += 32) {
     const int r = i / MLP_IN, f = i % MLP_IN;
     const int sidx = s0 + r;
-    sw.x[r * LDX + f] = __float2bfloat16(sidx < n ? X[(long)sidx * MLP_IN + f] : 0.f);
+    x[r * LDX + f] = __float2bfloat16(sidx < n ? X[(long)sidx * MLP_IN + f] : 0.f);
   }
   __syncwarp();
 }
 
-// inference: Y[n][8] = unstandardised outputs
-__global__ void __launch_bounds__(128) k_mlp_forward(const float *blob, Bf16Weights W, const float *X, int n,
-                                                     float *Y) {
+// inference: Y[n][8] = unstandardised outputs; the block's warps share the
+// weights
+__global__ void __launch_bounds__(32 * kInferWarps) k_mlp_forward(const float *blob, Bf16Weights W, const float *X,
+                                                                  int n, float *Y) {
   extern __shared__ __align__(16) unsigned char smem[];
   SmemW &w = *reinterpret_cast<SmemW *>(smem);
-  SmemWarp &sw = reinterpret_cast<SmemWarp *>(smem + sizeof(SmemW))[threadIdx.x >> 5];
+  SmemWarpInfer &sw = reinterpret_cast<SmemWarpInfer *>(smem + sizeof(SmemW))[threadIdx.x >> 5];
   load_weights(w, W, blob);
   __syncthreads();
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int s0 = warp * 16; s0 < n; s0 += nwarps * 16) {
-    load_x_tile(sw, X, n, s0);
-    warp_forward(w, sw);
+    load_x_tile(sw.x, X, n, s0);
+    warp_forward_t<false>(w, sw.x, sw.a, sw.a, nullptr, nullptr, sw.y);
     for (int i = lane_id(); i < 16 * MLP_OUTP; i += 32) {
       const int r = i / MLP_OUTP, o = i % MLP_OUTP;
       if (s0 + r < n) Y[(long)(s0 + r) * MLP_OUTP + o] = sw.y[i] * blob[OSCALE + o] + blob[OMEAN + o];
@@ -379,7 +419,7 @@ __global__ void k_mlp_to_bf16(const float *blob, Bf16Weights W) {
   }
 }
 
-size_t smem_forward() { return sizeof(SmemW) + 4 * sizeof(SmemWarp); }
+size_t smem_forward() { return sizeof(SmemW) + kInferWarps * sizeof(SmemWarpInfer); }
 size_t smem_train() { return sizeof(SmemW) + 4 * sizeof(SmemWarp) + sizeof(SmemBlock); }
 
 int sm_count_mlp() {
@@ -487,10 +527,10 @@ extern "C" int kgpu_mlp_forward(kgpu_mlp *M, const float *X, int n, float *Y, vo
   if (!M || n < 0 || (n > 0 && (!X || !Y))) return KGPU_EINVAL;
   if (n == 0) return 0;
   const int tiles = (n + 15) / 16;
-  int blocks = (tiles + 3) / 4;
-  const int cap = sm_count_mlp() * 2;
+  int blocks = (tiles + kInferWarps - 1) / kInferWarps;
+  const int cap = sm_count_mlp();
   if (blocks > cap) blocks = cap;
-  k_mlp_forward<<<blocks, 128, smem_forward(), (cudaStream_t)stream>>>(M->blob, M->W, X, n, Y);
+  k_mlp_forward<<<blocks, 32 * kInferWarps, smem_forward(), (cudaStream_t)stream>>>(M->blob, M->W, X, n, Y);
   MCK(cudaGetLastError());
   return 0;
 }
