@@ -70,7 +70,7 @@ typedef struct kgpu_ctx kgpu_ctx;
 typedef struct {
   int nx, ny, nz;          /* TNX, TNY, TNZ (one subdomain)                  */
   int ng;                  /* ghost layers, NG (3 for PPM, 4 for MP5)        */
-  int nv;                  /* variables per cell, NV (9: MHD)                 */
+  int nv;                  /* variables per cell, NV (9: MHD; 13: MHD + M1)   */
   int int_order;           /* KGPU_PPM or KGPU_MP5                           */
   int fluxmethod;          /* KGPU_LAXF or KGPU_HLL                          */
   int axisym_metric;       /* METRICAXISYMMETRIC: one phi slice of metric     */
@@ -121,7 +121,8 @@ int kgpu_download_array(kgpu_ctx *ctx, int which, double *out);
 /* op_explicit(t,dt), finite.c:646-1234 (set_bc, wavespeeds, reconstruction,
  * face fluxes, flux-CT, unsplit update with metric source terms). */
 int kgpu_op_explicit(kgpu_ctx *ctx, double t, double dt);
-/* op_implicit(t,dt), finite.c:1241-1292: radiation source; a no-op for MHD. */
+/* op_implicit(t,dt), finite.c:1241-1292: the implicit radiation source step
+ * over the domain and its fixup (kgpu_set_radiation); a no-op for MHD. */
 int kgpu_op_implicit(kgpu_ctx *ctx, double t, double dt);
 /* calc_u2p(), finite.c:501-561: inversion, floors, fixups, set_bc. */
 int kgpu_calc_u2p(kgpu_ctx *ctx);
@@ -151,9 +152,14 @@ int kgpu_rk2_steps_graph(kgpu_ctx *ctx, int nsteps);
  * out[0] cells flagged for fixup, out[1] entropy inversions,
  * out[2] failed inversions (old primitives kept), out[3] negative densities. */
 int kgpu_get_counters(kgpu_ctx *ctx, unsigned long long out[4]);
-/* All counters (up to n): the four above, then Newton steps of the energy
- * and of the entropy solves, energy solves paused after the first pass, and
- * cells handed to the entropy equation.  Returns how many were written. */
+/* All counters (up to n, 16 in all): the four above, then Newton steps of
+ * the energy and of the entropy solves, energy solves paused after the first
+ * pass, cells handed to the entropy equation; with radiation: [8] M1
+ * inversions corrected (U2PRAD fixup requests), [9] implicit solves where
+ * every attempt failed (RADIMP fixups), [10] their Newton iterations over
+ * all attempts, [11] passes of the batched solver with work, [12] warm-start
+ * fallbacks, [13] implicit solves, [14] cells where the radiation floors
+ * acted.  Returns how many were written. */
 int kgpu_get_counters_ex(kgpu_ctx *ctx, unsigned long long *out, int n);
 /* Tuning: Newton steps a cell may take in the first inversion pass before
  * it is queued for the resumption pass (default 8; results do not depend
@@ -271,6 +277,8 @@ typedef struct {
                                        /* RADIMPLICITMAXENCHANGEDOWN/UP           */
   double maxdamping, threshold;        /* MAXRADIMPDAMPING, RADIMPLICITTHRESHOLD  */
   double u2pconv;                      /* U2PCONV of the nested MHD inversion     */
+  double eerhoratiomin, eerhoratiomax; /* EERHORATIOMIN/MAX: radiation floors     */
+  double eeuuratiomin, eeuuratiomax;   /* EEUURATIOMIN/MAX                        */
 } kgpu_rad_params;
 
 /* KORAL's defaults (choices.h:320-597, ko.h:17-48) for a black hole of
@@ -361,6 +369,36 @@ int kgpu_ks_metric_batch(double a, int n, const double *r, const double *th, dou
  * contraction, as the library's kernels are built): the denominator of the
  * FP64 roofline of the solver kernels. */
 int kgpu_fp64_peak(double *ops_per_s);
+
+/* Radiation in the grid step (nv = 13: the nine MHD variables, then E and
+ * the radiation frame's relative four-velocity; conserved R^t_t, R^t_i).
+ * kgpu_set_radiation switches a 13-variable context to the RADIATION build
+ * of the time loop: M1 fluxes and characteristic speeds in op_explicit
+ * (optionally with the optical-depth limiter of calc_rad_wavespeeds,
+ * rad.c:2489-2502), u2p_rad and check_floors_rad in calc_u2p, and the
+ * implicit lab-frame source solve in op_implicit (finite.c:1242-1292) with
+ * the RADIMP fixup.  rp->gamma must equal the grid's adiabatic index.
+ * Allocates the solver's buffers for the domain cells once. */
+int kgpu_set_radiation(kgpu_ctx *ctx, const kgpu_rad_params *rp, int wavespeed_limiter);
+/* Solver of op_implicit: KGPU_RAD_PLAIN or KGPU_RAD_BATCHED (default), and
+ * the warm-start network (batched only; null for the reference's guess).
+ * The network is borrowed: it must outlive its use by the context. */
+int kgpu_set_implicit_solver(kgpu_ctx *ctx, int mode, kgpu_mlp *warm);
+/* Whole RK2IMEX steps (ko.c:444-570), dt in device memory; and the same
+ * replayed from a CUDA graph captured on the first call. */
+int kgpu_rk2imex_steps(kgpu_ctx *ctx, int nsteps);
+int kgpu_rk2imex_steps_graph(kgpu_ctx *ctx, int nsteps);
+
+/* The radiative torus (nv = 13): the pressure of the torus shared by gas and
+ * M1 radiation in thermal equilibrium at one temperature (radiation frame
+ * comoving with the gas), the atmosphere with a radiation energy of eradatm
+ * times its gas energy at rest with it; host-only state, and the whole
+ * set-up on a context with radiation switched on (kgpu_set_radiation). */
+int kgpu_fm_radtorus_state(const kgpu_torus_params *tp, const kgpu_rad_params *rp, double eradatm,
+                           const kgpu_config *cfg, const double *xbx, const double *xby, const double *xbz,
+                           const double *g, const double *G, double *u, double *p);
+int kgpu_init_fm_radtorus(kgpu_ctx *ctx, const kgpu_torus_params *tp, const kgpu_rad_params *rp, double eradatm,
+                          int wavespeed_limiter);
 
 /* Last CUDA error string of this thread's most recent failing call. */
 const char *kgpu_last_error(void);

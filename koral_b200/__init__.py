@@ -30,7 +30,8 @@ class RadParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "gamma", "kb", "mp", "sigma", "mu", "ggg", "ccc", "masscm", "kramers", "kes", "kes_gu", "gammamaxrad",
         "eradfloor", "gammasmalllimit", "numepsilon", "eps", "conv", "entrconv", "maxiter", "dampfac", "maxdown",
-        "maxup", "maxdamping", "threshold", "u2pconv")]
+        "maxup", "maxdamping", "threshold", "u2pconv", "eerhoratiomin", "eerhoratiomax", "eeuuratiomin",
+        "eeuuratiomax")]
 
 
 class KgpuError(RuntimeError):
@@ -156,6 +157,16 @@ def lib():
         L.kgpu_mlp_train_epoch.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                            ctypes.c_ulonglong, _dp]
         L.kgpu_u2p_cells_static.argtypes = sig["kgpu_u2p_cells"]
+        for name, args in (("kgpu_fm_radtorus_state", [ctypes.POINTER(TorusParams), rpp, ctypes.c_double,
+                                                        ctypes.POINTER(Config)] + [_dp] * 7),
+                           ("kgpu_init_fm_radtorus", [vp, ctypes.POINTER(TorusParams), rpp, ctypes.c_double,
+                                                      ctypes.c_int]),
+                           ("kgpu_set_radiation", [vp, rpp, ctypes.c_int]),
+                           ("kgpu_set_implicit_solver", [vp, ctypes.c_int, vp]),
+                           ("kgpu_rk2imex_steps", [vp, ctypes.c_int]),
+                           ("kgpu_rk2imex_steps_graph", [vp, ctypes.c_int])):
+            getattr(L, name).argtypes = args
+            getattr(L, name).restype = ctypes.c_int
         L.kgpu_u2p_cells_static.restype = ctypes.c_int
         L.kgpu_u2p_cells_static_error.restype = ctypes.c_char_p
         L.kgpu_abi_version.restype = ctypes.c_int
@@ -327,12 +338,32 @@ class Subdomain:
         _check(fn(self.h, int(n)), "kgpu_rk2_steps")
 
     def counters(self):
-        a = (ctypes.c_ulonglong * 8)()
-        n = self.L.kgpu_get_counters_ex(self.h, a, 8)
+        a = (ctypes.c_ulonglong * 16)()
+        n = self.L.kgpu_get_counters_ex(self.h, a, 16)
         if n < 0:
             _check(n, "kgpu_get_counters_ex")
         return dict(fixups=a[0], entropy=a[1], failed=a[2], negrho=a[3], iters_energy=a[4], iters_entropy=a[5],
-                    paused=a[6], to_entropy=a[7])
+                    paused=a[6], to_entropy=a[7], rad_corrected=a[8], radimp_failed=a[9], imp_iters=a[10],
+                    imp_passes=a[11], imp_fallbacks=a[12], imp_solves=a[13], rad_floors=a[14])
+
+    def set_radiation(self, rp, wavespeed_limiter=False):
+        """Radiation in the step (nv = 13): M1 fluxes and speeds, u2p_rad and
+        radiation floors, the implicit source operator (kgpu_set_radiation)."""
+        self._rp = rp
+        _check(self.L.kgpu_set_radiation(self.h, ctypes.byref(rp), int(bool(wavespeed_limiter))),
+               "kgpu_set_radiation")
+
+    def set_implicit_solver(self, mode=None, warm=None):
+        """Solver of op_implicit (RAD_PLAIN or RAD_BATCHED) and the warm-start
+        network (an Mlp, kept alive by this object), or None."""
+        mode = RAD_BATCHED if mode is None else mode
+        self._warm = warm
+        _check(self.L.kgpu_set_implicit_solver(self.h, int(mode), warm.h if warm is not None else None),
+               "kgpu_set_implicit_solver")
+
+    def rk2imex_steps(self, n=1, graph=False):
+        fn = self.L.kgpu_rk2imex_steps_graph if graph else self.L.kgpu_rk2imex_steps
+        _check(fn(self.h, int(n)), "kgpu_rk2imex_steps")
 
     def set_u2p_pass_iters(self, n):
         _check(self.L.kgpu_set_u2p_pass_iters(self.h, int(n)), "kgpu_set_u2p_pass_iters")
@@ -484,6 +515,41 @@ def fm_torus_state(tp, cfg, xb, g, G):
                                      _ptr(np.ascontiguousarray(g)), _ptr(np.ascontiguousarray(G)), _ptr(u), _ptr(p)),
            "kgpu_fm_torus_state")
     return u, p
+
+
+def fm_radtorus_state(tp, rp, eradatm, cfg, xb, g, G):
+    """The radiative torus state (nv = 13), host arrays in KORAL layout."""
+    sx, sy, sz = cfg.nx + 2 * cfg.ng, cfg.ny + 2 * cfg.ng, cfg.nz + 2 * cfg.ng
+    u = np.zeros((sz, sy, sx, cfg.nv))
+    p = np.zeros((sz, sy, sx, cfg.nv))
+    xb = [np.ascontiguousarray(x, dtype=np.float64) for x in xb]
+    _check(lib().kgpu_fm_radtorus_state(ctypes.byref(tp), ctypes.byref(rp), float(eradatm), ctypes.byref(cfg),
+                                        *[_ptr(x) for x in xb], _ptr(np.ascontiguousarray(g)),
+                                        _ptr(np.ascontiguousarray(G)), _ptr(u), _ptr(p)),
+           "kgpu_fm_radtorus_state")
+    return u, p
+
+
+RADTORUS_MASS = 1.e16      # black-hole mass (Msun) of the radiative torus: sets the radiation units
+RADTORUS_ERADATM = 1.e-6   # atmosphere radiation energy relative to its gas energy
+
+
+def radtorus_config(nx=256, ny=128, nz=64):
+    """The torus configuration with M1 radiation (13 variables)."""
+    cfg = torus_config(nx, ny, nz)
+    cfg.nv = 13
+    return cfg
+
+
+def radtorus(nx=256, ny=128, nz=64, tp=None, rp=None, eradatm=RADTORUS_ERADATM, wavespeed_limiter=False):
+    """A Subdomain holding the radiative torus, radiation switched on."""
+    tp = tp or torus_params()
+    rp = rp or rad_params(mass=RADTORUS_MASS, gamma=13.0 / 9.0)
+    s = Subdomain(radtorus_config(nx, ny, nz))
+    s._rp = rp
+    _check(lib().kgpu_init_fm_radtorus(s.h, ctypes.byref(tp), ctypes.byref(rp), float(eradatm),
+                                       int(bool(wavespeed_limiter))), "kgpu_init_fm_radtorus")
+    return s
 
 
 # ---------------------------------------------------------------------------

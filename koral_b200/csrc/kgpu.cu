@@ -25,7 +25,7 @@
 #include <vector>
 
 #include "../../include/koral_b200.h"
-#include "kgpu_physics.cuh"
+#include "kgpu_rad.cuh"
 
 using namespace kgpu;
 
@@ -88,6 +88,15 @@ __device__ inline void store_cell(double *arr, long ncell, long c, const double 
 #pragma unroll
   for (int iv = 0; iv < NVMAX; iv++) arr[iv * ncell + c] = v[iv];
 }
+// the four radiation variables (EE0..FZ0) of a 13-variable grid
+__device__ inline void load_rad(const double *arr, long ncell, long c, double *v) {
+#pragma unroll
+  for (int iv = EE0; iv <= FZ0; iv++) v[iv] = arr[iv * ncell + c];
+}
+__device__ inline void store_rad(double *arr, long ncell, long c, const double *v) {
+#pragma unroll
+  for (int iv = EE0; iv <= FZ0; iv++) arr[iv * ncell + c] = v[iv];
+}
 
 // ---------------------------------------------------------------------------
 // boundary conditions (set_bc, finite.c:2752-2803; set_bc_core 2673-2748)
@@ -113,22 +122,31 @@ __global__ void k_bc_faces(Grid G, Box b) {
     if (d > 0 && n < G.ng) s3[d] = 0;   // finite.c:2705, 2720
   }
   long c = cell_index(G, ix, iy, iz), s = cell_index(G, s3[0], s3[1], s3[2]);
-  double pp[NVMAX], uu[NVMAX];
+  double pp[NVR], uu[NVR];
   load_cell(G.p, G.ncell, s, pp);
+  if (G.rad) load_rad(G.p, G.ncell, s, pp);
   if (flip) {
-    // the component normal to the boundary: VX/B1 for x, VY/B2 for y, VZ/B3 for z
+    // the component normal to the boundary: VX/B1 for x, VY/B2 for y, VZ/B3
+    // for z, and the radiation frame's FX0/FY0/FZ0
     pp[VX + d] = -pp[VX + d];
     pp[B1 + d] = -pp[B1 + d];
+    if (G.rad) pp[FX0 + d] = -pp[FX0 + d];
   }
   if (kind == KGPU_BC_PERIODIC_COPY) {
     load_cell(G.u, G.ncell, s, uu);
+    if (G.rad) load_rad(G.u, G.ncell, s, uu);
   } else {
     Geom g;
     geom_centre(G, ix, iy, iz, g);
     p2u_full(G, pp, uu, g);
+    if (G.rad) p2u_rad(pp, uu, g);
   }
   store_cell(G.p, G.ncell, c, pp);
   store_cell(G.u, G.ncell, c, uu);
+  if (G.rad) {
+    store_rad(G.p, G.ncell, c, pp);
+    store_rad(G.u, G.ncell, c, uu);
+  }
 }
 
 // Corners of a 2D periodic domain, filled as the reference does
@@ -178,8 +196,9 @@ __global__ void k_bc_corners2d(Grid G) {
   int k = op % (2 * G.ng);
   bool avg = k >= 2 * (G.ng - 1);
   long ca = cell_index(G, ax, ay, 0), cb = cell_index(G, bx, by, 0), c = cell_index(G, tx, ty, 0);
-  double pp[NVMAX], uu[NVMAX];
-  for (int iv = 0; iv < NVMAX; iv++) {
+  double pp[NVR], uu[NVR];
+  const int nv = G.rad ? NVR : NVMAX;
+  for (int iv = 0; iv < nv; iv++) {
     double a = G.p[iv * G.ncell + ca];
     pp[iv] = avg ? .5 * (a + G.p[iv * G.ncell + cb]) : a;
   }
@@ -188,6 +207,11 @@ __global__ void k_bc_corners2d(Grid G) {
   p2u_full(G, pp, uu, g);
   store_cell(G.p, G.ncell, c, pp);
   store_cell(G.u, G.ncell, c, uu);
+  if (G.rad) {
+    p2u_rad(pp, uu, g);
+    store_rad(G.p, G.ncell, c, pp);
+    store_rad(G.u, G.ncell, c, uu);
+  }
 }
 
 // Edges and corners of a 3D domain with physical boundaries, in the
@@ -200,8 +224,9 @@ __global__ void k_bc_corners2d(Grid G) {
 __device__ inline void set_from(const Grid &G, int tx, int ty, int tz, int s1x, int s1y, int s1z, int s2x, int s2y,
                                 int s2z, bool avg) {
   long c = cell_index(G, tx, ty, tz), a = cell_index(G, s1x, s1y, s1z), b = cell_index(G, s2x, s2y, s2z);
-  double pp[NVMAX], uu[NVMAX];
-  for (int iv = 0; iv < NVMAX; iv++) {
+  double pp[NVR], uu[NVR];
+  const int nv = G.rad ? NVR : NVMAX;
+  for (int iv = 0; iv < nv; iv++) {
     double va = G.p[iv * G.ncell + a];
     pp[iv] = avg ? .5 * (va + G.p[iv * G.ncell + b]) : va;
   }
@@ -210,6 +235,11 @@ __device__ inline void set_from(const Grid &G, int tx, int ty, int tz, int s1x, 
   p2u_full(G, pp, uu, g);
   store_cell(G.p, G.ncell, c, pp);
   store_cell(G.u, G.ncell, c, uu);
+  if (G.rad) {
+    p2u_rad(pp, uu, g);
+    store_rad(G.p, G.ncell, c, pp);
+    store_rad(G.u, G.ncell, c, uu);
+  }
 }
 // one line of one elongated-edge pass.  Edge axis c, the two other axes
 // (a, b); corner k: bit 1 = high end of a, bit 0 = high end of b; position t
@@ -305,7 +335,7 @@ __global__ void k_wavespeeds(Grid G, Box b) {
   double tsd = -1.;
   if (box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) {
     long c = cell_index(G, ix, iy, iz);
-    double pp[NVMAX];
+    double pp[NVR];
     load_cell(G.p, G.ncell, c, pp);
     Geom g;
     geom_centre(G, ix, iy, iz, g);
@@ -316,10 +346,34 @@ __global__ void k_wavespeeds(Grid G, Box b) {
       G.al[d][c] = al[d];
       G.ar[d][c] = ar[d];
     }
+    double wsx = dmax(fabs(al[0]), fabs(ar[0]));
+    double wsy = dmax(fabs(al[1]), fabs(ar[1]));
+    double wsz = dmax(fabs(al[2]), fabs(ar[2]));
+    if (G.rad) {
+      // radiative characteristics (physics.c:170-197), stored apart for
+      // the radiation fluxes; the time step takes the faster of the two
+      load_rad(G.p, G.ncell, c, pp);
+      double tau[3] = {0., 0., 0.};
+      if (G.rad_limiter) {
+        const int ic[3] = {ix, iy, iz};
+        double lo[3], hi[3];
+        for (int d = 0; d < 3; d++) {
+          lo[d] = size_x(G, ic[d], d);
+          hi[d] = size_x(G, ic[d] + 1, d);
+        }
+        rad_tautot(*G.radp, pp, g, lo, hi, tau);
+      }
+      double rl[3], rr[3];
+      rad_wavespeeds(pp, g, tau, G.rad_limiter != 0, rl, rr);
+      for (int d = 0; d < 3; d++) {
+        G.arl[d][c] = rl[d];
+        G.arr[d][c] = rr[d];
+      }
+      wsx = dmax(wsx, dmax(fabs(rl[0]), fabs(rr[0])));
+      wsy = dmax(wsy, dmax(fabs(rl[1]), fabs(rr[1])));
+      wsz = dmax(wsz, dmax(fabs(rl[2]), fabs(rr[2])));
+    }
     if (in_domain(G, ix, iy, iz)) {
-      double wsx = dmax(fabs(al[0]), fabs(ar[0]));
-      double wsy = dmax(fabs(al[1]), fabs(ar[1]));
-      double wsz = dmax(fabs(al[2]), fabs(ar[2]));
       double dx = size_x(G, ix, 0), dy = size_x(G, iy, 1), dz = size_x(G, iz, 2);
       double tstepden;
       if (G.nz > 1 && G.ny > 1) tstepden = wsx / dx + wsy / dy + wsz / dz;
@@ -425,6 +479,81 @@ __global__ void __launch_bounds__(128, 4) k_flux(Grid G, Box b) {
       else fl = (-al * fR + ar * fL + al * ar * (uR - uL)) / (ar - al);
     }
     out[iv * nf] = fl;
+  }
+}
+
+// Radiative face fluxes (the EE0..FZ0 part of the same face loop): the
+// reference reconstructs all thirteen variables together, but nothing of
+// the radiation flux depends on the gas state of the face (the face floors
+// touch gas variables only, f_flux_prime_rad and the conserved variables
+// of the Riemann solver read the radiation primitives and the metric), so
+// the radiation runs as its own kernel with the same two-lane layout and
+// its own characteristic speeds (f_calc_fluxes_at_faces, finite.c:1379-1395).
+template <int D>
+__global__ void __launch_bounds__(128) k_flux_rad(Grid G, Box b) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int side = (int)(t & 1);
+  int ix, iy, iz;
+  const bool valid = box_coord(b, t >> 1, ix, iy, iz);
+  const unsigned pairmask = __ballot_sync(0xffffffffu, valid);
+  if (!valid) return;
+  const int i = D == 0 ? ix : (D == 1 ? iy : iz);
+  const long stride = D == 0 ? 1 : (D == 1 ? (long)G.sx : (long)G.sx * G.sy);
+  const long cR = cell_index(G, ix, iy, iz);
+  const long cL = cR - stride;
+  double ps[NVR];
+  if (G.int_order == 4) {
+    const long c0 = side ? cR + 2 * stride : cR - 3 * stride;
+    const long st = side ? -stride : stride;
+#pragma unroll
+    for (int iv = EE0; iv <= FZ0; iv++) {
+      const double *pv = G.p + iv * G.ncell + c0;
+      ps[iv] = mp5_face(pv[0], pv[st], pv[2 * st], pv[3 * st], pv[4 * st]);
+    }
+  } else {
+    const int i0 = i - 3 + side;
+    double dx[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) dx[k] = size_x(G, i0 + k, D);
+    const long c0 = cR + (side - 3) * stride;
+#pragma unroll
+    for (int iv = EE0; iv <= FZ0; iv++) {
+      const double *pv = G.p + iv * G.ncell + c0;
+      double ul, ur;
+      ppm(pv[0], pv[stride], pv[2 * stride], pv[3 * stride], pv[4 * stride], dx[0], dx[1], dx[2], dx[3], dx[4], ul,
+          ur);
+      ps[iv] = side ? ul : ur;
+    }
+  }
+  Geom g;
+  geom_face(G, ix, iy, iz, D, g);
+  double fs[4], us[NVR];
+  rad_flux(ps, D, g, fs);
+  p2u_rad(ps, us, g);
+  double ap1l = G.arl[D][cR], ap1r = G.arr[D][cR], am1l = G.arl[D][cL], am1r = G.arr[D][cL];
+  double ap1 = dmax(fabs(ap1l), fabs(ap1r)), am1 = dmax(fabs(am1l), fabs(am1r));
+  double ag = dmax(ap1, am1);
+  double al = dmin(ap1l, am1l);
+  double ar = dmax(ap1r, am1r);
+  const long f = face_index(G, ix, iy, iz, D);
+  double *out = G.flb[D] + f;
+  const long nf = G.nface[D];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const double fo = __shfl_xor_sync(pairmask, fs[j], 1);
+    const double uo = __shfl_xor_sync(pairmask, us[EE0 + j], 1);
+    const double fL = side ? fo : fs[j], fR = side ? fs[j] : fo;
+    const double uL = side ? uo : us[EE0 + j], uR = side ? us[EE0 + j] : uo;
+    if ((j & 1) != side) continue;
+    double fl;
+    if (G.fluxmethod == 0) {
+      fl = .5 * (fR + fL - ag * (uR - uL));
+    } else {
+      if (al > 0.) fl = fL;
+      else if (ar < 0.) fl = fL;
+      else fl = (-al * fR + ar * fL + al * ar * (uR - uL)) / (ar - al);
+    }
+    out[(EE0 + j) * nf] = fl;
   }
 }
 
@@ -596,6 +725,52 @@ __global__ void __launch_bounds__(128, 4) k_update(Grid G, Box b, const double *
     G.u[iv * G.ncell + c] = val;
   }
 #undef EMFV
+}
+
+// The radiation variables of the update (the same loop of finite.c:1062-1160
+// over EE0..FZ0): flux divergence plus the radiative metric source
+// gdet R^k_l Gamma^l_{jk} (f_metric_source_term_arb, physics.c:383-405).
+__global__ void __launch_bounds__(128) k_update_rad(Grid G, Box b, const double *dtp, double fac) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+  const double dt = fac * dtp[0];
+  double pp[NVR];
+  load_rad(G.p, G.ncell, c, pp);
+  Geom g;
+  geom_centre(G, ix, iy, iz, g);
+  double Rl[4][4];
+  rad_Rmixed(pp, g, Rl);
+  double ms[4];
+  {
+    const long mi = met_index(G, ix, iy, iz);
+    const double gdetu = g.gdet;
+    double s0 = 0., s1 = 0., s2 = 0., s3 = 0.;
+    for (int kk = 0; kk < 4; kk++)
+      for (int l = 0; l < 4; l++) {
+        double gt = gdetu * Rl[kk][l];
+        const double *K = G.gkr + (long)(l * 16 + kk) * G.nmet + mi;
+        s0 += gt * __ldg(K + 0 * 4 * G.nmet);
+        s1 += gt * __ldg(K + 1 * 4 * G.nmet);
+        s2 += gt * __ldg(K + 2 * 4 * G.nmet);
+        s3 += gt * __ldg(K + 3 * 4 * G.nmet);
+      }
+    ms[0] = s0; ms[1] = s1; ms[2] = s2; ms[3] = s3;
+  }
+  const double dx = size_x(G, ix, 0), dy = size_x(G, iy, 1), dz = size_x(G, iz, 2);
+  const long fxl = face_index(G, ix, iy, iz, 0), fxr = face_index(G, ix + 1, iy, iz, 0);
+  const long fyl = face_index(G, ix, iy, iz, 1), fyr = face_index(G, ix, iy + 1, iz, 1);
+  const long fzl = face_index(G, ix, iy, iz, 2), fzr = face_index(G, ix, iy, iz + 1, 2);
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int iv = EE0 + j;
+    double flxl = G.flb[0][iv * G.nface[0] + fxl], flxr = G.flb[0][iv * G.nface[0] + fxr];
+    double flyl = G.flb[1][iv * G.nface[1] + fyl], flyr = G.flb[1][iv * G.nface[1] + fyr];
+    double flzl = G.flb[2][iv * G.nface[2] + fzl], flzr = G.flb[2][iv * G.nface[2] + fzr];
+    double du = -(flxr - flxl) * dt / dx - (flyr - flyl) * dt / dy - (flzr - flzl) * dt / dz;
+    double uold = G.u[iv * G.ncell + c];
+    G.u[iv * G.ncell + c] = uold + du + ms[j] * dt;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -806,6 +981,144 @@ __global__ void __launch_bounds__(128) k_u2p_entropy(Grid G, Box b, U2PQueues Q,
   }
 }
 
+// The radiation part of calc_primitives (u2p.c:13-133, with u2p_rad called
+// from u2p, u2p.c:432): after the MHD inversion and its floors, the M1
+// inversion of the radiation conserved variables, the radiation floors
+// (which may raise the density or the gas energy) and the conserved
+// variables of the final primitives.  Runs after the MHD passes and before
+// the neighbour fixup, whose averages read these primitives.  The U2PRAD
+// fixup the reference then requests changes no data (cell_fixup,
+// finite.c:4599-4604, stores only the first NVMHD variables, and those
+// were not averaged for this kind), so a correction is only counted.
+__global__ void __launch_bounds__(128) k_u2p_rad(Grid G, Box b) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+  double uu[NVR], pp[NVR];
+  load_rad(G.u, G.ncell, c, uu);
+  load_cell(G.p, G.ncell, c, pp);
+  load_rad(G.p, G.ncell, c, pp);
+  RadGeom rg;
+  geom_centre(G, ix, iy, iz, rg.g);
+  rg.alpha = sqrt(-1. / rg.g.GG[0][0]);
+  const RadParams &R = *G.radp;
+  int corr = 0;
+  u2p_rad(R, uu, pp, rg, corr);
+  count_lanes(&G.cnt[C_RADCOR], corr != 0);
+  const double rho0 = pp[RHO], u0 = pp[UU];
+  const int fl = check_floors_rad(R, pp, rg.g);
+  count_lanes(&G.cnt[C_RADFLOOR], fl < 0);
+  if (pp[RHO] != rho0 || pp[UU] != u0) {
+    double um[NVMAX];
+    p2u_full(G, pp, um, rg.g);
+    store_cell(G.p, G.ncell, c, pp);
+    store_cell(G.u, G.ncell, c, um);
+  }
+  p2u_rad(pp, uu, rg.g);
+  store_rad(G.p, G.ncell, c, pp);
+  store_rad(G.u, G.ncell, c, uu);
+}
+
+// ---------------------------------------------------------------------------
+// implicit radiation source step over the domain (op_implicit,
+// finite.c:1242-1292): the domain cells are gathered into the batched
+// solver's cell-major arrays, solved, and scattered back; cells where every
+// attempt failed keep their state and get the RADIMP neighbour fixup.
+// ---------------------------------------------------------------------------
+// metric of each domain cell, 20 + 20 doubles (done once per metric)
+__global__ void k_imp_pack_metric(Grid G, Box b, double *g20, double *G20) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  int ix, iy, iz;
+  if (!box_coord(b, k, ix, iy, iz)) return;
+  const long mi = met_index(G, ix, iy, iz);
+  for (int a = 0; a < 20; a++) {
+    g20[k * 20 + a] = G.met_c[(long)a * G.nmet + mi];
+    G20[k * 20 + a] = G.met_c[(long)(20 + a) * G.nmet + mi];
+  }
+}
+// conserved state after the explicit part, primitive guess and time step
+// (solve_implicit_lab, rad.c:1230-1260; implicit_lab_rad_source_term is
+// called with dt times the unit multi-step multiplier)
+__global__ void k_imp_gather(Grid G, Box b, const double *dtp, double fac, double *uu, double *pp, double *dt) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  int ix, iy, iz;
+  if (!box_coord(b, k, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+#pragma unroll
+  for (int iv = 0; iv < NVR; iv++) {
+    uu[k * NVR + iv] = G.u[iv * G.ncell + c];
+    pp[k * NVR + iv] = G.p[iv * G.ncell + c];
+  }
+  dt[k] = (dtp[0] * fac) * 1.;
+}
+__global__ void k_imp_scatter(Grid G, Box b, const double *pp, const double *uu, const int *status) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  int ix, iy, iz;
+  if (!box_coord(b, k, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+  const bool ok = status[k] == 0;
+  count_lanes(&G.cnt[C_RADIMP_FAIL], !ok);
+  count_lanes(&G.cnt[C_IMP_SOLVES], true);
+  G.flag[c] = ok ? 0 : 1;
+  if (!ok) return;
+#pragma unroll
+  for (int iv = 0; iv < NVR; iv++) {
+    G.p[iv * G.ncell + c] = pp[k * NVR + iv];
+    G.u[iv * G.ncell + c] = uu[k * NVR + iv];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// RK2IMEX combinations over the domain, all thirteen variables, each in the
+// reference's operation order (ko.c:444-570)
+// ---------------------------------------------------------------------------
+// d = (1/(dt f)) u + (-1/(dt f)) base; optionally copy = u
+__global__ void k_imex_rate(Grid G, Box b, const double *dtp, double f, const double *base, double *d, double *copy) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+  const double dtcell = dtp[0];
+  const double a = 1. / (dtcell * f), m = -1. / (dtcell * f);
+  for (int iv = 0; iv < NVR; iv++) {
+    const long i = iv * G.ncell + c;
+    const double u = G.u[i];
+    d[i] = a * u + m * base[i];
+    if (copy) copy[i] = 1. * u;
+  }
+}
+// dut1 = (1/dt) u + (-1/dt) ut1, then u = ut0 + dt dut1 + dt (1 - 2 gamma) drt1,
+// and the copy of the new u that the second implicit stage starts from
+__global__ void k_imex_stage1(Grid G, Box b, const double *dtp, double gam, const double *ut0, const double *ut1,
+                              double *dut1, const double *drt1, double *copy) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+  const double dtcell = dtp[0];
+  for (int iv = 0; iv < NVR; iv++) {
+    const long i = iv * G.ncell + c;
+    const double d = (1. / (dtcell)) * G.u[i] + (-1. / (dtcell)) * ut1[i];
+    dut1[i] = d;
+    const double un = ut0[i] + (dtcell) * d + (dtcell * (1. - 2. * gam)) * drt1[i];
+    G.u[i] = un;
+    copy[i] = 1. * un;
+  }
+}
+// dut2 = (1/dt) u + (-1/dt) ut2; u = ut0 + dt/2 dut1 + dt/2 dut2, then
+// u += dt/2 drt1 + dt/2 drt2
+__global__ void k_imex_final(Grid G, Box b, const double *dtp, const double *ut0, const double *ut2,
+                             const double *dut1, const double *drt1, const double *drt2) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+  const double dtcell = dtp[0];
+  for (int iv = 0; iv < NVR; iv++) {
+    const long i = iv * G.ncell + c;
+    const double dut2 = (1. / (dtcell)) * G.u[i] + (-1. / (dtcell)) * ut2[i];
+    const double ue = ut0[i] + (dtcell / 2.) * dut1[i] + (dtcell / 2.) * dut2;
+    G.u[i] = ue + (dtcell / 2.) * drt1[i] + (dtcell / 2.) * drt2[i];
+  }
+}
+
 // The reference visits cells in loop_0 order (x outer, z inner) and clears
 // each flag as it goes, so a neighbour that precedes the cell in that order
 // always counts as good, one that follows counts when its own inversion
@@ -930,10 +1243,20 @@ __global__ void k_fill(double *a, long n, double v) {
 // context
 // ---------------------------------------------------------------------------
 enum KernelId { K_BC = 0, K_WAVESPEEDS, K_FLUX0, K_FLUX1, K_FLUX2, K_EMF, K_UPDATE, K_U2P, K_U2P_RESUME,
-                K_U2P_ENT, K_U2P_RESUME_ENT, K_FIXUP, K_COMMIT, K_BEGIN, K_NKERNELS };
+                K_U2P_ENT, K_U2P_RESUME_ENT, K_FIXUP, K_COMMIT, K_BEGIN, K_FLUXRAD0, K_FLUXRAD1, K_FLUXRAD2,
+                K_UPDATE_RAD, K_U2P_RAD, K_IMP_GATHER, K_IMP_WARM, K_IMP_SOLVE, K_IMP_SCATTER, K_IMEX, K_NKERNELS };
 static const char *kKernelNames[K_NKERNELS] = {"k_bc", "k_wavespeeds", "k_flux_x", "k_flux_y", "k_flux_z", "k_emf",
                                                "k_update", "k_u2p", "k_u2p_resume", "k_u2p_entropy",
-                                               "k_u2p_resume_entropy", "k_fixup", "k_commit", "k_begin_step"};
+                                               "k_u2p_resume_entropy", "k_fixup", "k_commit", "k_begin_step",
+                                               "k_flux_rad_x", "k_flux_rad_y", "k_flux_rad_z", "k_update_rad",
+                                               "k_u2p_rad", "k_imp_gather", "k_imp_warm_start", "k_imp_solve",
+                                               "k_imp_scatter", "k_imex"};
+
+int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
+                           const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
+                           int *status, int *attempt, int *iters, int mode, void *work, void *stream,
+                           unsigned long long *acc, long long *launches);
+kgpu::RadParams kgpu_rad_device_params(const kgpu_rad_params &p);
 
 struct ProfRec {
   int id;
@@ -964,6 +1287,19 @@ struct kgpu_ctx {
   cudaGraph_t graph;
   cudaGraphExec_t graph_exec;
   bool graph_ready;
+  int graph_kind = 0;            // 0: RK2 step, 1: RK2IMEX step
+  // radiation (nv == 13)
+  kgpu_rad_params rp;
+  double *drt1 = nullptr, *dut1 = nullptr, *drt2 = nullptr, *dut2 = nullptr;   // RK2IMEX rates
+  long nimp = 0;                 // domain cells of the implicit solve
+  double *imp_uu = nullptr, *imp_pp = nullptr, *imp_g = nullptr, *imp_G = nullptr, *imp_dt = nullptr;
+  double *imp_ppo = nullptr, *imp_uuo = nullptr;
+  int *imp_status = nullptr, *imp_att = nullptr, *imp_it = nullptr;
+  void *imp_work = nullptr;
+  float *imp_X = nullptr, *imp_Y = nullptr;
+  int imp_mode = KGPU_RAD_BATCHED;
+  kgpu_mlp *warm = nullptr;      // warm-start network, or none
+  long long metric_gen = 0, packed_gen = -1;
 };
 
 static cudaEvent_t pool_event(kgpu_ctx *c) {
@@ -1054,7 +1390,7 @@ static void fill_grid_params(Grid &G, const kgpu_config &c) {
 
 static int check_config(const kgpu_config *c) {
   if (!c || c->nx < 1 || c->ny < 1 || c->nz < 1) return KGPU_EINVAL;
-  if (c->nv != 9) return KGPU_EINVAL;               // MHD with magnetic field
+  if (c->nv != 9 && c->nv != 13) return KGPU_EINVAL;   // MHD with magnetic field, optionally M1 radiation
   if (c->int_order != KGPU_PPM && c->int_order != KGPU_MP5) return KGPU_EINVAL;
   if (c->int_order == KGPU_PPM && c->ng < 3) return KGPU_EINVAL;
   if (c->int_order == KGPU_MP5 && c->ng < 4) return KGPU_EINVAL;
@@ -1130,6 +1466,13 @@ extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
   AL(c->u2pq.it, G.ncell * sizeof(int));
   AL(G.scal, S_NSCAL * d8);
   AL(G.cnt, C_NCNT * sizeof(unsigned long long));
+  if (G.nv == NVR) {
+    for (int d = 0; d < 3; d++) {
+      AL(G.arl[d], G.ncell * d8);
+      AL(G.arr[d], G.ncell * d8);
+    }
+    AL(c->drt1, ncv * d8); AL(c->dut1, ncv * d8); AL(c->drt2, ncv * d8); AL(c->dut2, ncv * d8);
+  }
 #undef AL
   CK(cudaMemsetAsync(G.u, 0, ncv * d8, c->stream));
   CK(cudaMemsetAsync(G.p, 0, ncv * d8, c->stream));
@@ -1147,6 +1490,11 @@ extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
   CK(cudaMemsetAsync(G.scal, 0, S_NSCAL * d8, c->stream));
   CK(cudaMemsetAsync(G.cnt, 0, C_NCNT * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync((void *)G.gkr, 0, G.nmet * 64 * d8, c->stream));
+  if (G.nv == NVR)
+    for (int d = 0; d < 3; d++) {
+      CK(cudaMemsetAsync(G.arl[d], 0, G.ncell * d8, c->stream));
+      CK(cudaMemsetAsync(G.arr[d], 0, G.ncell * d8, c->stream));
+    }
   CK(cudaStreamSynchronize(c->stream));
   *out = c;
   return 0;
@@ -1252,6 +1600,7 @@ extern "C" int kgpu_upload_metric(kgpu_ctx *c, const double *g, const double *Gi
   CK(cudaMemcpyAsync((void *)G.gkr, h.data(), G.nmet * 64 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->have_metric = true;
+  c->metric_gen++;
   return 0;
 }
 
@@ -1289,6 +1638,7 @@ extern "C" int kgpu_set_minkowski_metric(kgpu_ctx *c) {
   CKL("k_minkowski");
   CK(cudaStreamSynchronize(c->stream));
   c->have_metric = true;
+  c->metric_gen++;
   return 0;
 }
 
@@ -1381,21 +1731,33 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
   int ex0 = -1, enx = G.nx + 2;
   if (G.nx > 1) {
     Box b{0, ey0, ez0, G.nx + 1, eny, enz};
-    LaunchScope ls(c, K_FLUX0);
-    k_flux<0><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);
+    { LaunchScope ls(c, K_FLUX0); k_flux<0><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b); }
     CKL("k_flux<0>");
+    if (G.rad) {
+      LaunchScope ls(c, K_FLUXRAD0);
+      k_flux_rad<0><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);
+      CKL("k_flux_rad<0>");
+    }
   }
   if (G.ny > 1) {
     Box b{ex0, 0, ez0, enx, G.ny + 1, enz};
-    LaunchScope ls(c, K_FLUX1);
-    k_flux<1><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);
+    { LaunchScope ls(c, K_FLUX1); k_flux<1><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b); }
     CKL("k_flux<1>");
+    if (G.rad) {
+      LaunchScope ls(c, K_FLUXRAD1);
+      k_flux_rad<1><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);
+      CKL("k_flux_rad<1>");
+    }
   }
   if (G.nz > 1) {
     Box b{ex0, ey0, 0, enx, eny, G.nz + 1};
-    LaunchScope ls(c, K_FLUX2);
-    k_flux<2><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);
+    { LaunchScope ls(c, K_FLUX2); k_flux<2><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b); }
     CKL("k_flux<2>");
+    if (G.rad) {
+      LaunchScope ls(c, K_FLUXRAD2);
+      k_flux_rad<2><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);
+      CKL("k_flux_rad<2>");
+    }
   }
   Box eb{0, 0, 0, G.nx + 1, G.ny + 1, G.nz + 1};
   { LaunchScope ls(c, K_EMF); k_emf<<<nblocks(eb.n(), 128), 128, 0, c->stream>>>(G, eb); }
@@ -1403,6 +1765,10 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
   Box db = domain_box(G);
   { LaunchScope ls(c, K_UPDATE); k_update<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, dtp, fac, save); }
   CKL("k_update");
+  if (G.rad) {
+    { LaunchScope ls(c, K_UPDATE_RAD); k_update_rad<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, dtp, fac); }
+    CKL("k_update_rad");
+  }
   return 0;
 }
 
@@ -1418,6 +1784,10 @@ static int launch_u2p(kgpu_ctx *c, int combine) {
   CKL("k_u2p_entropy");
   { LaunchScope ls(c, K_U2P_RESUME_ENT); k_u2p_resume<<<sweep, 128, 0, c->stream>>>(G, db, c->u2pq, 1); }
   CKL("k_u2p_resume_entropy");
+  if (G.rad) {
+    { LaunchScope ls(c, K_U2P_RAD); k_u2p_rad<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db); }
+    CKL("k_u2p_rad");
+  }
   { LaunchScope ls(c, K_FIXUP); k_fixup<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, c->fixmark); }
   CKL("k_fixup");
   { LaunchScope ls(c, K_COMMIT); k_commit<<<nblocks(db.n(), 256), 256, 0, c->stream>>>(G, db, c->fixmark, combine, c->u2pq.n); }
@@ -1449,9 +1819,12 @@ extern "C" int kgpu_op_explicit(kgpu_ctx *c, double t, double dt) {
   return 0;
 }
 
+int kgpu_op_implicit_impl(kgpu_ctx *c, double dt);
 extern "C" int kgpu_op_implicit(kgpu_ctx *c, double t, double dt) {
-  (void)t; (void)dt;
-  return c ? 0 : KGPU_EINVAL;
+  (void)t;
+  if (!c) return KGPU_EINVAL;
+  if (!c->G.rad) return 0;   // no radiation: nothing to do, as in the reference
+  return kgpu_op_implicit_impl(c, dt);
 }
 
 extern "C" int kgpu_calc_u2p(kgpu_ctx *c) {
@@ -1544,16 +1917,16 @@ extern "C" int kgpu_rk2_steps(kgpu_ctx *c, int nsteps) {
   return 0;
 }
 
-extern "C" int kgpu_rk2_steps_graph(kgpu_ctx *c, int nsteps) {
-  int r = ready(c);
-  if (r) return r;
-  if (nsteps < 1) return KGPU_EINVAL;
+// Captures one step of the given kind into a CUDA graph (kept until the
+// kernel arguments change) and replays it nsteps times.
+static int run_graph(kgpu_ctx *c, int nsteps, int kind, int (*enqueue)(kgpu_ctx *)) {
+  if (c->graph_ready && c->graph_kind != kind) drop_graph(c);
   if (!c->graph_ready) {
     bool prof = c->profiling;
     c->profiling = false;
     long long before = c->launches;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    r = enqueue_rk2(c);
+    int r = enqueue(c);
     c->graph_launches = c->launches - before;
     c->launches = before;
     c->profiling = prof;
@@ -1564,11 +1937,190 @@ extern "C" int kgpu_rk2_steps_graph(kgpu_ctx *c, int nsteps) {
     CK(cudaGraphInstantiate(&c->graph_exec, gph, 0));
     c->graph = gph;
     c->graph_ready = true;
+    c->graph_kind = kind;
   }
   for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(c->graph_exec, c->stream));
   c->launches += c->graph_launches * nsteps;
   CK(cudaStreamSynchronize(c->stream));
   return 0;
+}
+
+extern "C" int kgpu_rk2_steps_graph(kgpu_ctx *c, int nsteps) {
+  int r = ready(c);
+  if (r) return r;
+  if (nsteps < 1) return KGPU_EINVAL;
+  return run_graph(c, nsteps, 0, enqueue_rk2);
+}
+
+// ---------------------------------------------------------------------------
+// radiation: the implicit source operator and the RK2IMEX step
+// ---------------------------------------------------------------------------
+extern "C" int kgpu_set_radiation(kgpu_ctx *c, const kgpu_rad_params *rp, int wavespeed_limiter) {
+  if (!c || !rp) return KGPU_EINVAL;
+  Grid &G = c->G;
+  if (G.nv != NVR) return KGPU_EINVAL;
+  if (!(rp->gamma == G.gamma)) return KGPU_EINVAL;   // one adiabatic index for the grid and the solver
+  int r;
+  void *p;
+  if (!G.radp) {
+    if ((r = dalloc(c, &p, sizeof(RadParams)))) return r;
+    G.radp = (const RadParams *)p;
+  }
+  c->rp = *rp;
+  RadParams R = kgpu_rad_device_params(*rp);
+  CK(cudaMemcpyAsync((void *)G.radp, &R, sizeof(R), cudaMemcpyHostToDevice, c->stream));
+  if (!c->imp_uu) {
+    const long n = (long)G.nx * G.ny * G.nz;
+    if (n > 0x7fffffffL) return KGPU_EINVAL;
+    c->nimp = n;
+    const size_t d8 = sizeof(double);
+#define AL(ptr, bytes)                                  \
+  do {                                                  \
+    if ((r = dalloc(c, &p, (bytes))) != 0) return r;    \
+    ptr = (decltype(ptr))p;                             \
+  } while (0)
+    AL(c->imp_uu, n * NVR * d8); AL(c->imp_pp, n * NVR * d8);
+    AL(c->imp_ppo, n * NVR * d8); AL(c->imp_uuo, n * NVR * d8);
+    AL(c->imp_g, n * 20 * d8); AL(c->imp_G, n * 20 * d8); AL(c->imp_dt, n * d8);
+    AL(c->imp_status, n * sizeof(int)); AL(c->imp_att, n * sizeof(int)); AL(c->imp_it, n * sizeof(int));
+    AL(c->imp_work, kgpu_rad_work_bytes((int)n));
+#undef AL
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  G.rad = 1;
+  G.rad_limiter = wavespeed_limiter ? 1 : 0;
+  c->packed_gen = -1;
+  drop_graph(c);
+  return 0;
+}
+
+extern "C" int kgpu_set_implicit_solver(kgpu_ctx *c, int mode, kgpu_mlp *warm) {
+  if (!c || (mode != KGPU_RAD_PLAIN && mode != KGPU_RAD_BATCHED)) return KGPU_EINVAL;
+  if (warm && mode != KGPU_RAD_BATCHED) return KGPU_EINVAL;   // the warm start runs in the batched solver
+  if (!c->G.rad) return KGPU_ESTATE;
+  if (warm && !c->imp_X) {
+    void *p;
+    int r;
+    if ((r = dalloc(c, &p, c->nimp * 16 * sizeof(float)))) return r;
+    c->imp_X = (float *)p;
+    if ((r = dalloc(c, &p, c->nimp * 8 * sizeof(float)))) return r;
+    c->imp_Y = (float *)p;
+  }
+  c->imp_mode = mode;
+  c->warm = warm;
+  drop_graph(c);
+  return 0;
+}
+
+// the per-cell metric of the domain for the solver, once per metric
+static int ensure_packed(kgpu_ctx *c) {
+  if (c->packed_gen == c->metric_gen) return 0;
+  Box db = domain_box(c->G);
+  k_imp_pack_metric<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(c->G, db, c->imp_g, c->imp_G);
+  CKL("k_imp_pack_metric");
+  CK(cudaStreamSynchronize(c->stream));
+  c->packed_gen = c->metric_gen;
+  return 0;
+}
+
+// op_implicit with time step fac * dtp[0]: solve, scatter, RADIMP fixup
+static int enqueue_implicit(kgpu_ctx *c, const double *dtp, double fac) {
+  Grid &G = c->G;
+  Box db = domain_box(G);
+  const int n = (int)c->nimp;
+  { LaunchScope ls(c, K_IMP_GATHER);
+    k_imp_gather<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, dtp, fac, c->imp_uu, c->imp_pp, c->imp_dt); }
+  CKL("k_imp_gather");
+  const float *ypred = nullptr;
+  if (c->warm) {
+    LaunchScope ls(c, K_IMP_WARM);
+    int r = kgpu_rad_features_device(n, &c->rp, c->imp_pp, c->imp_g, c->imp_G, c->imp_dt, c->imp_X, c->stream);
+    if (!r) r = kgpu_mlp_forward(c->warm, c->imp_X, n, c->imp_Y, c->stream);
+    if (r) return r;
+    c->launches += 1;   // two kernels under one scope
+    ypred = c->imp_Y;
+  }
+  {
+    LaunchScope ls(c, K_IMP_SOLVE);
+    long long nl = 0;
+    int r = kgpu_rad_solve_enqueue(n, &c->rp, c->imp_uu, c->imp_pp, c->imp_g, c->imp_G, c->imp_dt, ypred, c->imp_ppo,
+                                   c->imp_uuo, c->imp_status, c->imp_att, c->imp_it, c->imp_mode, c->imp_work,
+                                   c->stream, G.cnt + C_IMP_ITERS, &nl);
+    if (r) return r;
+    c->launches += nl - 1;
+  }
+  { LaunchScope ls(c, K_IMP_SCATTER);
+    k_imp_scatter<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, c->imp_ppo, c->imp_uuo, c->imp_status); }
+  CKL("k_imp_scatter");
+  { LaunchScope ls(c, K_FIXUP); k_fixup<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, c->fixmark); }
+  CKL("k_fixup");
+  { LaunchScope ls(c, K_COMMIT); k_commit<<<nblocks(db.n(), 256), 256, 0, c->stream>>>(G, db, c->fixmark, 0, c->u2pq.n); }
+  CKL("k_commit");
+  return 0;
+}
+
+// one RK2IMEX step (ko.c:444-570) with dt in device memory
+static int enqueue_rk2imex(kgpu_ctx *c) {
+  Grid &G = c->G;
+  const double gam = 1. - 1. / sqrt(2.);
+  const double *dtp = G.scal + S_DT;
+  Box db = domain_box(G);
+  const unsigned nb = nblocks(db.n(), 128);
+  int r;
+  { LaunchScope ls(c, K_BEGIN); k_begin_step<<<1, 1, 0, c->stream>>>(G); }
+  CKL("k_begin_step");
+  CK(cudaMemcpyAsync(G.ut0, G.u, G.ncell * G.nv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  if ((r = enqueue_implicit(c, dtp, gam))) return r;                       // U(1) = implicit from U(n)
+  { LaunchScope ls(c, K_IMEX); k_imex_rate<<<nb, 128, 0, c->stream>>>(G, db, dtp, gam, G.ut0, c->drt1, G.ut1); }
+  CKL("k_imex_rate");                                                       // R(U(1)); ut1 = U(1)
+  if ((r = launch_u2p(c, 0))) return r;
+  if ((r = launch_explicit(c, dtp, 1.0, nullptr))) return r;
+  { LaunchScope ls(c, K_IMEX);
+    k_imex_stage1<<<nb, 128, 0, c->stream>>>(G, db, dtp, gam, G.ut0, G.ut1, c->dut1, c->drt1, G.ut1); }
+  CKL("k_imex_stage1");                                                     // F(U(1)); u; uforget = u
+  if ((r = launch_u2p(c, 0))) return r;
+  if ((r = enqueue_implicit(c, dtp, gam))) return r;                       // U(2)
+  { LaunchScope ls(c, K_IMEX); k_imex_rate<<<nb, 128, 0, c->stream>>>(G, db, dtp, gam, G.ut1, c->drt2, G.ut1); }
+  CKL("k_imex_rate");                                                       // R(U(2)); ut2 = U(2)
+  if ((r = launch_u2p(c, 0))) return r;
+  if ((r = launch_explicit(c, dtp, 1.0, nullptr))) return r;
+  { LaunchScope ls(c, K_IMEX);
+    k_imex_final<<<nb, 128, 0, c->stream>>>(G, db, dtp, G.ut0, G.ut1, c->dut1, c->drt1, c->drt2); }
+  CKL("k_imex_final");
+  return launch_u2p(c, 0);
+}
+
+static int ready_rad(kgpu_ctx *c) {
+  int r = ready(c);
+  if (r) return r;
+  if (!c->G.rad) return KGPU_ESTATE;
+  return ensure_packed(c);
+}
+
+extern "C" int kgpu_rk2imex_steps(kgpu_ctx *c, int nsteps) {
+  int r = ready_rad(c);
+  if (r) return r;
+  if (nsteps < 1) return KGPU_EINVAL;
+  for (int s = 0; s < nsteps; s++)
+    if ((r = enqueue_rk2imex(c))) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int kgpu_op_implicit_impl(kgpu_ctx *c, double dt) {
+  int r = ready_rad(c);
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->G.scal + S_T, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if ((r = enqueue_implicit(c, c->G.scal + S_T, 1.0))) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_rk2imex_steps_graph(kgpu_ctx *c, int nsteps) {
+  int r = ready_rad(c);
+  if (r) return r;
+  if (nsteps < 1) return KGPU_EINVAL;
+  return run_graph(c, nsteps, 1, enqueue_rk2imex);
 }
 
 extern "C" int kgpu_get_counters(kgpu_ctx *c, unsigned long long out[4]) {
@@ -1842,6 +2394,46 @@ extern "C" int kgpu_init_fm_torus(kgpu_ctx *c, const kgpu_torus_params *tp) {
   std::vector<double> u(G.ncell * G.nv), p(G.ncell * G.nv);
   if ((r = kgpu_fm_torus_state(tp, &k, c->hxb[0].data(), c->hxb[1].data(), c->hxb[2].data(), g.data(), Gi.data(),
                                u.data(), p.data())))
+    return r;
+  if ((r = kgpu_upload_state(c, u.data(), p.data()))) return r;
+  if ((r = launch_bc(c))) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return kgpu_begin_run(c);
+}
+
+// The radiative torus: the same set-up with the torus pressure shared by gas
+// and radiation in thermal equilibrium, a faint radiation field at rest in
+// the atmosphere (eradatm times its gas energy), radiation switched on.
+extern "C" int kgpu_init_fm_radtorus(kgpu_ctx *c, const kgpu_torus_params *tp, const kgpu_rad_params *rp,
+                                     double eradatm, int wavespeed_limiter) {
+  if (!c || !tp || !rp) return KGPU_EINVAL;
+  const kgpu_config &k = c->cfg;
+  if (k.nz < 2 || k.ny < 2 || k.nv != NVR) return KGPU_EINVAL;
+  int r;
+  double lo[3] = {log(tp->r_lo - tp->r0), tp->x2_lo, 0.}, hi[3] = {log(tp->r_hi - tp->r0), tp->x2_hi, 2. * M_PI};
+  if ((r = kgpu_set_uniform_grid(c, lo, hi))) return r;
+  Grid &G = c->G;
+  std::vector<double> g(G.nmet * 20), Gi(G.nmet * 20), kr(G.nmet * 64);
+  std::vector<double> gb[3], Gb[3];
+  for (int d = 0; d < 3; d++) {
+    gb[d].resize(G.nfmet[d] * 20);
+    Gb[d].resize(G.nfmet[d] * 20);
+  }
+  if ((r = kgpu_mks2_metric_tables(tp->spin, tp->r0, tp->h0, k.nx, k.ny, k.nz, k.ng, k.axisym_metric,
+                                   c->hxb[0].data(), c->hxb[1].data(), c->hxb[2].data(), g.data(), Gi.data(),
+                                   kr.data(), gb[0].data(), gb[1].data(), gb[2].data(), Gb[0].data(), Gb[1].data(),
+                                   Gb[2].data())))
+    return r;
+  if ((r = kgpu_upload_metric(c, g.data(), Gi.data(), kr.data(), gb[0].data(), gb[1].data(), gb[2].data(),
+                              Gb[0].data(), Gb[1].data(), Gb[2].data())))
+    return r;
+  std::vector<double> fc(G.sx), ff(G.sx + 1);
+  if ((r = kgpu_fm_torus_floor(tp, k.nx, k.ng, c->hxb[0].data(), fc.data(), ff.data()))) return r;
+  if ((r = kgpu_set_density_floor(c, fc.data(), ff.data()))) return r;
+  if ((r = kgpu_set_radiation(c, rp, wavespeed_limiter))) return r;
+  std::vector<double> u(G.ncell * G.nv), p(G.ncell * G.nv);
+  if ((r = kgpu_fm_radtorus_state(tp, rp, eradatm, &k, c->hxb[0].data(), c->hxb[1].data(), c->hxb[2].data(), g.data(),
+                                  Gi.data(), u.data(), p.data())))
     return r;
   if ((r = kgpu_upload_state(c, u.data(), p.data()))) return r;
   if ((r = launch_bc(c))) return r;

@@ -20,6 +20,8 @@ constexpr bool kMagn = NVMAX > 8;  // the magnetic field is always carried
 constexpr int RHO = 0, UU = 1, VX = 2, VY = 3, VZ = 4, ENTR = 5, B1 = 6, B2 = 7, B3 = 8;
 constexpr double SMALL = 1.e-50, BIG = 1. / SMALL;
 
+struct RadParams;   // radiation constants (kgpu_rad.cuh)
+
 // Run-time description of one grid, passed by value to every kernel.
 struct Grid {
   int nx, ny, nz, ng, nv;
@@ -48,6 +50,11 @@ struct Grid {
   int bc[3];                         // boundary kind per axis (KGPU_BC_*)
   double *scal;                      // device scalars (see ScalarSlot)
   unsigned long long *cnt;           // device counters
+  // radiation (nv == 13): variables EE0..FZ0 follow the nine MHD ones
+  int rad;                           // radiation carried
+  int rad_limiter;                   // optical-depth limiter of the radiative wave speeds
+  const RadParams *radp;             // device copy of the radiation constants
+  double *arl[3], *arr[3];           // radiative wave speeds per cell and direction
 };
 
 enum ScalarSlot { S_TSTEPDENMAX = 0, S_TSTEPDENMIN = 1, S_DT = 2, S_T = 3, S_NSCAL = 8 };
@@ -57,7 +64,15 @@ enum CounterSlot {
   C_ITERS_ENT = 5,   // Newton steps of entropy-equation solves
   C_SLOW = 6,        // energy solves paused after the first pass and resumed
   C_ENTQ = 7,        // cells handed to the entropy equation
-  C_NCNT = 8
+  C_RADCOR = 8,      // M1 inversions that needed a correction (U2PRAD fixup requests)
+  C_RADIMP_FAIL = 9, // implicit source solves where every attempt failed
+  C_IMP_ITERS = 10,  // Newton iterations of the implicit solves, all attempts
+  C_IMP_PASSES = 11, // passes of the batched solver that had work
+  C_IMP_FALLBACK = 12,  // warm-started solves that fell back to the reference cascade
+                        // (10..12 are the solver's own statistics, in its order)
+  C_IMP_SOLVES = 13, // implicit source solves
+  C_RADFLOOR = 14,   // cells whose radiation floors acted
+  C_NCNT = 16
 };
 
 // ---------------------------------------------------------------------------

@@ -46,6 +46,8 @@ RadParams to_dev(const kgpu_rad_params &p) {
   R.dampfac = p.dampfac; R.maxdown = p.maxdown; R.maxup = p.maxup;
   R.maxdamping = p.maxdamping; R.threshold = p.threshold;
   R.u2pconv = p.u2pconv;
+  R.eerhoratiomin = p.eerhoratiomin; R.eerhoratiomax = p.eerhoratiomax;
+  R.eeuuratiomin = p.eeuuratiomin; R.eeuuratiomax = p.eeuuratiomax;
   return R;
 }
 
@@ -340,6 +342,10 @@ extern "C" int kgpu_rad_default_params(kgpu_rad_params *rp, double mass, double 
   rp->maxdamping = 1.e-5;
   rp->threshold = 1.e-2;
   rp->u2pconv = 1.e-10;
+  rp->eerhoratiomin = 1.e-30;
+  rp->eerhoratiomax = 1.e30;
+  rp->eeuuratiomin = 1.e-30;
+  rp->eeuuratiomax = 1.e30;
   return 0;
 }
 
@@ -354,10 +360,14 @@ extern "C" size_t kgpu_rad_work_bytes(int n) {
   return work_layout(n, kMaxPasses, nullptr, nullptr) + 256;
 }
 
+// acc (device, optional): counters the solve adds to instead of reporting
+// through stats: [0] Newton iterations, [1] passes with work, [2] warm-start
+// fallbacks.  Launches only (no allocation, no synchronisation) when stats
+// is null, so that a time step can be captured in a CUDA graph.
 static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
                             const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
                             int *status, int *attempt, int *iters, int mode, void *work, void *stream,
-                            unsigned long long *stats, int nstats) {
+                            unsigned long long *stats, int nstats, unsigned long long *acc = nullptr) {
   if (n < 0 || !rp || (mode != KGPU_RAD_PLAIN && mode != KGPU_RAD_BATCHED)) return KGPU_EINVAL;
   if (n > 0 && (!uu || !pp || !g || !G || !dt || !pp_out || !uu_out || !status || !attempt || !iters))
     return KGPU_EINVAL;
@@ -369,7 +379,7 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
   RadParams R = to_dev(*rp);
   Cell C{uu, pp, g, G, dt, pp_out, uu_out, status, attempt, iters};
   if (mode == KGPU_RAD_PLAIN) {
-    unsigned long long *dstats = nullptr;
+    unsigned long long *dstats = acc;
     DevMem sm;
     if (stats) {
       RCK(cudaMalloc(&sm.p, sizeof(unsigned long long)));
@@ -391,7 +401,8 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
   Work W;
   work_layout(n, passes, &W, base);   // fits: the area is sized for kMaxPasses >= passes
   RCK(cudaMemsetAsync(W.count, 0, (size_t)(passes + 2) * 2 * 4, st));
-  RCK(cudaMemsetAsync(W.stats, 0, 4 * sizeof(unsigned long long), st));
+  if (acc) W.stats = acc;
+  else RCK(cudaMemsetAsync(W.stats, 0, 4 * sizeof(unsigned long long), st));
   const int grid = sm_count() * 8;
   k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n, ypred);
   RCK(cudaGetLastError());
@@ -407,6 +418,23 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
   }
   return 0;
 }
+
+// The grid step's entry to the solver (kgpu.cu): launches only, counters
+// added to acc; the number of kernels launched is returned in *launches.
+int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
+                           const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
+                           int *status, int *attempt, int *iters, int mode, void *work, void *stream,
+                           unsigned long long *acc, long long *launches) {
+  if (launches) {
+    RadParams R = to_dev(*rp);
+    *launches = mode == KGPU_RAD_PLAIN ? 1 : 1 + max_passes(R, g_pass_iters);
+  }
+  return rad_solve_device(n, rp, uu, pp, g, G, dt, ypred, pp_out, uu_out, status, attempt, iters, mode, work, stream,
+                          nullptr, 0, acc);
+}
+
+// Device form of the radiation constants, for the grid step.
+kgpu::RadParams kgpu_rad_device_params(const kgpu_rad_params &p) { return to_dev(p); }
 
 extern "C" int kgpu_rad_implicit_cells_device(int n, const kgpu_rad_params *rp, const double *uu, const double *pp,
                                               const double *g, const double *G, const double *dt, double *pp_out,

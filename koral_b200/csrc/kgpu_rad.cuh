@@ -38,6 +38,7 @@ struct RadParams {
   double eps, conv, entrconv, maxiter;
   double dampfac, maxdown, maxup, maxdamping, threshold;
   double u2pconv;
+  double eerhoratiomin, eerhoratiomax, eeuuratiomin, eeuuratiomax;
 };
 
 struct RadGeom {
@@ -711,6 +712,126 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
   if (P.prim == IMP_MHD && corr > 0) u2pret = -2;
   if (u2pret < -1) return imp_next_attempt(pp00, warm_guess, s);
   return IMP_DONE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// M1 radiation inside the grid step: characteristic speeds, face fluxes,
+// floors
+// ---------------------------------------------------------------------------
+
+// Lab-frame speeds of the radiative characteristics per direction
+// (calc_rad_wavespeeds, rad.c:2451-2557, analytic branch): the rest-frame
+// speed 1/sqrt(3), limited by the optical depth tautot of the cell when
+// `limiter` is set, boosted with the HARM quadratic; co-going speeds zeroed
+// as calc_wavespeeds_lr_pure does (physics.c:209-226).
+KG_HD void rad_wavespeeds(const double *pp, const Geom &g, const double tautot[3], bool limiter, double al[3],
+                          double ar[3]) {
+  double urf[4];
+  rad_urf4(pp, g, urf);
+  const double rv2rad = 1. / 3.;
+  for (int dim = 0; dim < 3; dim++) {
+    double rv2 = rv2rad;
+    if (limiter && tautot[dim] > 0.) {
+      double rv2tau = 4. / 3. / tautot[dim] * 4. / 3. / tautot[dim];
+      rv2 = dmin(rv2rad, rv2tau);
+    }
+    double Acov[4] = {0., 0., 0., 0.}, Acon[4], Bcov[4] = {1., 0., 0., 0.}, Bcon[4];
+    Acov[dim + 1] = 1.;
+    raise(Acov, Acon, g.GG);
+    raise(Bcov, Bcon, g.GG);
+    double Asq = dot4(Acon, Acov);
+    double Bsq = dot4(Bcon, Bcov);
+    double Au = dot4(Acov, urf);
+    double Bu = dot4(Bcov, urf);
+    double AB = dot4(Acon, Bcov);
+    double Au2 = Au * Au, Bu2 = Bu * Bu, AuBu = Au * Bu;
+    double wspeed2 = rv2;
+    double B = 2. * (AuBu * (1.0 - wspeed2) - AB * wspeed2);
+    double A = Bu2 * (1.0 - wspeed2) - Bsq * wspeed2;
+    double discr = 4.0 * wspeed2 *
+                   ((AB * AB - Asq * Bsq) * wspeed2 + (2.0 * AB * Au * Bu - Asq * Bu2 - Bsq * Au2) * (wspeed2 - 1.0));
+    if (discr < 0.) discr = 0.;
+    discr = sqrt(discr);
+    double cst1 = -(-B + discr) / (2. * A);
+    double cst2 = -(-B - discr) / (2. * A);
+    double l = dmin(cst1, cst2), r = dmax(cst1, cst2);
+    al[dim] = l > 0. ? 0. : l;
+    ar[dim] = r < 0. ? 0. : r;
+  }
+}
+
+// Total opacity times the cell's proper size per direction (calc_tautot,
+// rad.c:55-65, with the sizes of calc_wavespeeds_lr_pure, physics.c:180-184:
+// the larger of this cell's and the next cell's).
+KG_HD void rad_tautot(const RadParams &R, const double *pp, const Geom &g, const double size_lo[3],
+                      const double size_hi[3], double tautot[3]) {
+  double chi = rad_kappa_abs(R, pp) + rad_kappa_es(R, pp);
+  for (int d = 0; d < 3; d++) {
+    double sq = sqrt(g.gg[d + 1][d + 1]);
+    tautot[d] = chi * dmax(size_lo[d] * sq, size_hi[d] * sq);
+  }
+}
+
+// gdet R^{idim+1}_j, j = 0..3: the radiative fluxes through a face
+// (f_flux_prime_rad, rad.c:3280-3330, with f_flux_prime_rad_total
+// 3125-3160 and indices_2221 frames.c:1966-1993 restricted to one row)
+KG_HD void rad_flux(const double *pp, int idim, const Geom &g, double ff[4]) {
+  double urf[4];
+  rad_urf4(pp, g, urf);
+  const double Erf = pp[EE0];
+  const int i = idim + 1;
+  double Ri[4];
+  for (int k = 0; k < 4; k++) Ri[k] = 4. / 3. * Erf * urf[i] * urf[k] + 1. / 3. * Erf * g.GG[i][k];
+  for (int j = 0; j < 4; j++) {
+    double s = 0.;
+    for (int k = 0; k < 4; k++) s += Ri[k] * g.gg[k][j];
+    ff[j] = g.gdet * s;
+  }
+}
+
+// R^k_l of the cell (calc_Rij then indices_2221), for the metric source
+KG_HD void rad_Rmixed(const double *pp, const Geom &g, double Rl[4][4]) {
+  double Rij[4][4];
+  calc_Rij_M1(pp, g, Rij);
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      double s = 0.;
+      for (int k = 0; k < 4; k++) s += Rij[i][k] * g.gg[k][j];
+      Rl[i][j] = s;
+    }
+}
+
+// check_floors_rad (u2prad.c:687-790; the magnetic-pressure branch is not
+// compiled in a build with the magnetic field evolved): the radiation
+// energy floor, then the fluid-frame radiation energy against density and
+// gas energy.  Returns -1 when a floor acted.
+KG_HD int check_floors_rad(const RadParams &R, double *pp, const Geom &g) {
+  int ret = 0;
+  double Rtt, ugas[4];
+  calc_ff_Rtt(pp, g, Rtt, ugas);
+  const double Ehat = -Rtt;
+  const double Eratio = pp[EE0] / Ehat;
+  if (pp[EE0] < R.eradfloor) {
+    pp[EE0] = R.eradfloor;
+    ret = -1;
+  }
+  if (Ehat < R.eerhoratiomin * pp[0]) {
+    pp[EE0] = Eratio * R.eerhoratiomin * pp[0];
+    ret = -1;
+  }
+  if (Ehat > R.eerhoratiomax * pp[0]) {
+    pp[0] = 1. / R.eerhoratiomax * Ehat;
+    ret = -1;
+  }
+  if (Ehat < R.eeuuratiomin * pp[1]) {
+    pp[EE0] = Eratio * R.eeuuratiomin * pp[1];
+    ret = -1;
+  }
+  if (Ehat > R.eeuuratiomax * pp[1]) {
+    pp[1] = 1. / R.eeuuratiomax * Ehat;
+    ret = -1;
+  }
+  return ret;
 }
 
 }  // namespace kgpu

@@ -213,7 +213,7 @@ extern "C" int kgpu_mks2_metric_tables(double a, double R0, double H0, int nx, i
 // (Boyer-Lindquist, M = 1).  Same construction as the KORAL plug-in used by
 // the oracle (oracle/ref/problems/FMTORUS).
 // ---------------------------------------------------------------------------
-#include "kgpu_physics.cuh"
+#include "kgpu_rad.cuh"
 
 namespace {
 
@@ -256,13 +256,17 @@ double fm_noise(unsigned long long seed, unsigned long long idx) {
 // magnetised torus.  g and G are the centre tables of kgpu_mks2_metric_tables
 // for the same grid.  Ghost cells are left zero: the caller applies the
 // boundary conditions (kgpu_set_bc) after uploading.
-extern "C" int kgpu_fm_torus_state(const kgpu_torus_params *tp, const kgpu_config *cfg, const double *xbx,
-                                   const double *xby, const double *xbz, const double *g, const double *G, double *u,
-                                   double *p) {
+// The torus state; with rp (nv = 13) the torus pressure is shared by gas
+// and radiation in thermal equilibrium and the atmosphere gets radiation of
+// eradatm times its gas energy, at rest with it (as the radiative build of
+// the torus plug-in sets it up).
+static int fm_torus_state(const kgpu_torus_params *tp, const kgpu_config *cfg, const kgpu_rad_params *rp,
+                          double eradatm, const double *xbx, const double *xby, const double *xbz, const double *g,
+                          const double *G, double *u, double *p) {
   using namespace kgpu;
   if (!tp || !cfg || !xbx || !xby || !xbz || !g || !G || !u || !p) return KGPU_EINVAL;
   const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, ng = cfg->ng, nv = cfg->nv;
-  if (nv != 9 || ny < 2 || nz < 2) return KGPU_EINVAL;
+  if (nv != (rp ? 13 : 9) || ny < 2 || nz < 2) return KGPU_EINVAL;
   Grid Gr;
   memset(&Gr, 0, sizeof(Gr));
   Gr.nx = nx; Gr.ny = ny; Gr.nz = nz; Gr.ng = ng; Gr.nv = nv;
@@ -297,7 +301,7 @@ extern "C" int kgpu_fm_torus_state(const kgpu_torus_params *tp, const kgpu_confi
       for (int ix = 0; ix < nx; ix++) {
         double x1 = xc(xbx, ix), x2 = xc(xby, iy);
         double r = m.r(x1), th = m.th(x2);
-        double pp[NVMAX], uu[NVMAX];
+        double pp[NVR], uu[NVR];
         double rhoatm = tp->atm_rho0 * pow(r, -1.5), uuatm = tp->atm_uu0 * pow(r, -2.5);
         pp[RHO] = rhoatm;
         pp[UU] = uuatm;
@@ -306,7 +310,8 @@ extern "C" int kgpu_fm_torus_state(const kgpu_torus_params *tp, const kgpu_confi
         Geom gm;
         geom_at(ix, iy, iz, gm);
         double lnh = fm_lnh_raw(a, l, r, th) - lnh0;
-        if (lnh > 0. && r >= tp->rin) {
+        const bool intorus = lnh > 0. && r >= tp->rin;
+        if (intorus) {
           double h = exp(lnh);
           double rho = pow((h - 1.) * (GAM - 1.) / (tp->kappa * GAM), 1. / (GAM - 1.)) / rhomax;
           double ui = tp->kappa * pow(rho * rhomax, GAM) / (GAM - 1.) / rhomax;
@@ -327,8 +332,29 @@ extern "C" int kgpu_fm_torus_state(const kgpu_torus_params *tp, const kgpu_confi
           pp[VX] = v[1]; pp[VY] = v[2]; pp[VZ] = v[3];
           Aphi[cell_index(Gr, ix, iy, iz)] = rho - 0.2 > 0. ? rho - 0.2 : 0.;
         }
+        if (rp) {
+          if (intorus || eradatm < 0.) {
+            // the temperature at which gas and radiation carry the torus
+            // pressure together, b T + a T^4 = p: Newton steps from the
+            // smaller one-component solution fall monotonically onto it
+            const double P = (GAM - 1.) * pp[UU];
+            const double aa = 4. * rp->sigma / 3., bb = rp->kb * pp[RHO] / rp->mu / rp->mp;
+            double T = P / bb, T4 = sqrt(sqrt(P / aa));
+            if (T4 < T) T = T4;
+            for (int it = 0; it < 100; it++) T -= (bb * T + aa * T * T * T * T - P) / (bb + 4. * aa * T * T * T);
+            pp[UU] = rp->kb * pp[RHO] * T / rp->mu / rp->mp / (GAM - 1.);
+            pp[EE0] = 4. * rp->sigma * T * T * T * T;
+            pp[FX0] = pp[VX];
+            pp[FY0] = pp[VY];
+            pp[FZ0] = pp[VZ];
+          } else {
+            pp[EE0] = eradatm * pp[UU];
+            pp[FX0] = pp[FY0] = pp[FZ0] = 0.;
+          }
+        }
         pp[ENTR] = calc_Sfromu(GAM, pp[RHO], pp[UU]);
         p2u_full(Gr, pp, uu, gm);
+        if (rp) p2u_rad(pp, uu, gm);
         long c = cell_index(Gr, ix, iy, iz);
         for (int iv = 0; iv < nv; iv++) {
           p[c * nv + iv] = pp[iv];
@@ -385,8 +411,22 @@ extern "C" int kgpu_fm_torus_state(const kgpu_torus_params *tp, const kgpu_confi
         Geom gm;
         geom_at(ix, iy, iz, gm);
         p2u_full(Gr, pp, u + c * nv, gm);
+        if (rp) p2u_rad(pp, u + c * nv, gm);
       }
   return 0;
+}
+
+extern "C" int kgpu_fm_torus_state(const kgpu_torus_params *tp, const kgpu_config *cfg, const double *xbx,
+                                   const double *xby, const double *xbz, const double *g, const double *G, double *u,
+                                   double *p) {
+  return fm_torus_state(tp, cfg, nullptr, 0., xbx, xby, xbz, g, G, u, p);
+}
+
+extern "C" int kgpu_fm_radtorus_state(const kgpu_torus_params *tp, const kgpu_rad_params *rp, double eradatm,
+                                      const kgpu_config *cfg, const double *xbx, const double *xby, const double *xbz,
+                                      const double *g, const double *G, double *u, double *p) {
+  if (!rp) return KGPU_EINVAL;
+  return fm_torus_state(tp, cfg, rp, eradatm, xbx, xby, xbz, g, G, u, p);
 }
 
 // Density floor rho >= atm_rho0 * r^-1.5 tabulated per x-index at cell

@@ -5,13 +5,26 @@
  * with r_in = 6, r_max = 12, Gamma = 13/9, one poloidal loop from
  * A_phi = max(rho/rho_max - 0.2, 0) normalised to beta_min = 100, 2% seeded
  * pressure noise, density floor 1e-4 r^-1.5.  MP5 + HLL + flux-CT, RK2.
- * The grid may be overridden with -DTNX/-DTNY/-DTNZ for small parity builds. */
+ * The grid may be overridden with -DTNX/-DTNY/-DTNZ for small parity builds.
+ *
+ * With -DTORUS_RADIATION the same torus carries M1 radiation, initialised
+ * in local thermal equilibrium with the gas: the pressure of the torus
+ * solution is shared by gas and radiation at one temperature T
+ * (p = k rho T / (mu m_p) + 4 sigma T^4 / 3), E = 4 sigma T^4 in the frame
+ * of the gas; Kramers-type absorption 6.4e22 rho T^-3.5 and electron
+ * scattering 0.34 cm^2/g; the implicit lab-frame source solve; RK2IMEX
+ * time stepping.  The torus keeps its code-unit density (maximum 1), as
+ * without radiation; the black-hole mass (default 1e16 Msun) sets the
+ * radiation units: with it the torus is optically thick to scattering
+ * (kappa_es rho = 3.1e6 per GM/c^2 at the maximum) and radiation-pressure
+ * dominated, and kappa dt of the implicit solve stays of order 1e4.  The
+ * atmosphere keeps its gas energy and carries a faint radiation field at
+ * rest with it (E = TORUS_ERADATM u, default 1e-6). */
 #define MYCOORDS MKS2COORDS
 #define MKSR0 0.
 #define MKSH0 0.6
 #define METRICAXISYMMETRIC
 #define BHSPIN 0.9
-#define MASS 10.
 
 #define MAGNFIELD
 #define VECPOTGIVEN
@@ -19,7 +32,35 @@
 
 #define INT_ORDER 4
 #define FLUXMETHOD HLL_FLUX
+#ifdef TORUS_RADIATION
+#define RADIATION
+#define TIMESTEPPING RK2IMEX
+#ifndef TORUS_KRAMERS
+#define TORUS_KRAMERS 6.4e22
+#endif
+#ifndef TORUS_KES
+#define TORUS_KES 0.34
+#endif
+#ifndef TORUS_MASS
+#define TORUS_MASS 1.e16
+#endif
+/* radiative wave speeds from the rest-frame 1/sqrt(3) without the
+ * optical-depth limiter (rad.c:2489-2502): with the limiter the time step
+ * of this optically thick, radiation-supported torus follows the gas sound
+ * speed alone and the explicit update is unstable */
+#define SKIPRADWAVESPEEDLIMITER
+#ifndef TORUS_ERADATM
+#define TORUS_ERADATM 1.e-6
+#endif
+#else
 #define TIMESTEPPING RK2
+#endif
+/* black-hole mass in solar masses: sets the units of the radiation physics
+ * only */
+#ifndef TORUS_MASS
+#define TORUS_MASS 10.
+#endif
+#define MASS TORUS_MASS
 #define TSTEPLIM 0.5
 #define FLUXLIMITER 0
 #define MINMOD_THETA 1.5

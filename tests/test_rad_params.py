@@ -18,7 +18,8 @@ def test_rad_params_equal_reference(kgpu, oracle):
              (rp.masscm, c[6]), (rp.gammamaxrad, c[7]), (rp.eradfloor, c[8]), (rp.eps, c[9]), (rp.conv, c[10]),
              (rp.entrconv, c[11]), (rp.maxiter, c[12]), (rp.dampfac, c[13]), (rp.maxdown, c[14]),
              (rp.maxup, c[15]), (rp.maxdamping, c[16]), (rp.threshold, c[17]), (rp.gammasmalllimit, c[18]),
-             (rp.numepsilon, c[19])]
+             (rp.numepsilon, c[19]), (rp.eerhoratiomin, c[20]), (rp.eerhoratiomax, c[21]),
+             (rp.eeuuratiomin, c[22]), (rp.eeuuratiomax, c[23])]
     for i, (a, b) in enumerate(pairs):
         assert a == b, (i, a, b)
 

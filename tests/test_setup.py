@@ -69,3 +69,25 @@ def test_fm_torus_floor_matches_reference(kgpu, ref):
                                           c.ctypes.data_as(dp), f.ctypes.data_as(dp)) == 0
     rc, rf = ref.rhofloor_table()
     assert np.allclose(c, rc, rtol=1e-13, atol=0) and np.allclose(f, rf, rtol=1e-13, atol=0)
+
+
+@pytest.mark.skipif(not ref_lib_available("libkref_radtorus_small.so"), reason="radiative torus build not present")
+def test_fm_radtorus_state_matches_reference(kgpu, oracle):
+    """The radiative torus: gas and radiation share the torus pressure at one
+    temperature; the partition and the radiation energy are computed with the
+    reference's operations, so they agree bit for bit where the MHD state
+    does (density, gas energy); velocities to the metric's precision."""
+    R = oracle.RefKoral("libkref_radtorus_small.so")
+    R.init()
+    tp = kgpu.torus_params()
+    cfg = kgpu.radtorus_config(R.nx, R.ny, R.nz)
+    xb = R.grid_faces()
+    tabs = kgpu.mks2_metric_tables(tp, cfg, xb)
+    rp = kgpu.rad_params(mass=kgpu.RADTORUS_MASS, gamma=13.0 / 9.0)
+    u, p = kgpu.fm_radtorus_state(tp, rp, kgpu.RADTORUS_ERADATM, cfg, xb, tabs[0], tabs[1])
+    g = R.ng
+    mine, theirs = p[g:-g, g:-g, g:-g], R.array("p")[g:-g, g:-g, g:-g]
+    for v, tol in ((0, 0.), (1, 0.), (5, 0.), (9, 0.), (2, 1e-10), (3, 1e-10), (4, 1e-10), (10, 1e-10), (11, 1e-10),
+                   (12, 1e-10), (6, 1e-9), (7, 1e-9), (8, 1e-9)):
+        scale = np.abs(theirs[..., v]).max() + 1e-300
+        assert np.abs(mine[..., v] - theirs[..., v]).max() <= tol * scale, v
