@@ -47,6 +47,12 @@ WORKLOADS = {
     "ot128": dict(desc="relativistic Orszag-Tang vortex 128x128 (Minkowski, PPM+LLF+flux-CT, RK2, CFL 0.5, Gamma 5/3)",
                   shape=(128, 128, 1), ref_lib="libkref_orszagrel_128_omp.so", ref_serial="libkref_orszagrel_128.so",
                   ref_sample_steps=40),
+    "radtorus": dict(desc="3D magnetised radiative Kerr torus 256x128x64 (the torus above plus M1 radiation in LTE "
+                          "with the gas at one temperature, Kramers + electron scattering, M = 1e16 Msun, faint "
+                          "atmosphere radiation 1e-6 u; MP5+HLL+flux-CT, RK2IMEX with the implicit source solve "
+                          "every substep, batched solver + learned warm start, one CUDA graph per step, CFL 0.5)",
+                     shape=(256, 128, 64), ref_lib="libkref_radtorus_omp.so", ref_serial="libkref_radtorus_omp.so",
+                     ref_sample_steps=1, radiation=True),
     "radcells": dict(desc="batched implicit gas-radiation source solve, 2^22 independent cells (Kerr-Schild a=0.9, "
                           "r log-U[2,100] M, theta U[0.1,pi-0.1], log-U rho [1e-8,1], T [1e4,1e12] K, "
                           "E_rad/rho [1e-10,1e2], tau [1e-3,1e5], gas Lorentz factor [1,20], flux fraction [0,0.99], "
@@ -63,6 +69,8 @@ def make_subdomain(kgpu, name):
     nx, ny, nz = wl["shape"]
     if name == "torus":
         return kgpu.fm_torus(nx, ny, nz)
+    if name == "radtorus":
+        return kgpu.radtorus(nx, ny, nz)
     return kgpu.orszag_tang(nx)
 
 
@@ -389,6 +397,190 @@ def our_arm(args, wl, rank, world, local_rank):
 
 
 # ---------------------------------------------------------------------------
+# our arm, radiative torus (RK2IMEX)
+# ---------------------------------------------------------------------------
+def warmstart_network(k):
+    """The warm-start network for the radiative torus: the weights trained on
+    the torus's own implicit solves when present, else those trained on the
+    batched-solve distribution."""
+    from koral_b200 import train_warmstart as tw
+    for name in ("warmstart_radtorus.npz", "warmstart_mlp.npz"):
+        path = os.path.join(ROOT, "koral_b200", "data", name)
+        if os.path.exists(path):
+            return tw.load(k, path), name
+    return None, None
+
+
+def our_arm_radtorus(args, wl, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import koral_b200 as k
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    from koral_b200 import build
+    build.build()
+    s = make_subdomain(k, args.workload)
+    mlp, mlp_name = warmstart_network(k)
+    ext = torch.cuda.ExternalStream(s.stream, device=dev)
+    nx, ny, nz = wl["shape"]
+    cells = nx * ny * nz
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # 256 MB > 126 MB L2
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        dist = dist_
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def dmax(ms):
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_steps(kk, graph=True, profile=False):
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(kk)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(kk)]
+        if profile:
+            s.profile(True)
+            s.profile_reset()
+        for i in range(kk):
+            with torch.cuda.stream(ext):
+                flush.fill_(float(i))
+                starts[i].record(ext)
+            s.rk2imex_steps(1, graph=graph and not profile)
+            with torch.cuda.stream(ext):
+                ends[i].record(ext)
+        torch.cuda.synchronize(dev)
+        if profile:
+            s.profile(False)
+        return sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+
+    def leg(mode, warm, kk):
+        """kk steps from the saved state with the given solver; device ms,
+        solver statistics and the end state"""
+        s.set_implicit_solver(mode, warm)
+        s.upload_state(u_start.copy(), p_start.copy())
+        s.tstepdenmax = tsd_start
+        s.reset_counters()
+        barrier()
+        ms = dmax(timed_steps(kk))
+        c = s.counters()
+        u, _ = s.download_state()
+        return ms, c, u
+
+    def newton(c):
+        return {"solves": int(c["imp_solves"]), "mean_iterations_per_solve": c["imp_iters"] / max(1, c["imp_solves"]),
+                "mean_evaluations_per_solve": c["imp_evals"] / max(1, c["imp_solves"]),
+                "failed_solves": int(c["radimp_failed"]), "fallbacks": int(c["imp_fallbacks"]),
+                "radiation_corrections": int(c["rad_corrected"])}
+
+    # warm-up from the initial torus, then the timed run from the state reached
+    s.set_implicit_solver(k.RAD_BATCHED, mlp)
+    s.rk2imex_steps(max(1, args.warmup), graph=True)
+    u_start, p_start = s.download_state()
+    tsd_start = s.tstepdenmax
+    launches0 = s.launches
+    with ClockSampler(local_rank) as clk:
+        ms, c_main, u_main = leg(k.RAD_BATCHED, mlp, args.steps)
+    launches = s.launches - launches0
+    value = cells * args.steps * world / (ms / 1e3)
+    # the same steps without the network and with the one-thread-per-cell solver
+    ms_b, c_b, u_b = leg(k.RAD_BATCHED, None, args.steps)
+    kp = max(1, min(args.steps, 3))
+    ms_p, c_p, u_p = leg(k.RAD_PLAIN, None, kp)
+    g = s.cfg.ng
+
+    def l1(a, b):
+        a, b = a[g:-g, g:-g, g:-g], b[g:-g, g:-g, g:-g]
+        return [float(np.abs(a[..., v] - b[..., v]).sum() / (np.abs(b[..., v]).sum() + 1e-300)) for v in range(13)]
+
+    # per-kernel device times (events around each launch, stream replay)
+    s.set_implicit_solver(k.RAD_BATCHED, mlp)
+    s.upload_state(u_start.copy(), p_start.copy())
+    s.tstepdenmax = tsd_start
+    timed_steps(min(args.steps, 3), profile=True)
+    prof = s.profile_read()
+    total = sum(v[0] for v in prof.values())
+    top = max(prof.items(), key=lambda kv: kv[1][0])
+
+    # e2e through the C-ABI with pinned host buffers
+    shape = s.shape
+    hu = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+    hp = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+    hu.numpy()[...] = u_start
+    hp.numpy()[...] = p_start
+    L = k.lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    pu = ctypes.cast(hu.data_ptr(), dp)
+    pp = ctypes.cast(hp.data_ptr(), dp)
+    ke = max(1, min(args.steps, 3))
+    s.tstepdenmax = tsd_start
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(ext):
+        e0.record(ext)
+    for _ in range(ke):
+        k._check(L.kgpu_upload_state(s.h, pu, pp), "upload")
+        k._check(L.kgpu_rk2imex_steps(s.h, 1), "step")
+        k._check(L.kgpu_download_state(s.h, pu, pp), "download")
+    with torch.cuda.stream(ext):
+        e1.record(ext)
+    torch.cuda.synchronize(dev)
+    e2e_value = cells * ke * world / (dmax(e0.elapsed_time(e1)) / 1e3)
+    state_bytes = 2 * int(np.prod(shape)) * 8
+    if rank != 0:
+        return
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    nfaces = (nx + 1) * (ny + 2) * (nz + 2)
+    flux_ms = prof["k_flux_x"][0] / max(1, prof["k_flux_x"][1])
+    flux_gbs = 16 * 9 * nfaces / (flux_ms / 1e3) / 1e9 if flux_ms > 0 else None
+    it_main = c_main["imp_iters"] / max(1, c_main["imp_solves"])
+    it_b = c_b["imp_iters"] / max(1, c_b["imp_solves"])
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["desc"], "cells_per_gpu": cells, "l2": "flushed (256 MB write) before every step",
+                   "parallelism": "replicas" if world > 1 else "single subdomain",
+                   "graph": "one CUDA graph per RK2IMEX step", "warm_start_weights": mlp_name},
+        "newton": {"learned": newton(c_main), "batched_no_network": newton(c_b),
+                   "iteration_ratio": it_b / it_main if it_main > 0 else None},
+        "batched_no_network": {"value": cells * args.steps * world / (ms_b / 1e3), "unit": UNIT,
+                               "ms_per_step": ms_b / args.steps,
+                               "end_state_l1_vs_learned": l1(u_main, u_b)},
+        "plain": {"value": cells * kp * world / (ms_p / 1e3), "unit": UNIT, "ms_per_step": ms_p / kp,
+                  "steps": kp, "newton": newton(c_p)},
+        "roofline": {"kernel": "k_flux_x", "bound": "hbm", "achieved": flux_gbs, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": (flux_gbs / hbm_peak) if flux_gbs else None, "traffic": None,
+                     "peak_source": peak_src, "algorithmic_bytes_per_launch": 16 * 9 * nfaces},
+        "kernels": {kk: {"ms_per_launch": v[0] / max(1, v[1]), "share": v[0] / total if total else 0.}
+                    for kk, v in prof.items() if v[1]},
+        "top_kernel": top[0],
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        val, err = run_reference_cpu(wl, 1, 0, threads)
+        line["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": threads, "kind": "reference",
+                                "sample": ("1 full RK2IMEX step of the same workload from its initial state"
+                                           if val is not None else f"unavailable: {err}")}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
 # our arm, batched implicit solve
 # ---------------------------------------------------------------------------
 def learned_leg(k, rp, d_in, work, stream, n, st_plain, it_plain, args, dev):
@@ -597,6 +789,8 @@ def main():
     try:
         if "ncells" in wl:
             our_arm_radcells(args, wl, rank, world, local_rank)
+        elif wl.get("radiation"):
+            our_arm_radtorus(args, wl, rank, world, local_rank)
         else:
             our_arm(args, wl, rank, world, local_rank)
     finally:

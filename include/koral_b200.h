@@ -158,8 +158,9 @@ int kgpu_get_counters(kgpu_ctx *ctx, unsigned long long out[4]);
  * inversions corrected (U2PRAD fixup requests), [9] implicit solves where
  * every attempt failed (RADIMP fixups), [10] their Newton iterations over
  * all attempts, [11] passes of the batched solver with work, [12] warm-start
- * fallbacks, [13] implicit solves, [14] cells where the radiation floors
- * acted.  Returns how many were written. */
+ * fallbacks, [13] residual evaluations of the implicit solves, [14] implicit
+ * solves, [15] cells where the radiation floors acted.  Returns how many were
+ * written. */
 int kgpu_get_counters_ex(kgpu_ctx *ctx, unsigned long long *out, int n);
 /* Tuning: Newton steps a cell may take in the first inversion pass before
  * it is queued for the resumption pass (default 8; results do not depend
@@ -388,6 +389,15 @@ int kgpu_set_implicit_solver(kgpu_ctx *ctx, int mode, kgpu_mlp *warm);
  * replayed from a CUDA graph captured on the first call. */
 int kgpu_rk2imex_steps(kgpu_ctx *ctx, int nsteps);
 int kgpu_rk2imex_steps_graph(kgpu_ctx *ctx, int nsteps);
+/* Device buffers of the most recent implicit source step (cell-major, the
+ * domain cells with x fastest): its n cells' primitive guess and conserved
+ * input, the primitives it produced (the input where every attempt failed),
+ * metric points (20 + 20 doubles), time steps and status.  Valid until the
+ * next step; for diagnostics and for training the warm-start network on
+ * the cells a run solves. */
+int kgpu_get_implicit_buffers(kgpu_ctx *ctx, int *n, const double **pp_in, const double **uu_in,
+                              const double **pp_out, const double **g20, const double **G20, const double **dt,
+                              const int **status);
 
 /* The radiative torus (nv = 13): the pressure of the torus shared by gas and
  * M1 radiation in thermal equilibrium at one temperature (radiation frame

@@ -161,6 +161,8 @@ def lib():
                                                         ctypes.POINTER(Config)] + [_dp] * 7),
                            ("kgpu_init_fm_radtorus", [vp, ctypes.POINTER(TorusParams), rpp, ctypes.c_double,
                                                       ctypes.c_int]),
+                           ("kgpu_get_implicit_buffers", [vp, ctypes.POINTER(ctypes.c_int)] +
+                            [ctypes.POINTER(vp)] * 7),
                            ("kgpu_set_radiation", [vp, rpp, ctypes.c_int]),
                            ("kgpu_set_implicit_solver", [vp, ctypes.c_int, vp]),
                            ("kgpu_rk2imex_steps", [vp, ctypes.c_int]),
@@ -344,7 +346,7 @@ class Subdomain:
             _check(n, "kgpu_get_counters_ex")
         return dict(fixups=a[0], entropy=a[1], failed=a[2], negrho=a[3], iters_energy=a[4], iters_entropy=a[5],
                     paused=a[6], to_entropy=a[7], rad_corrected=a[8], radimp_failed=a[9], imp_iters=a[10],
-                    imp_passes=a[11], imp_fallbacks=a[12], imp_solves=a[13], rad_floors=a[14])
+                    imp_passes=a[11], imp_fallbacks=a[12], imp_evals=a[13], imp_solves=a[14], rad_floors=a[15])
 
     def set_radiation(self, rp, wavespeed_limiter=False):
         """Radiation in the step (nv = 13): M1 fluxes and speeds, u2p_rad and
@@ -360,6 +362,33 @@ class Subdomain:
         self._warm = warm
         _check(self.L.kgpu_set_implicit_solver(self.h, int(mode), warm.h if warm is not None else None),
                "kgpu_set_implicit_solver")
+
+    def implicit_buffers(self):
+        """Device pointers of the last implicit step's buffers: n and a dict of
+        pp_in, uu_in, pp_out ([n][13] doubles), g20, G20 ([n][20]), dt ([n]),
+        status ([n] int32)."""
+        n = ctypes.c_int()
+        ptrs = [ctypes.c_void_p() for _ in range(7)]
+        _check(self.L.kgpu_get_implicit_buffers(self.h, ctypes.byref(n), *[ctypes.byref(q) for q in ptrs]),
+               "kgpu_get_implicit_buffers")
+        names = ("pp_in", "uu_in", "pp_out", "g20", "G20", "dt", "status")
+        return n.value, {k: q.value for k, q in zip(names, ptrs)}
+
+    def implicit_pairs(self, rp):
+        """Warm-start network inputs and training targets (float device
+        tensors [n][16] and [n][5], targets NaN where the solve failed) of the
+        cells of the last implicit step."""
+        import torch
+        n, b = self.implicit_buffers()
+        X = torch.empty((n, 16), dtype=torch.float32, device="cuda")
+        T = torch.empty((n, 5), dtype=torch.float32, device="cuda")
+        vp = ctypes.c_void_p
+        _check(self.L.kgpu_rad_features_device(n, ctypes.byref(rp), vp(b["pp_in"]), vp(b["g20"]), vp(b["G20"]),
+                                               vp(b["dt"]), _vp(X), _stream()), "kgpu_rad_features_device")
+        _check(self.L.kgpu_rad_targets_device(n, ctypes.byref(rp), vp(b["pp_in"]), vp(b["pp_out"]), vp(b["g20"]),
+                                              vp(b["G20"]), vp(b["status"]), _vp(T), _stream()),
+               "kgpu_rad_targets_device")
+        return X, T
 
     def rk2imex_steps(self, n=1, graph=False):
         fn = self.L.kgpu_rk2imex_steps_graph if graph else self.L.kgpu_rk2imex_steps

@@ -2097,6 +2097,22 @@ static int ready_rad(kgpu_ctx *c) {
   return ensure_packed(c);
 }
 
+extern "C" int kgpu_get_implicit_buffers(kgpu_ctx *c, int *n, const double **pp_in, const double **uu_in,
+                                         const double **pp_out, const double **g20, const double **G20,
+                                         const double **dt, const int **status) {
+  if (!c || !n) return KGPU_EINVAL;
+  if (!c->G.rad) return KGPU_ESTATE;
+  *n = (int)c->nimp;
+  if (pp_in) *pp_in = c->imp_pp;
+  if (uu_in) *uu_in = c->imp_uu;
+  if (pp_out) *pp_out = c->imp_ppo;
+  if (g20) *g20 = c->imp_g;
+  if (G20) *G20 = c->imp_G;
+  if (dt) *dt = c->imp_dt;
+  if (status) *status = c->imp_status;
+  return 0;
+}
+
 extern "C" int kgpu_rk2imex_steps(kgpu_ctx *c, int nsteps) {
   int r = ready_rad(c);
   if (r) return r;

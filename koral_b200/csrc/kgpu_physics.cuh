@@ -69,9 +69,10 @@ enum CounterSlot {
   C_IMP_ITERS = 10,  // Newton iterations of the implicit solves, all attempts
   C_IMP_PASSES = 11, // passes of the batched solver that had work
   C_IMP_FALLBACK = 12,  // warm-started solves that fell back to the reference cascade
-                        // (10..12 are the solver's own statistics, in its order)
-  C_IMP_SOLVES = 13, // implicit source solves
-  C_RADFLOOR = 14,   // cells whose radiation floors acted
+  C_IMP_EVALS = 13,  // residual evaluations of the implicit solves
+                     // (10..13 are the solver's own statistics, in its order)
+  C_IMP_SOLVES = 14, // implicit source solves
+  C_RADFLOOR = 15,   // cells whose radiation floors acted
   C_NCNT = 16
 };
 

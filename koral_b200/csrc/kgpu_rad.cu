@@ -78,7 +78,8 @@ struct Work {
   double *wguess;   // [n][13] the predicted iterate (warm start only)
   int *q[2][2];     // queues of cell indices [pass parity][primitives of the running attempt]
   int *count;       // [passes + 2][2] queue lengths
-  unsigned long long *stats;  // [0] Newton iterations, [1] passes, [2] fallbacks of the warm start
+  unsigned long long *stats;  // [0] Newton iterations, [1] passes, [2] fallbacks of the warm start,
+                              // [3] residual evaluations
 };
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -167,7 +168,10 @@ __global__ void __launch_bounds__(128) k_rad_plain(RadParams R, Cell C, int n, u
   }
   if (r == IMP_DONE_OK) cell_success(R, C, k, rg, s.pp, s.att, s.iter);
   else cell_failure(C, k);
-  if (stats) warp_add(stats, (unsigned)((1 << 30) - budget));
+  if (stats) {
+    warp_add(stats, (unsigned)((1 << 30) - budget));
+    warp_add(stats + 3, s.evals);
+  }
 }
 
 // Start of the batched form: every cell's cascade state (first attempt,
@@ -236,6 +240,7 @@ __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, i
     }
     warp_add(W.stats, (unsigned)(K - budget));
     warp_add(W.stats + 2, (unsigned)(warm0 && !s.warm));
+    warp_add(W.stats + 3, s.evals);
     const bool paused = r == IMP_PAUSE;
     const int type = paused ? imp_attempt(s.att, s.sw).prim : 0;
     warp_push(W.q[par ^ 1][0], W.count + (p + 1) * 2 + 0, paused && type == 0, k);
@@ -382,9 +387,9 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
     unsigned long long *dstats = acc;
     DevMem sm;
     if (stats) {
-      RCK(cudaMalloc(&sm.p, sizeof(unsigned long long)));
+      RCK(cudaMalloc(&sm.p, 4 * sizeof(unsigned long long)));
       dstats = (unsigned long long *)sm.p;
-      RCK(cudaMemsetAsync(dstats, 0, sizeof(unsigned long long), st));
+      RCK(cudaMemsetAsync(dstats, 0, 4 * sizeof(unsigned long long), st));
     }
     k_rad_plain<<<(n + 127) / 128, 128, 0, st>>>(R, C, n, dstats);
     RCK(cudaGetLastError());

@@ -1,13 +1,17 @@
 """Train the warm-start network of the implicit radiation solve on the GPU.
 
-    python -m koral_b200.train_warmstart [--n 16777216] [--epochs 6] [--out FILE]
+    python -m koral_b200.train_warmstart [--source cells|radtorus] [--n 16777216]
+                                         [--epochs 24] [--out FILE]
 
-Training pairs come from the product's own plain solver: random radiating
-cells of the batched-solve distribution extended with a magnetic field
-(B^i g_ij B^j / rho log-uniform in [1e-3, 1e3]), solved to RADIMPCONV; the
-input is the cell's state before the solve (16 features), the target the
-change to the converged state (5 numbers).  Cells whose solve fails are
-left out.  The network (16 -> 128 -> 128 -> 5, BF16 tensor-core kernels
+Training pairs come from the product's own solver without a warm start,
+solved to RADIMPCONV; the input is the cell's state before the solve (16
+features), the target the change to the converged state (5 numbers); cells
+whose solve fails are left out.  Two sources:
+  cells     random radiating cells of the batched-solve distribution
+            extended with a magnetic field (B^i g_ij B^j / rho log-uniform in
+            [1e-3, 1e3]);
+  radtorus  the cells of the radiative torus (256x128x64) as its own RK2IMEX
+            run solves them, one implicit step per time step.  The network (16 -> 128 -> 128 -> 5, BF16 tensor-core kernels
 with FP32 accumulation) is trained with Adam by the library's own forward
 and backward kernels; the outputs are standardised with the targets' mean
 and standard deviation, which are stored with the weights.  The velocity
@@ -26,6 +30,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "data", "warmstart_mlp.npz")
+DEFAULT_OUT_RADTORUS = os.path.join(HERE, "data", "warmstart_radtorus.npz")
 SIGMA = (1e-3, 1e3)
 
 
@@ -49,6 +54,49 @@ def make_pairs(k, rp, n, seed, chunk=1 << 20, log=print):
         c += 1
         log(f"  pairs {done}/{n}: kept {int(ok.sum())} of {m}")
     return torch.cat(Xs), torch.cat(Ts)
+
+
+def make_pairs_radtorus(k, rp, n, log=print, shape=(256, 128, 64)):
+    """Features and targets of the implicit solves of a radiative torus run
+    (the second implicit step of each time step), and the running context."""
+    import torch
+    s = k.radtorus(*shape, rp=rp)
+    s.set_implicit_solver(k.RAD_BATCHED, None)
+    Xs, Ts = [], []
+    done = 0
+    step = 0
+    while done < n:
+        s.rk2imex_steps(1, graph=True)
+        X, T = s.implicit_pairs(rp)
+        ok = torch.isfinite(T).all(dim=1) & torch.isfinite(X).all(dim=1)
+        m = min(int(ok.sum()), n - done)
+        Xs.append(X[ok][:m])
+        Ts.append(T[ok][:m])
+        done += m
+        step += 1
+        log(f"  torus step {step}: pairs {done}/{n}")
+    return torch.cat(Xs), torch.cat(Ts), s
+
+
+def evaluate_radtorus(k, mlp, rp, s, advance=2):
+    """Held-out: the torus run advanced further, then one implicit step from
+    the same state without and with the network (mean Newton iterations per
+    solve over all attempts, failed solves, fallbacks)."""
+    s.set_implicit_solver(k.RAD_BATCHED, None)
+    s.rk2imex_steps(advance, graph=True)
+    u, p = s.download_state()
+    dt = (1. - 2. ** -0.5) / s.tstepdenmax
+    res = {}
+    for tag, warm in (("plain", None), ("learned", mlp)):
+        s.set_implicit_solver(k.RAD_BATCHED, warm)
+        s.upload_state(u.copy(), p.copy())
+        s.reset_counters()
+        s.op_implicit(0., dt)
+        c = s.counters()
+        res[tag] = dict(iterations=c["imp_iters"] / max(1, c["imp_solves"]), failed=int(c["radimp_failed"]),
+                        fallbacks=int(c["imp_fallbacks"]), solves=int(c["imp_solves"]))
+    res["ratio"] = res["plain"]["iterations"] / max(1e-300, res["learned"]["iterations"])
+    return res
 
 
 VELOCITY_WEIGHT = 3.0
@@ -77,12 +125,18 @@ def evaluate(k, mlp, rp, n=1 << 16, seed=99001, sigma=SIGMA):
                 guess_error_median_E=float(np.median(err[ok, 1])), cells=n, seed=seed)
 
 
-def train(n=1 << 24, epochs=24, batch=8192, lr=2e-3, decay=0.85, seed=4000, out=DEFAULT_OUT, log=print):
+def train(n=1 << 24, epochs=24, batch=8192, lr=2e-3, decay=0.85, seed=4000, out=None, log=print, source="cells"):
     import torch
     import koral_b200 as k
-    rp = k.rad_params()
     t0 = time.time()
-    X, T = make_pairs(k, rp, n, seed, log=log)
+    if source == "radtorus":
+        rp = k.rad_params(mass=k.RADTORUS_MASS, gamma=13.0 / 9.0)
+        X, T, run = make_pairs_radtorus(k, rp, n, log=log)
+        out = out or DEFAULT_OUT_RADTORUS
+    else:
+        rp = k.rad_params()
+        X, T = make_pairs(k, rp, n, seed, log=log)
+        out = out or DEFAULT_OUT
     t1 = time.time()
     mlp = k.Mlp(seed=7)
     blob = mlp.get()
@@ -101,9 +155,13 @@ def train(n=1 << 24, epochs=24, batch=8192, lr=2e-3, decay=0.85, seed=4000, out=
         log(f"  epoch {e}: lr {rate:.2e} mean loss {losses[-1]:.5f}")
     torch.cuda.synchronize()
     t2 = time.time()
-    meta = dict(pairs=int(X.shape[0]), cells=n, epochs=epochs, batch=batch, lr=lr, decay=decay, seed=seed,
-                losses=losses, pair_seconds=t1 - t0, train_seconds=t2 - t1, sigma=list(SIGMA))
-    meta["held_out"] = evaluate(k, mlp, rp)
+    meta = dict(source=source, pairs=int(X.shape[0]), cells=n, epochs=epochs, batch=batch, lr=lr, decay=decay,
+                seed=seed, losses=losses, pair_seconds=t1 - t0, train_seconds=t2 - t1)
+    if source == "radtorus":
+        meta["held_out"] = evaluate_radtorus(k, mlp, rp, run)
+    else:
+        meta["sigma"] = list(SIGMA)
+        meta["held_out"] = evaluate(k, mlp, rp)
     os.makedirs(os.path.dirname(out), exist_ok=True)
     np.savez(out, blob=mlp.get(), meta=json.dumps(meta))
     log(json.dumps(meta))
@@ -125,10 +183,11 @@ def main():
     ap.add_argument("--decay", type=float, default=0.85)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--source", default="cells", choices=["cells", "radtorus"])
     a = ap.parse_args()
     sys.path.insert(0, os.path.dirname(HERE))
-    train(a.n, a.epochs, a.batch, a.lr, a.decay, out=a.out, log=lambda s: print(s, flush=True))
+    train(a.n, a.epochs, a.batch, a.lr, a.decay, out=a.out, log=lambda s: print(s, flush=True), source=a.source)
 
 
 if __name__ == "__main__":
