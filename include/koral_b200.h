@@ -152,14 +152,17 @@ int kgpu_rk2_steps_graph(kgpu_ctx *ctx, int nsteps);
  * out[0] cells flagged for fixup, out[1] entropy inversions,
  * out[2] failed inversions (old primitives kept), out[3] negative densities. */
 int kgpu_get_counters(kgpu_ctx *ctx, unsigned long long out[4]);
-/* All counters (up to n, 16 in all): the four above, then Newton steps of
+/* All counters (up to n, 20 in all): the four above, then Newton steps of
  * the energy and of the entropy solves, energy solves paused after the first
  * pass, cells handed to the entropy equation; with radiation: [8] M1
  * inversions corrected (U2PRAD fixup requests), [9] implicit solves where
  * every attempt failed (RADIMP fixups), [10] their Newton iterations over
  * all attempts, [11] passes of the batched solver with work, [12] warm-start
- * fallbacks, [13] residual evaluations of the implicit solves, [14] implicit
- * solves, [15] cells where the radiation floors acted.  Returns how many were
+ * fallbacks, [13] residual evaluations of the implicit solves, [14] Newton
+ * steps of the MHD inversions nested in those evaluations, [15] their
+ * W-function evaluations, [16] evaluations whose nested inversion went over
+ * its per-lane cap and was handed to a whole warp, [17] implicit solves,
+ * [18] cells where the radiation floors acted.  Returns how many were
  * written. */
 int kgpu_get_counters_ex(kgpu_ctx *ctx, unsigned long long *out, int n);
 /* Tuning: Newton steps a cell may take in the first inversion pass before
@@ -356,6 +359,17 @@ int kgpu_mlp_train_epoch(kgpu_mlp *mlp, const float *X, const float *T, int n, i
 /* Tuning of the batched form: Newton iterations a cell may take per pass
  * (default 8; results do not depend on it).  Process-wide. */
 int kgpu_rad_set_pass_iters(int k);
+/* Tuning of the batched form: W-function evaluations the MHD inversion
+ * nested in one residual evaluation may take in a single lane before that
+ * evaluation is repeated by a whole warp with the damped trials tried 32 at a
+ * time (default 64; 0: never).  Results do not depend on it.  Process-wide;
+ * a context's captured step keeps the value it was captured with. */
+int kgpu_rad_set_inner_cap(int cap);
+/* Learned warm start: how many attempts of the cascade a warm-started cell
+ * runs from the predicted iterate (1..6, default 6) before the reference
+ * cascade runs from the reference guess.  Every cell still converges to
+ * RADIMPCONV or fails as the reference would.  Process-wide. */
+int kgpu_rad_set_warm_attempts(int k);
 /* M1 closure u2p_rad (u2prad.c:485) and p2u (p2u.c:40) of n cells, host
  * pointers; corrected[i] is u2p_rad's corrected flag. */
 int kgpu_rad_u2p_cells(int n, const kgpu_rad_params *rp, const double *uu, double *pp, const double *g,
@@ -385,6 +399,12 @@ int kgpu_set_radiation(kgpu_ctx *ctx, const kgpu_rad_params *rp, int wavespeed_l
  * the warm-start network (batched only; null for the reference's guess).
  * The network is borrowed: it must outlive its use by the context. */
 int kgpu_set_implicit_solver(kgpu_ctx *ctx, int mode, kgpu_mlp *warm);
+/* With a warm-start network: start from the prediction only the cells whose
+ * previous implicit solve in this context needed a later attempt of the
+ * cascade or more than `iters` Newton iterations (the others start from the
+ * reference guess, which the time step's own evolution keeps close);
+ * -1 (default): every cell. */
+int kgpu_set_warm_gate(kgpu_ctx *ctx, int iters);
 /* Whole RK2IMEX steps (ko.c:444-570), dt in device memory; and the same
  * replayed from a CUDA graph captured on the first call. */
 int kgpu_rk2imex_steps(kgpu_ctx *ctx, int nsteps);
@@ -392,12 +412,13 @@ int kgpu_rk2imex_steps_graph(kgpu_ctx *ctx, int nsteps);
 /* Device buffers of the most recent implicit source step (cell-major, the
  * domain cells with x fastest): its n cells' primitive guess and conserved
  * input, the primitives it produced (the input where every attempt failed),
- * metric points (20 + 20 doubles), time steps and status.  Valid until the
- * next step; for diagnostics and for training the warm-start network on
- * the cells a run solves. */
+ * metric points (20 + 20 doubles), time steps, status, the attempt that
+ * succeeded (0..5, -1) and its Newton iterations.  Valid until the next
+ * step; for diagnostics and for training the warm-start network on the
+ * cells a run solves.  Null output pointers are skipped. */
 int kgpu_get_implicit_buffers(kgpu_ctx *ctx, int *n, const double **pp_in, const double **uu_in,
                               const double **pp_out, const double **g20, const double **G20, const double **dt,
-                              const int **status);
+                              const int **status, const int **attempt, const int **iters);
 
 /* The radiative torus (nv = 13): the pressure of the torus shared by gas and
  * M1 radiation in thermal equilibrium at one temperature (radiation frame

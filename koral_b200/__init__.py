@@ -140,6 +140,8 @@ def lib():
         L.kgpu_rad_u2p_cells.argtypes = [ctypes.c_int, rpp] + [_dp] * 4 + [ip_] * 2
         L.kgpu_rad_p2u_cells.argtypes = [ctypes.c_int, rpp] + [_dp] * 4
         L.kgpu_rad_set_pass_iters.argtypes = [ctypes.c_int]
+        L.kgpu_rad_set_inner_cap.argtypes = [ctypes.c_int]
+        L.kgpu_rad_set_warm_attempts.argtypes = [ctypes.c_int]
         L.kgpu_ks_metric.argtypes = [ctypes.c_double] * 3 + [_dp] * 2
         L.kgpu_ks_metric_batch.argtypes = [ctypes.c_double, ctypes.c_int] + [_dp] * 4
         L.kgpu_fp64_peak.argtypes = [_dp]
@@ -162,9 +164,10 @@ def lib():
                            ("kgpu_init_fm_radtorus", [vp, ctypes.POINTER(TorusParams), rpp, ctypes.c_double,
                                                       ctypes.c_int]),
                            ("kgpu_get_implicit_buffers", [vp, ctypes.POINTER(ctypes.c_int)] +
-                            [ctypes.POINTER(vp)] * 7),
+                            [ctypes.POINTER(vp)] * 9),
                            ("kgpu_set_radiation", [vp, rpp, ctypes.c_int]),
                            ("kgpu_set_implicit_solver", [vp, ctypes.c_int, vp]),
+                           ("kgpu_set_warm_gate", [vp, ctypes.c_int]),
                            ("kgpu_rk2imex_steps", [vp, ctypes.c_int]),
                            ("kgpu_rk2imex_steps_graph", [vp, ctypes.c_int])):
             getattr(L, name).argtypes = args
@@ -340,13 +343,14 @@ class Subdomain:
         _check(fn(self.h, int(n)), "kgpu_rk2_steps")
 
     def counters(self):
-        a = (ctypes.c_ulonglong * 16)()
-        n = self.L.kgpu_get_counters_ex(self.h, a, 16)
+        a = (ctypes.c_ulonglong * 20)()
+        n = self.L.kgpu_get_counters_ex(self.h, a, 20)
         if n < 0:
             _check(n, "kgpu_get_counters_ex")
         return dict(fixups=a[0], entropy=a[1], failed=a[2], negrho=a[3], iters_energy=a[4], iters_entropy=a[5],
                     paused=a[6], to_entropy=a[7], rad_corrected=a[8], radimp_failed=a[9], imp_iters=a[10],
-                    imp_passes=a[11], imp_fallbacks=a[12], imp_evals=a[13], imp_solves=a[14], rad_floors=a[15])
+                    imp_passes=a[11], imp_fallbacks=a[12], imp_evals=a[13], imp_inner=a[14], imp_inner_f=a[15],
+                    imp_cooperative=a[16], imp_solves=a[17], rad_floors=a[18])
 
     def set_radiation(self, rp, wavespeed_limiter=False):
         """Radiation in the step (nv = 13): M1 fluxes and speeds, u2p_rad and
@@ -366,12 +370,12 @@ class Subdomain:
     def implicit_buffers(self):
         """Device pointers of the last implicit step's buffers: n and a dict of
         pp_in, uu_in, pp_out ([n][13] doubles), g20, G20 ([n][20]), dt ([n]),
-        status ([n] int32)."""
+        status, attempt, iters ([n] int32)."""
         n = ctypes.c_int()
-        ptrs = [ctypes.c_void_p() for _ in range(7)]
+        ptrs = [ctypes.c_void_p() for _ in range(9)]
         _check(self.L.kgpu_get_implicit_buffers(self.h, ctypes.byref(n), *[ctypes.byref(q) for q in ptrs]),
                "kgpu_get_implicit_buffers")
-        names = ("pp_in", "uu_in", "pp_out", "g20", "G20", "dt", "status")
+        names = ("pp_in", "uu_in", "pp_out", "g20", "G20", "dt", "status", "attempt", "iters")
         return n.value, {k: q.value for k, q in zip(names, ptrs)}
 
     def implicit_pairs(self, rp):
@@ -389,6 +393,11 @@ class Subdomain:
                                               vp(b["G20"]), vp(b["status"]), _vp(T), _stream()),
                "kgpu_rad_targets_device")
         return X, T
+
+    def set_warm_gate(self, iters):
+        """Warm-start only cells whose previous solve took a later attempt or
+        more than `iters` Newton iterations (-1: every cell)."""
+        _check(self.L.kgpu_set_warm_gate(self.h, int(iters)), "kgpu_set_warm_gate")
 
     def rk2imex_steps(self, n=1, graph=False):
         fn = self.L.kgpu_rk2imex_steps_graph if graph else self.L.kgpu_rk2imex_steps

@@ -1255,7 +1255,7 @@ static const char *kKernelNames[K_NKERNELS] = {"k_bc", "k_wavespeeds", "k_flux_x
 int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
                            const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
                            int *status, int *attempt, int *iters, int mode, void *work, void *stream,
-                           unsigned long long *acc, long long *launches);
+                           unsigned long long *acc, long long *launches, int gate);
 kgpu::RadParams kgpu_rad_device_params(const kgpu_rad_params &p);
 
 struct ProfRec {
@@ -1299,6 +1299,7 @@ struct kgpu_ctx {
   float *imp_X = nullptr, *imp_Y = nullptr;
   int imp_mode = KGPU_RAD_BATCHED;
   kgpu_mlp *warm = nullptr;      // warm-start network, or none
+  int warm_gate = -1;            // warm-start only cells whose previous solve took more than this (-1: all)
   long long metric_gen = 0, packed_gen = -1;
 };
 
@@ -1983,6 +1984,8 @@ extern "C" int kgpu_set_radiation(kgpu_ctx *c, const kgpu_rad_params *rp, int wa
     AL(c->imp_ppo, n * NVR * d8); AL(c->imp_uuo, n * NVR * d8);
     AL(c->imp_g, n * 20 * d8); AL(c->imp_G, n * 20 * d8); AL(c->imp_dt, n * d8);
     AL(c->imp_status, n * sizeof(int)); AL(c->imp_att, n * sizeof(int)); AL(c->imp_it, n * sizeof(int));
+    CK(cudaMemsetAsync(c->imp_att, 0, n * sizeof(int), c->stream));
+    CK(cudaMemsetAsync(c->imp_it, 0, n * sizeof(int), c->stream));
     AL(c->imp_work, kgpu_rad_work_bytes((int)n));
 #undef AL
   }
@@ -2008,6 +2011,13 @@ extern "C" int kgpu_set_implicit_solver(kgpu_ctx *c, int mode, kgpu_mlp *warm) {
   }
   c->imp_mode = mode;
   c->warm = warm;
+  drop_graph(c);
+  return 0;
+}
+
+extern "C" int kgpu_set_warm_gate(kgpu_ctx *c, int iters) {
+  if (!c || iters < -1) return KGPU_EINVAL;
+  c->warm_gate = iters;
   drop_graph(c);
   return 0;
 }
@@ -2045,7 +2055,7 @@ static int enqueue_implicit(kgpu_ctx *c, const double *dtp, double fac) {
     long long nl = 0;
     int r = kgpu_rad_solve_enqueue(n, &c->rp, c->imp_uu, c->imp_pp, c->imp_g, c->imp_G, c->imp_dt, ypred, c->imp_ppo,
                                    c->imp_uuo, c->imp_status, c->imp_att, c->imp_it, c->imp_mode, c->imp_work,
-                                   c->stream, G.cnt + C_IMP_ITERS, &nl);
+                                   c->stream, G.cnt + C_IMP_ITERS, &nl, c->warm_gate);
     if (r) return r;
     c->launches += nl - 1;
   }
@@ -2099,7 +2109,8 @@ static int ready_rad(kgpu_ctx *c) {
 
 extern "C" int kgpu_get_implicit_buffers(kgpu_ctx *c, int *n, const double **pp_in, const double **uu_in,
                                          const double **pp_out, const double **g20, const double **G20,
-                                         const double **dt, const int **status) {
+                                         const double **dt, const int **status, const int **attempt,
+                                         const int **iters) {
   if (!c || !n) return KGPU_EINVAL;
   if (!c->G.rad) return KGPU_ESTATE;
   *n = (int)c->nimp;
@@ -2110,6 +2121,8 @@ extern "C" int kgpu_get_implicit_buffers(kgpu_ctx *c, int *n, const double **pp_
   if (G20) *G20 = c->imp_G;
   if (dt) *dt = c->imp_dt;
   if (status) *status = c->imp_status;
+  if (attempt) *attempt = c->imp_att;
+  if (iters) *iters = c->imp_it;
   return 0;
 }
 

@@ -70,10 +70,13 @@ enum CounterSlot {
   C_IMP_PASSES = 11, // passes of the batched solver that had work
   C_IMP_FALLBACK = 12,  // warm-started solves that fell back to the reference cascade
   C_IMP_EVALS = 13,  // residual evaluations of the implicit solves
-                     // (10..13 are the solver's own statistics, in its order)
-  C_IMP_SOLVES = 14, // implicit source solves
-  C_RADFLOOR = 15,   // cells whose radiation floors acted
-  C_NCNT = 16
+  C_IMP_INNER = 14,  // Newton steps of the MHD inversions nested in those evaluations
+  C_IMP_INNER_F = 15,   // their W-function evaluations (bracketing, steps, damped trials)
+  C_IMP_COOP = 16,   // evaluations handed to a whole warp (nested inversion over its cap)
+                     // (10..16 are the solver's own statistics, in its order)
+  C_IMP_SOLVES = 17, // implicit source solves
+  C_RADFLOOR = 18,   // cells whose radiation floors acted
+  C_NCNT = 20
 };
 
 // ---------------------------------------------------------------------------
@@ -495,11 +498,12 @@ KG_HD double u2p_initial_w(double GAMMA, const double *pp, const Geom &g) {
 }
 
 // W x 10 until the state is physical (u2p.c:2117-2135); 0 or -150
-KG_HD int u2p_bracket(double GAMMA, int Etype, const U2PCons &c, double &W) {
+KG_HD int u2p_bracket(double GAMMA, int Etype, const U2PCons &c, double &W, unsigned *fevals = nullptr) {
   double f0, dfdW, err;
   int i_increase = 0;
   while (true) {
     f0 = dfdW = 0.;
+    if (fevals) (*fevals)++;
     f_u2p(GAMMA, Etype, W - c.D, c, f0, dfdW, err);
     if (u2p_bad_w(W, c.Bsq, c.QdotBsq, c.Qt2, f0, dfdW) && (i_increase < 50)) {
       W *= 10.;
@@ -512,6 +516,9 @@ KG_HD int u2p_bracket(double GAMMA, int Etype, const U2PCons &c, double &W) {
 }
 
 constexpr int U2P_PAUSED = 1;
+// returned by a capped W solve that used up its function evaluations (the
+// caller repeats the whole inversion another way; nothing is kept)
+constexpr int U2P_OVER_CAP = 7;
 
 // Newton iterations (u2p.c:2140-2200) until convergence, failure, or a
 // pause: at the top of an iteration once iter reaches `stop`, or before an
@@ -521,13 +528,15 @@ constexpr int U2P_PAUSED = 1;
 // takes.  Returns 0 when the loop has ended (the caller finishes with
 // u2p_final), U2P_PAUSED, or a negative reference status on failure.
 KG_HD int u2p_newton(double GAMMA, double CONV, int Etype, const U2PCons &c, double &W, int &iter, int stop,
-                     int damp_budget = 1 << 30) {
+                     int damp_budget = 1 << 30, unsigned *fevals = nullptr, unsigned fcap = 0) {
   const double D = c.D;
   double f0, dfdW, err;
   while (true) {
     if (iter >= stop && iter < 50) return U2P_PAUSED;
+    if (fcap && *fevals >= fcap) return U2P_OVER_CAP;
     double Wprev = W;
     iter++;
+    if (fevals) (*fevals)++;
     f_u2p(GAMMA, Etype, W - D, c, f0, dfdW, err);
     if (err < CONV) break;
     if (dfdW == 0.) {
@@ -540,8 +549,10 @@ KG_HD int u2p_newton(double GAMMA, double CONV, int Etype, const U2PCons &c, dou
     double dumpfac = 1.;
     while (true) {
       double f0t = 0., dft = 0., errt;
+      if (fevals) (*fevals)++;
       f_u2p(GAMMA, Etype, Wnew - D, c, f0t, dft, errt);
       if (u2p_bad_w(Wnew, c.Bsq, c.QdotBsq, c.Qt2, f0t, dft) && (idump < 100)) {
+        if (fcap && *fevals >= fcap) return U2P_OVER_CAP;
         idump++;
         if (idump >= damp_budget) {
           W = Wprev;
@@ -620,6 +631,25 @@ __device__ inline int u2p_newton_warp(double GAMMA, double CONV, int Etype, cons
 }
 #endif
 
+#ifdef __CUDACC__
+KG_HD int u2p_final(double GAMMA, const struct U2PState &s, double W, int iter, const double *uu, double *pp,
+                    const Geom &g);
+// u2p_solver_W with all 32 lanes of a warp on the same cell: the damped
+// trials of a Newton step are tried 32 at a time; same result.
+__device__ inline int u2p_solver_W_warp(const Grid &G, const double *uu, double *pp, const Geom &g, int Etype,
+                                        unsigned *iters = nullptr, unsigned *fevals = nullptr) {
+  U2PState s;
+  u2p_setup(uu, g, s);
+  double W = u2p_initial_w(G.gamma, pp, g);
+  if (u2p_bracket(G.gamma, Etype, s.c, W, fevals)) return -150;
+  int iter = 0;
+  int r = u2p_newton_warp(G.gamma, G.u2pconv, Etype, s.c, W, iter);
+  if (iters) *iters += (unsigned)iter;
+  if (r < 0) return r;
+  return u2p_final(G.gamma, s, W, iter, uu, pp, g);
+}
+#endif
+
 // checks and primitives from the converged W (u2p.c:2205-2292)
 KG_HD int u2p_final(double GAMMA, const U2PState &s, double W, int iter, const double *uu, double *pp, const Geom &g) {
   if (iter >= 50) return -102;
@@ -656,13 +686,20 @@ KG_HD int u2p_final(double GAMMA, const U2PState &s, double W, int iter, const d
 // Returns 0 on success or the reference's negative status codes.
 // Iteration counts are bounded exactly as in the reference (50 bracket
 // expansions, 50 Newton steps, 100 halvings), so every call terminates.
-KG_HD int u2p_solver_W(const Grid &G, const double *uu, double *pp, const Geom &g, int Etype) {
+// iters, when given, accumulates the Newton steps taken, fevals the
+// evaluations of the W function (bracketing, steps, damped trials); with
+// fcap the solve gives up (U2P_OVER_CAP, pp untouched) once *fevals reaches
+// fcap during the Newton steps
+KG_HD int u2p_solver_W(const Grid &G, const double *uu, double *pp, const Geom &g, int Etype,
+                       unsigned *iters = nullptr, unsigned *fevals = nullptr, unsigned fcap = 0) {
   U2PState s;
   u2p_setup(uu, g, s);
   double W = u2p_initial_w(G.gamma, pp, g);
-  if (u2p_bracket(G.gamma, Etype, s.c, W)) return -150;
+  if (u2p_bracket(G.gamma, Etype, s.c, W, fevals)) return -150;
   int iter = 0;
-  int r = u2p_newton(G.gamma, G.u2pconv, Etype, s.c, W, iter, 1 << 30);
+  int r = u2p_newton(G.gamma, G.u2pconv, Etype, s.c, W, iter, 1 << 30, 1 << 30, fevals, fcap);
+  if (r == U2P_OVER_CAP) return r;
+  if (iters) *iters += (unsigned)iter;
   if (r < 0) return r;
   return u2p_final(G.gamma, s, W, iter, uu, pp, g);
 }

@@ -77,12 +77,27 @@ struct Work {
   int *wwarm;       // [n] the cascade still runs from the predicted iterate
   double *wguess;   // [n][13] the predicted iterate (warm start only)
   int *q[2][2];     // queues of cell indices [pass parity][primitives of the running attempt]
-  int *count;       // [passes + 2][2] queue lengths
+  int *count;       // [passes + 2][3] queue lengths: the two queues of a pass, then its cooperative queue
+  int *qs;          // cooperative queue of the current pass: cell indices ...
+  ImpState *ss;     // ... and the states of their interrupted evaluations
+  int nslots;       // its capacity
   unsigned long long *stats;  // [0] Newton iterations, [1] passes, [2] fallbacks of the warm start,
-                              // [3] residual evaluations
+                              // [3] residual evaluations, [4] Newton steps of the nested MHD inversions,
+                              // [5] their W-function evaluations, [6] evaluations handed to a warp
 };
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+// capacity of the cooperative queue: an eighth of the cells (a cell that
+// finds the queue full carries on alone, without the cap)
+inline int slow_slots(int n) { return n / 8 > 1024 ? n / 8 : 1024; }
+
+// W-function evaluations a nested MHD inversion may take in one lane before
+// the evaluation is handed to a whole warp (a converged inversion typically
+// takes 3-6); 0 turns the cooperative pass off
+unsigned g_inner_cap = 64;
+// attempts of the cascade a warm-started cell runs from the predicted iterate
+// before the reference cascade from the reference guess
+int g_warm_attempts = IMP_NATTEMPTS;
 size_t work_layout(int n, int passes, Work *w, char *base) {
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -102,8 +117,12 @@ size_t work_layout(int n, int passes, Work *w, char *base) {
       p = take((size_t)n * 4);
       if (w) w->q[a][b] = (int *)p;
     }
-  p = take((size_t)(passes + 2) * 2 * 4); if (w) w->count = (int *)p;
-  p = take(4 * sizeof(unsigned long long)); if (w) w->stats = (unsigned long long *)p;
+  p = take((size_t)(passes + 2) * 3 * 4); if (w) w->count = (int *)p;
+  p = take(8 * sizeof(unsigned long long)); if (w) w->stats = (unsigned long long *)p;
+  const int slots = slow_slots(n);
+  p = take((size_t)slots * 4); if (w) w->qs = (int *)p;
+  p = take((size_t)slots * sizeof(ImpState)); if (w) w->ss = (ImpState *)p;
+  if (w) w->nslots = slots;
   return off;
 }
 
@@ -171,13 +190,18 @@ __global__ void __launch_bounds__(128) k_rad_plain(RadParams R, Cell C, int n, u
   if (stats) {
     warp_add(stats, (unsigned)((1 << 30) - budget));
     warp_add(stats + 3, s.evals);
+    warp_add(stats + 4, s.inner[0]);
+    warp_add(stats + 5, s.inner[1]);
   }
 }
 
 // Start of the batched form: every cell's cascade state (first attempt,
 // no iteration yet, the guess as iterate), queued by the primitives its
 // first attempt works on, so that warps of a pass run one kind of inversion.
-__global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypred) {
+// gate >= 0: only cells whose previous solve (the attempt and iteration
+// outputs, read before this solve overwrites them) needed a later attempt
+// or more than gate Newton iterations start from the prediction
+__global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypred, int gate) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   RadGeom rg;
@@ -187,7 +211,7 @@ __global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypr
   W.wsw[k] = sw;
   W.watt[k] = 0;
   W.wit[k] = 0;
-  if (ypred) {
+  if (ypred && (gate < 0 || C.attempt[k] != 0 || C.iters[k] > gate)) {
     // learned warm start: the first attempt begins at the predicted state
     double t[MLP_OUT], guess[NVR];
     for (int o = 0; o < MLP_OUT; o++) t[o] = ypred[(long)k * MLP_OUTP + o];
@@ -208,11 +232,24 @@ __global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypr
   warp_push(W.q[0][1], W.count + 1, type == 1, k);
 }
 
+// warp-aggregated append that returns each pushing lane's slot (or -1)
+__device__ inline int warp_slot(int *qcount, bool pred) {
+  const unsigned m = __activemask();
+  const unsigned bits = __ballot_sync(m, pred);
+  if (!bits) return -1;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(qcount, __popc(bits));
+  base = __shfl_sync(m, base, leader);
+  return pred ? base + __popc(bits & ((1u << lane) - 1u)) : -1;
+}
+
 // Pass p: the cells of queue p may start up to K Newton iterations;
 // unfinished ones keep their state (the iterate, its iteration count, the
 // attempt) and go to queue p+1, by the primitives of their running attempt.
-__global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, int n, int p, int K) {
-  const int n0 = W.count[p * 2 + 0], n1 = W.count[p * 2 + 1];
+__global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, int n, int p, int K,
+                                                  unsigned inner_cap, int warm_attempts) {
+  const int n0 = W.count[p * 3 + 0], n1 = W.count[p * 3 + 1];
   const int nin = n0 + n1;
   const int par = p & 1;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nin; q += gridDim.x * blockDim.x) {
@@ -227,6 +264,7 @@ __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, i
     s.sign = -1.;
     s.xiapp = 1.;
     s.evals = 0;
+    s.inner[0] = s.inner[1] = 0;
     s.sw = W.wsw[k];
     s.att = W.watt[k];
     s.iter = W.wit[k];
@@ -236,15 +274,33 @@ __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, i
     int budget = K;
     int r;
     const double *wg = W.wguess + (long)k * NVR;
-    while ((r = imp_advance(R, u0, p0, dt, rg, s, budget, wg)) == IMP_RUNNING) {
+    ImpInner how{nullptr, inner_cap, false, warm_attempts};
+    while (true) {
+      while ((r = imp_advance(R, u0, p0, dt, rg, s, budget, wg, &how)) == IMP_RUNNING) {
+      }
+      // an evaluation whose nested inversion ran out of its cap goes to the
+      // cooperative pass with the whole state; with the queue full the lane
+      // repeats it alone, without the cap
+      const int slot = warp_slot(W.count + p * 3 + 2, r == IMP_OVER_CAP);
+      if (r != IMP_OVER_CAP) break;
+      if (slot < W.nslots) {
+        W.qs[slot] = k;
+        W.ss[slot] = s;
+        break;
+      }
+      how.cap = 0;
     }
     warp_add(W.stats, (unsigned)(K - budget));
     warp_add(W.stats + 2, (unsigned)(warm0 && !s.warm));
     warp_add(W.stats + 3, s.evals);
+    warp_add(W.stats + 4, s.inner[0]);
+    warp_add(W.stats + 5, s.inner[1]);
+    warp_add(W.stats + 6, (unsigned)(r == IMP_OVER_CAP));
+    if (r == IMP_OVER_CAP) continue;
     const bool paused = r == IMP_PAUSE;
     const int type = paused ? imp_attempt(s.att, s.sw).prim : 0;
-    warp_push(W.q[par ^ 1][0], W.count + (p + 1) * 2 + 0, paused && type == 0, k);
-    warp_push(W.q[par ^ 1][1], W.count + (p + 1) * 2 + 1, paused && type == 1, k);
+    warp_push(W.q[par ^ 1][0], W.count + (p + 1) * 3 + 0, paused && type == 0, k);
+    warp_push(W.q[par ^ 1][1], W.count + (p + 1) * 3 + 1, paused && type == 1, k);
     if (paused) {
       W.watt[k] = s.att;
       W.wit[k] = s.iter;
@@ -257,6 +313,60 @@ __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, i
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && nin > 0) atomicAdd(W.stats + 1, 1ull);
+}
+
+// The cooperative part of pass p: each cell whose evaluation was handed
+// over is taken by a whole warp, which repeats that evaluation and goes on
+// with the cell for the rest of the pass's budget, every nested MHD
+// inversion run by the 32 lanes together; the arithmetic is the same, so
+// the cell's results are too.  Unfinished cells join the next pass.
+__global__ void __launch_bounds__(128) k_rad_slow(RadParams R, Cell C, Work W, int n, int p, int K,
+                                                  int warm_attempts) {
+  const int ns0 = W.count[p * 3 + 2];
+  const int ns = ns0 < W.nslots ? ns0 : W.nslots;
+  const int par = p & 1;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < ns; q += nwarps) {
+    const int k = W.qs[q];
+    ImpState s = W.ss[q];
+    RadGeom rg;
+    rad_geom(C.g + 20L * k, C.G + 20L * k, rg);
+    const double *u0 = C.uu + (long)k * NVR, *p0 = C.pp + (long)k * NVR;
+    const double dt = C.dt[k];
+    const double *wg = W.wguess + (long)k * NVR;
+    const int warm0 = s.warm;
+    const unsigned it0 = s.iter;
+    s.evals = 0;
+    s.inner[0] = s.inner[1] = 0;
+    int budget = K;
+    ImpInner how{nullptr, 0u, true, warm_attempts};
+    int r;
+    while ((r = imp_advance(R, u0, p0, dt, rg, s, budget, wg, &how)) == IMP_RUNNING) {
+    }
+    if (lane == 0) {
+      atomicAdd(W.stats, (unsigned long long)(K - budget));
+      if (warm0 && !s.warm) atomicAdd(W.stats + 2, 1ull);
+      atomicAdd(W.stats + 3, (unsigned long long)s.evals);
+      atomicAdd(W.stats + 4, (unsigned long long)s.inner[0]);
+      atomicAdd(W.stats + 5, (unsigned long long)s.inner[1]);
+      if (r == IMP_PAUSE) {
+        const int type = imp_attempt(s.att, s.sw).prim;
+        const int at = atomicAdd(W.count + (p + 1) * 3 + type, 1);
+        W.q[par ^ 1][type][at] = k;
+        W.watt[k] = s.att;
+        W.wit[k] = s.iter;
+        W.wwarm[k] = s.warm;
+        for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = s.pp[i];
+      } else if (r == IMP_DONE_OK) {
+        cell_success(R, C, k, rg, s.pp, s.att, s.iter);
+      } else {
+        cell_failure(C, k);
+      }
+    }
+    (void)it0;
+    __syncwarp();
+  }
 }
 
 __global__ void k_rad_u2p(RadParams R, int n, const double *uu, double *pp, const double *g, const double *G,
@@ -354,6 +464,18 @@ extern "C" int kgpu_rad_default_params(kgpu_rad_params *rp, double mass, double 
   return 0;
 }
 
+extern "C" int kgpu_rad_set_warm_attempts(int k) {
+  if (k < 1 || k > IMP_NATTEMPTS) return KGPU_EINVAL;
+  g_warm_attempts = k;
+  return 0;
+}
+
+extern "C" int kgpu_rad_set_inner_cap(int cap) {
+  if (cap < 0) return KGPU_EINVAL;
+  g_inner_cap = (unsigned)cap;
+  return 0;
+}
+
 extern "C" int kgpu_rad_set_pass_iters(int k) {
   if (k < 1) return KGPU_EINVAL;
   g_pass_iters = k;
@@ -372,7 +494,8 @@ extern "C" size_t kgpu_rad_work_bytes(int n) {
 static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
                             const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
                             int *status, int *attempt, int *iters, int mode, void *work, void *stream,
-                            unsigned long long *stats, int nstats, unsigned long long *acc = nullptr) {
+                            unsigned long long *stats, int nstats, unsigned long long *acc = nullptr,
+                            int gate = -1) {
   if (n < 0 || !rp || (mode != KGPU_RAD_PLAIN && mode != KGPU_RAD_BATCHED)) return KGPU_EINVAL;
   if (n > 0 && (!uu || !pp || !g || !G || !dt || !pp_out || !uu_out || !status || !attempt || !iters))
     return KGPU_EINVAL;
@@ -387,9 +510,9 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
     unsigned long long *dstats = acc;
     DevMem sm;
     if (stats) {
-      RCK(cudaMalloc(&sm.p, 4 * sizeof(unsigned long long)));
+      RCK(cudaMalloc(&sm.p, 8 * sizeof(unsigned long long)));
       dstats = (unsigned long long *)sm.p;
-      RCK(cudaMemsetAsync(dstats, 0, 4 * sizeof(unsigned long long), st));
+      RCK(cudaMemsetAsync(dstats, 0, 8 * sizeof(unsigned long long), st));
     }
     k_rad_plain<<<(n + 127) / 128, 128, 0, st>>>(R, C, n, dstats);
     RCK(cudaGetLastError());
@@ -405,17 +528,21 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
   char *base = (char *)(((uintptr_t)work + 255) & ~(uintptr_t)255);
   Work W;
   work_layout(n, passes, &W, base);   // fits: the area is sized for kMaxPasses >= passes
-  RCK(cudaMemsetAsync(W.count, 0, (size_t)(passes + 2) * 2 * 4, st));
+  RCK(cudaMemsetAsync(W.count, 0, (size_t)(passes + 2) * 3 * 4, st));
   if (acc) W.stats = acc;
-  else RCK(cudaMemsetAsync(W.stats, 0, 4 * sizeof(unsigned long long), st));
+  else RCK(cudaMemsetAsync(W.stats, 0, 8 * sizeof(unsigned long long), st));
   const int grid = sm_count() * 8;
-  k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n, ypred);
+  k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n, ypred, gate);
   RCK(cudaGetLastError());
   for (int p = 0; p < passes; p++) {
     const int Kp = p == passes - 1 ? (1 << 30) : K;   // the last pass finishes whatever is left
     const int blocks = p == 0 ? (n + 127) / 128 : grid;
-    k_rad_pass<<<blocks, 128, 0, st>>>(R, C, W, n, p, Kp);
+    k_rad_pass<<<blocks, 128, 0, st>>>(R, C, W, n, p, Kp, g_inner_cap, g_warm_attempts);
     RCK(cudaGetLastError());
+    if (g_inner_cap) {
+      k_rad_slow<<<grid / 2, 128, 0, st>>>(R, C, W, n, p, Kp, g_warm_attempts);
+      RCK(cudaGetLastError());
+    }
   }
   if (stats) {
     RCK(cudaMemcpyAsync(stats, W.stats, nstats * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
@@ -429,13 +556,13 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
 int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
                            const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
                            int *status, int *attempt, int *iters, int mode, void *work, void *stream,
-                           unsigned long long *acc, long long *launches) {
+                           unsigned long long *acc, long long *launches, int gate) {
   if (launches) {
     RadParams R = to_dev(*rp);
-    *launches = mode == KGPU_RAD_PLAIN ? 1 : 1 + max_passes(R, g_pass_iters);
+    *launches = mode == KGPU_RAD_PLAIN ? 1 : 1 + (g_inner_cap ? 2 : 1) * max_passes(R, g_pass_iters);
   }
   return rad_solve_device(n, rp, uu, pp, g, G, dt, ypred, pp_out, uu_out, status, attempt, iters, mode, work, stream,
-                          nullptr, 0, acc);
+                          nullptr, 0, acc, gate);
 }
 
 // Device form of the radiation constants, for the grid step.

@@ -375,12 +375,34 @@ struct ImpParams {
 };
 
 // MHD u2p inside the residual: energy equation only (u2p_solver, u2p.c:1219)
-KG_HD int imp_u2p_hot(const RadParams &R, const double *uu, double *pp, const Geom &g) {
+// How the nested MHD inversion of an evaluation runs: by one lane alone,
+// optionally with a cap on its W-function evaluations (a capped inversion
+// that runs out returns U2P_OVER_CAP and the evaluation is repeated in the
+// cooperative form), or by all 32 lanes of a warp on the same cell.
+struct ImpInner {
+  unsigned *stats;   // [0] Newton steps, [1] W-function evaluations, or null
+  unsigned cap;      // 0: no cap
+  bool warp;
+  int warm_attempts; // attempts of the cascade run from the predicted iterate (1..6)
+};
+
+// inner: where and how the nested inversion runs (see ImpInner)
+KG_HD int imp_u2p_hot(const RadParams &R, const double *uu, double *pp, const Geom &g, const ImpInner *inner = nullptr) {
   Grid G;
   G.gamma = R.gamma;
   G.u2pconv = R.u2pconv;
   G.nv = NVMAX;
-  return u2p_solver_W(G, uu, pp, g, 0);
+  unsigned *st = inner ? inner->stats : nullptr;
+#ifdef __CUDA_ARCH__
+  if (inner && inner->warp) return u2p_solver_W_warp(G, uu, pp, g, 0, st, st ? st + 1 : nullptr);
+#endif
+  if (inner && inner->cap) {
+    unsigned used = 0;
+    int r = u2p_solver_W(G, uu, pp, g, 0, st, &used, inner->cap);
+    if (st) st[1] += used;
+    return r;
+  }
+  return u2p_solver_W(G, uu, pp, g, 0, st, st ? st + 1 : nullptr);
 }
 
 KG_HD double rad_Sfromu(const RadParams &R, double rho, double u) { return calc_Sfromu(R.gamma, rho, u); }
@@ -391,7 +413,7 @@ KG_HD double rad_Sfromu(const RadParams &R, double rho, double u) { return calc_
 // verdict as the residual sees it: 0 or -1 usable, -2 failed; corr set
 // when the M1 closure was corrected.
 KG_HD int imp_counterpart(const RadParams &R, int prim, const double *uu0, double *pp, double *uu, const RadGeom &rg,
-                          int &corr) {
+                          int &corr, const ImpInner *inner = nullptr) {
   Grid G;
   G.gamma = R.gamma;
   G.nv = NVMAX;
@@ -404,7 +426,9 @@ KG_HD int imp_counterpart(const RadParams &R, int prim, const double *uu0, doubl
     uu[2] = uu0[2] - (uu[FX0] - uu0[FX0]);
     uu[3] = uu0[3] - (uu[FY0] - uu0[FY0]);
     uu[4] = uu0[4] - (uu[FZ0] - uu0[FZ0]);
-    return imp_u2p_hot(R, uu, pp, rg.g) < 0 ? -2 : 0;
+    const int r = imp_u2p_hot(R, uu, pp, rg.g, inner);
+    if (r == U2P_OVER_CAP) return r;
+    return r < 0 ? -2 : 0;
   }
   uu[EE0] = uu0[EE0] - (uu[1] - uu0[1]);
   uu[FX0] = uu0[FX0] - (uu[2] - uu0[2]);
@@ -425,10 +449,10 @@ KG_HD void imp_rho_from_velocity(const double *uu0, double *pp, const Geom &g) {
 // primitives, the entropy, the conserved state that goes with pp, and the
 // inversion of the other component (which updates pp in place).
 KG_HD int imp_prepare(const RadParams &R, const ImpParams &P, const double *uu0, double *pp, double *uu,
-                      const RadGeom &rg, int &corr) {
+                      const RadGeom &rg, int &corr, const ImpInner *inner = nullptr) {
   if (P.prim == IMP_MHD) imp_rho_from_velocity(uu0, pp, rg.g);
   pp[ENTR] = rad_Sfromu(R, pp[RHO], pp[UU]);
-  return imp_counterpart(R, P.prim, uu0, pp, uu, rg, corr);
+  return imp_counterpart(R, P.prim, uu0, pp, uu, rg, corr, inner);
 }
 
 // residual f[4] and its relative size from a prepared state (the rest of
@@ -556,7 +580,7 @@ KG_HD int imp_startwith(const RadParams &R, const double *pp0, const Geom &g) {
 // is in.  The sequence of operations per cell is the reference's.
 // ---------------------------------------------------------------------------
 enum ImpPhase { PH_BASE = 0, PH_JAC = 1, PH_DAMP = 2, PH_FINAL = 3 };
-enum ImpAdvance { IMP_RUNNING = 0, IMP_DONE_OK = 1, IMP_DONE_FAIL = 2, IMP_PAUSE = 3 };
+enum ImpAdvance { IMP_RUNNING = 0, IMP_DONE_OK = 1, IMP_DONE_FAIL = 2, IMP_PAUSE = 3, IMP_OVER_CAP = 4 };
 
 struct ImpState {
   double pp[NVR];      // the iterate
@@ -570,6 +594,7 @@ struct ImpState {
   int phase, j;
   int warm;            // the first attempt runs from a predicted iterate
   unsigned evals;      // evaluations performed (statistics)
+  unsigned inner[2];   // nested MHD inversions: Newton steps, W-function evaluations (statistics)
 };
 
 KG_HD void imp_begin(const RadParams &R, const double *pp00, const Geom &g, ImpState &s) {
@@ -583,6 +608,7 @@ KG_HD void imp_begin(const RadParams &R, const double *pp00, const Geom &g, ImpS
   s.xiapp = 1.;
   s.warm = 0;
   s.evals = 0;
+  s.inner[0] = s.inner[1] = 0;
 }
 
 // The attempt failed: the next one starts afresh, from the cell's guess, or
@@ -590,12 +616,16 @@ KG_HD void imp_begin(const RadParams &R, const double *pp00, const Geom &g, ImpS
 // warm cascade has failed in every attempt, the reference cascade runs
 // from the guess (the fallback), so a cell fails only where the reference
 // fails.
-KG_HD int imp_next_attempt(const double *pp00, const double *warm_guess, ImpState &s) {
+// With a warm start the first warm_attempts attempts run from the predicted
+// iterate; then the reference cascade runs from the reference guess.
+KG_HD int imp_next_attempt(const double *pp00, const double *warm_guess, ImpState &s,
+                           int warm_attempts = IMP_NATTEMPTS) {
   s.att++;
-  if (s.att >= IMP_NATTEMPTS) {
-    if (!s.warm) return IMP_DONE_FAIL;
+  if (s.warm && s.att >= warm_attempts) {
     s.warm = 0;
     s.att = 0;
+  } else if (s.att >= IMP_NATTEMPTS) {
+    return IMP_DONE_FAIL;
   }
   const double *start = s.warm ? warm_guess : pp00;
   for (int i = 0; i < NVR; i++) s.pp[i] = start[i];
@@ -608,8 +638,11 @@ KG_HD int imp_next_attempt(const double *pp00, const double *warm_guess, ImpStat
 // Newton iterations the cell may still start in this call sequence; at the
 // start of an iteration with no budget left the cell pauses (IMP_PAUSE)
 // with its state intact.
+// `how` sets how the nested MHD inversion runs (ImpInner); when a capped
+// inversion runs out the evaluation is abandoned with the state as before
+// the call (IMP_OVER_CAP), to be repeated in the cooperative form.
 KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00, double dt, const RadGeom &rg,
-                      ImpState &s, int &budget, const double *warm_guess = nullptr) {
+                      ImpState &s, int &budget, const double *warm_guess = nullptr, const ImpInner *how = nullptr) {
   const ImpParams P = imp_attempt(s.att, s.sw);
   const int sh = P.prim == IMP_MHD ? UU : EE0;
   const double CONV = P.eq == IMP_ENTROPY ? R.entrconv : R.conv;
@@ -648,17 +681,26 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
     for (int i = 0; i < NVR; i++) pin[i] = s.pp[i];
   }
   // the evaluation: other component's inversion, residual where needed
-  s.evals++;
+  ImpInner in{s.inner, how ? how->cap : 0u, how ? how->warp : false, IMP_NATTEMPTS};
+  const int wa = how ? how->warm_attempts : IMP_NATTEMPTS;
   int corr = 0;
-  int u2pret = imp_prepare(R, P, uu0, pin, uu, rg, corr);
+  int u2pret = imp_prepare(R, P, uu0, pin, uu, rg, corr, &in);
+  if (u2pret == U2P_OVER_CAP) {
+    if (s.phase == PH_BASE) {   // undo the start of the iteration
+      budget++;
+      s.iter--;
+    }
+    return IMP_OVER_CAP;
+  }
+  s.evals++;
   int fret = 0;
   if (s.phase == PH_BASE || s.phase == PH_JAC)
     fret = imp_residual(R, P, pin, uu, uu0, pp00, dt, rg, u2pret, corr, f, err);
   // transition
   if (s.phase == PH_BASE) {
-    if (fret < 0) return imp_next_attempt(pp00, warm_guess, s);
+    if (fret < 0) return imp_next_attempt(pp00, warm_guess, s, wa);
     if (err < CONV) {
-      if (s.iter > R.maxiter) return imp_next_attempt(pp00, warm_guess, s);   // converged past the limit (rad.c:1051)
+      if (s.iter > R.maxiter) return imp_next_attempt(pp00, warm_guess, s, wa);   // converged past the limit (rad.c:1051)
       s.phase = PH_FINAL;
       return IMP_RUNNING;
     }
@@ -671,7 +713,7 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
   if (s.phase == PH_JAC) {
     const int j = s.j;
     if (fret < 0) {
-      if (s.sign > 0.) return imp_next_attempt(pp00, warm_guess, s);
+      if (s.sign > 0.) return imp_next_attempt(pp00, warm_guess, s, wa);
       s.sign = 1.;
       return IMP_RUNNING;
     }
@@ -680,7 +722,7 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
     s.sign = -1.;
     if (s.j == 4) {
       double iJ[4][4];
-      if (inverse_44(s.J, iJ) < 0) return imp_next_attempt(pp00, warm_guess, s);
+      if (inverse_44(s.J, iJ) < 0) return imp_next_attempt(pp00, warm_guess, s, wa);
       for (int a = 0; a < 4; a++)
         for (int b = 0; b < 4; b++) s.J[a][b] = iJ[a][b];
       s.xiapp = 1.;
@@ -694,7 +736,7 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
     const double edenmin = s.ppp[sh] / R.maxdown;
     const double edenmax = s.ppp[sh] * R.maxup;
     if (xxx0 > edenmin && xxx0 < edenmax && u2pret >= -1) {
-      if (s.iter > R.maxiter) return imp_next_attempt(pp00, warm_guess, s);
+      if (s.iter > R.maxiter) return imp_next_attempt(pp00, warm_guess, s, wa);
       s.phase = PH_BASE;
       return IMP_RUNNING;
     }
@@ -704,13 +746,13 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
     } else {
       s.xiapp /= R.dampfac;
     }
-    if (s.xiapp < R.maxdamping) return imp_next_attempt(pp00, warm_guess, s);
+    if (s.xiapp < R.maxdamping) return imp_next_attempt(pp00, warm_guess, s, wa);
     return IMP_RUNNING;
   }
   // final inversion of the converged state (rad.c:1088-1150)
   for (int i = 0; i < NVR; i++) s.pp[i] = pin[i];
   if (P.prim == IMP_MHD && corr > 0) u2pret = -2;
-  if (u2pret < -1) return imp_next_attempt(pp00, warm_guess, s);
+  if (u2pret < -1) return imp_next_attempt(pp00, warm_guess, s, wa);
   return IMP_DONE_OK;
 }
 

@@ -56,12 +56,15 @@ def make_pairs(k, rp, n, seed, chunk=1 << 20, log=print):
     return torch.cat(Xs), torch.cat(Ts)
 
 
-def make_pairs_radtorus(k, rp, n, log=print, shape=(256, 128, 64)):
+def make_pairs_radtorus(k, rp, n, log=print, shape=(256, 128, 64), skip=3):
     """Features and targets of the implicit solves of a radiative torus run
-    (the second implicit step of each time step), and the running context."""
+    (the second implicit step of each time step, after `skip` steps), and
+    the running context."""
     import torch
     s = k.radtorus(*shape, rp=rp)
     s.set_implicit_solver(k.RAD_BATCHED, None)
+    if skip:
+        s.rk2imex_steps(skip, graph=True)
     Xs, Ts = [], []
     done = 0
     step = 0
