@@ -61,6 +61,38 @@ WORKLOADS = {
                      ref_sample_cells=1 << 17),
 }
 RAD_METRIC = "implicit solves/s (1 B200)"
+
+# From the ncu capture of the x-face flux kernel on the 192x96x64 torus
+# (profiles/k_flux_x_torus_192x96x64.md): DRAM bytes per launch and FP64
+# operations per face (DADD + DMUL + 2 DFMA thread instructions / faces).
+FLUX_X_TRAFFIC_BYTES_192 = 188.58e6
+FLUX_X_FACES_192 = 193 * 98 * 66
+FLUX_FP64_PER_FACE = 2420.
+
+
+def flux_roofline(prof, nx, ny, nz, hbm_peak, peak_src, fp64_peak):
+    """HBM roofline of the x-face flux kernel (algorithmic bytes 16 NV per
+    face over its event time) with the DRAM traffic ncu measured (scaled by
+    faces from the 192x96x64 capture), and its FP64 rate."""
+    nfaces = (nx + 1) * (ny + 2) * (nz + 2)
+    flux_ms = prof["k_flux_x"][0] / max(1, prof["k_flux_x"][1])
+    flux_gbs = 16 * 9 * nfaces / (flux_ms / 1e3) / 1e9 if flux_ms > 0 else None
+    tflops = FLUX_FP64_PER_FACE * nfaces / (flux_ms / 1e3) / 1e12 if flux_ms > 0 else None
+    return {"kernel": "k_flux_x", "bound": "hbm", "achieved": flux_gbs, "peak": hbm_peak, "unit": "GB/s",
+            "frac": (flux_gbs / hbm_peak) if flux_gbs else None,
+            "traffic": FLUX_X_TRAFFIC_BYTES_192 * nfaces / FLUX_X_FACES_192,
+            "traffic_source": "ncu dram bytes of one launch on 192x96x64, scaled by faces",
+            "peak_source": peak_src, "algorithmic_bytes_per_launch": 16 * 9 * nfaces,
+            "fp64": {"achieved_tflops": tflops, "peak_tflops": fp64_peak,
+                     "frac": (tflops / fp64_peak) if (tflops and fp64_peak) else None,
+                     "flop_per_face": FLUX_FP64_PER_FACE,
+                     "note": "the kernel is FP64-bound: 16.8 FLOP per algorithmic byte"}}
+
+
+def fp64_peak_tflops(k):
+    peak = ctypes.c_double()
+    k._check(k.lib().kgpu_fp64_peak(ctypes.byref(peak)), "kgpu_fp64_peak")
+    return peak.value / 1e12
 RAD_UNIT = "solves/s"
 
 
@@ -366,6 +398,11 @@ def our_arm(args, wl, rank, world, local_rank):
     nfaces = (nx + 1) * (ny + 2 if ny > 1 else 1) * (nz + 2 if nz > 1 else 1)
     flux_ms = prof["k_flux_x"][0] / max(1, prof["k_flux_x"][1])
     flux_gbs = 16 * nv * nfaces / (flux_ms / 1e3) / 1e9 if flux_ms > 0 else None
+    roof = (flux_roofline(prof, nx, ny, nz, hbm_peak, peak_src, fp64_peak_tflops(koral_b200))
+            if args.workload == "torus" else
+            {"kernel": "k_flux_x", "bound": "hbm", "achieved": flux_gbs, "peak": hbm_peak, "unit": "GB/s",
+             "frac": (flux_gbs / hbm_peak) if flux_gbs else None, "traffic": None, "peak_source": peak_src,
+             "algorithmic_bytes_per_launch": 16 * nv * nfaces})
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -373,9 +410,7 @@ def our_arm(args, wl, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": wl["desc"], "cells_per_gpu": cells, "l2": "flushed (256 MB write) before every step",
                    "parallelism": "replicas" if world > 1 else "single subdomain", "graph": "one CUDA graph per RK2 step"},
-        "roofline": {"kernel": "k_flux_x", "bound": "hbm", "achieved": flux_gbs, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": (flux_gbs / hbm_peak) if flux_gbs else None, "traffic": None,
-                     "peak_source": peak_src, "algorithmic_bytes_per_launch": 16 * nv * nfaces},
+        "roofline": roof,
         "kernels": {k: {"ms_per_launch": v[0] / max(1, v[1]), "share": v[0] / total if total else 0.}
                     for k, v in prof.items() if v[1]},
         "top_kernel": top[0],
@@ -551,9 +586,6 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    nfaces = (nx + 1) * (ny + 2) * (nz + 2)
-    flux_ms = prof["k_flux_x"][0] / max(1, prof["k_flux_x"][1])
-    flux_gbs = 16 * 9 * nfaces / (flux_ms / 1e3) / 1e9 if flux_ms > 0 else None
     it_main = c_main["imp_iters"] / max(1, c_main["imp_solves"])
     it_b = c_b["imp_iters"] / max(1, c_b["imp_solves"])
     line = {
@@ -571,9 +603,7 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
                                "end_state_l1_vs_learned": l1(u_main, u_b)},
         "plain": {"value": cells * kp * world / (ms_p / 1e3), "unit": UNIT, "ms_per_step": ms_p / kp,
                   "steps": kp, "newton": newton(c_p)},
-        "roofline": {"kernel": "k_flux_x", "bound": "hbm", "achieved": flux_gbs, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": (flux_gbs / hbm_peak) if flux_gbs else None, "traffic": None,
-                     "peak_source": peak_src, "algorithmic_bytes_per_launch": 16 * 9 * nfaces},
+        "roofline": flux_roofline(prof, nx, ny, nz, hbm_peak, peak_src, fp64_peak_tflops(k)),
         "kernels": {kk: {"ms_per_launch": v[0] / max(1, v[1]), "share": v[0] / total if total else 0.}
                     for kk, v in prof.items() if v[1]},
         "top_kernel": top[0],

@@ -15,7 +15,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libkoral_b200.so")
+LIB_PATH = os.environ.get("KORAL_B200_LIB") or os.path.join(HERE, "_lib", "libkoral_b200.so")
 
 PPM, MP5 = 2, 4
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECT, BC_PERIODIC_COPY = 0, 1, 2, 3
