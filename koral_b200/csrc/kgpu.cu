@@ -400,8 +400,22 @@ __global__ void k_wavespeeds(Grid G, Box b) {
 // floors and evaluates its own state; the pair then swaps fluxes and
 // conserved values with shuffles and each lane stores every other variable.
 // Per face the arithmetic is exactly that of the one-thread form.
+// blocks per SM the face-flux, update and first inversion kernels are
+// compiled for (registers per thread = 65536 / (128 x this)); they are
+// FP64-latency bound, so occupancy is traded against spills (measured: the
+// flux kernel at 8 blocks, 64 registers with spills, is 12% faster than at
+// 4 blocks, 128 registers)
+#ifndef KGPU_FLUX_MIN_BLOCKS
+#define KGPU_FLUX_MIN_BLOCKS 8
+#endif
+#ifndef KGPU_UPDATE_MIN_BLOCKS
+#define KGPU_UPDATE_MIN_BLOCKS 4
+#endif
+#ifndef KGPU_U2P_MIN_BLOCKS
+#define KGPU_U2P_MIN_BLOCKS 5
+#endif
 template <int D>
-__global__ void __launch_bounds__(128, 4) k_flux(Grid G, Box b) {
+__global__ void __launch_bounds__(128, KGPU_FLUX_MIN_BLOCKS) k_flux(Grid G, Box b) {
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const int side = (int)(t & 1);
   int ix, iy, iz;
@@ -619,7 +633,8 @@ __global__ void k_emf(Grid G, Box b) {
 // unsplit update with metric source terms (finite.c:1062-1160,
 // f_metric_source_term_arb physics.c:324-465)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 4) k_update(Grid G, Box b, const double *dtp, double fac, double *save) {
+__global__ void __launch_bounds__(128, KGPU_UPDATE_MIN_BLOCKS) k_update(Grid G, Box b, const double *dtp, double fac,
+                                                                        double *save) {
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
   constexpr int nv = NVMAX;
@@ -902,7 +917,7 @@ __device__ inline int u2p_run(const Grid &G, int Etype, U2PCell &x, int stop, do
   return u2p_final(G.gamma, st, W, iter, x.uc, x.pp, x.g);
 }
 
-__global__ void __launch_bounds__(128, 3) k_u2p(Grid G, Box b, U2PQueues Q, int stop) {
+__global__ void __launch_bounds__(128, KGPU_U2P_MIN_BLOCKS) k_u2p(Grid G, Box b, U2PQueues Q, int stop) {
   int ix, iy, iz;
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (!box_coord(b, t, ix, iy, iz)) return;

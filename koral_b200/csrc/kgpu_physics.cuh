@@ -741,8 +741,12 @@ KG_HD int u2p(const Grid &G, const double *uu0, double *pp, const Geom &g, int &
 KG_HD int check_floors_mhd(const Grid &G, double *pp, const Geom &g, double rhofloor_bh = -1.) {
   int ret = 0;
   const bool magn = kMagn;
-  double uu[NVMAX];
-  p2u_full(G, pp, uu, g);
+  // the reference converts the incoming primitives first (u2p.c:505); the
+  // conserved state is only read by the magnetic floor, so it is computed
+  // there, from a copy of the incoming primitives
+  double pin[NVMAX];
+#pragma unroll
+  for (int iv = 0; iv < NVMAX; iv++) pin[iv] = pp[iv];
   if (pp[0] < G.rhofloor) {
     pp[0] = G.rhofloor;
     ret = -1;
@@ -782,6 +786,8 @@ KG_HD int check_floors_mhd(const Grid &G, double *pp, const Geom &g, double rhof
       dpp[VY] = etacon[2] - etacon[0] * g.GG[0][2] / g.GG[0][0];
       dpp[VZ] = etacon[3] - etacon[0] * g.GG[0][3] / g.GG[0][0];
       p2u_full(G, dpp, duu, g);
+      double uu[NVMAX];
+      p2u_full(G, pin, uu, g);
       for (int iv = 0; iv < NVMAX; iv++) uu[iv] += duu[iv];
       int rt = u2p_solver_W(G, uu, pp, g, 0);
       if (rt < 0) u2p_solver_W(G, uu, pp, g, 1);
