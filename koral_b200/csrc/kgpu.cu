@@ -463,9 +463,10 @@ __global__ void __launch_bounds__(128, KGPU_FLUX_MIN_BLOCKS) k_flux(Grid G, Box 
   const double rfl = G.rhofl_c ? (D == 0 ? G.rhofl_f[ix + G.ng] : G.rhofl_c[ix + G.ng]) : -1.;
   double fs[NVMAX], us[NVMAX];
   {
-    check_floors_mhd(G, ps, g, rfl);
     Kin k;
-    kinematics(ps, g, kMagn, k);
+    bool kv;
+    check_floors_mhd(G, ps, g, rfl, &k, &kv);
+    if (!kv) kinematics(ps, g, kMagn, k);
     flux_prime(G, ps, D, g, k, fs);
     p2u_mhd(G, ps, us, g, k);
   }
@@ -803,8 +804,11 @@ __device__ inline void count_lanes(unsigned long long *ctr, bool pred) {
 // Floors, conserved from primitives and the stores that end a cell's
 // inversion (calc_primitives u2p.c:82-127).
 __device__ inline void u2p_finish(const Grid &G, long c, int ix, double *pp, double *uu, const Geom &g, int fix) {
-  check_floors_mhd(G, pp, g, G.rhofl_c ? G.rhofl_c[ix + G.ng] : -1.);
-  p2u_full(G, pp, uu, g);
+  Kin k;
+  bool kv;
+  check_floors_mhd(G, pp, g, G.rhofl_c ? G.rhofl_c[ix + G.ng] : -1., &k, &kv);
+  if (!kv) kinematics(pp, g, kMagn, k);
+  p2u_mhd(G, pp, uu, g, k);
   store_cell(G.p, G.ncell, c, pp);
   store_cell(G.u, G.ncell, c, uu);
   G.flag[c] = fix;

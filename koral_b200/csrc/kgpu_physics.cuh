@@ -738,8 +738,15 @@ KG_HD int u2p(const Grid &G, const double *uu0, double *pp, const Geom &g, int &
 
 // density, internal-energy, magnetisation and Lorentz-factor floors
 // (check_floors_mhd, u2p.c:492-695, B2RHOFLOORFRAME = ZAMO)
-KG_HD int check_floors_mhd(const Grid &G, double *pp, const Geom &g, double rhofloor_bh = -1.) {
+// kout (optional): the four-velocity and magnetic four-vector the floor
+// computes for the magnetic test; *kvalid tells whether they still hold for
+// the returned primitives (neither the magnetic floor nor the Lorentz-factor
+// ceiling changed velocities or field; the density and energy floors do
+// not enter them), so a caller can skip computing them again.
+KG_HD int check_floors_mhd(const Grid &G, double *pp, const Geom &g, double rhofloor_bh = -1., Kin *kout = nullptr,
+                           bool *kvalid = nullptr) {
   int ret = 0;
+  if (kvalid) *kvalid = false;
   const bool magn = kMagn;
   // the reference converts the incoming primitives first (u2p.c:505); the
   // conserved state is only read by the magnetic floor, so it is computed
@@ -770,8 +777,21 @@ KG_HD int check_floors_mhd(const Grid &G, double *pp, const Geom &g, double rhof
     lower(ucond, ucovd, g.gg);
     bcon_4vel(pp, ucond, ucovd, bcond);
     lower(bcond, bcovd, g.gg);
-    double magpre = dot4(bcond, bcovd) / 2.;
+    const double bsq = dot4(bcond, bcovd);
+    double magpre = bsq / 2.;
+    if (kout) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        kout->ucon[i] = ucond[i];
+        kout->ucov[i] = ucovd[i];
+        kout->bcon[i] = bcond[i];
+        kout->bcov[i] = bcovd[i];
+      }
+      kout->bsq = bsq;
+      if (kvalid) *kvalid = true;
+    }
     if (magpre > G.b2rhoratiomax * pp[RHO]) {
+      if (kvalid) *kvalid = false;
       // normal observer as a relative velocity (relele.c:569-575, 282-307)
       double alp = 1. / sqrt(-g.GG[0][0]);
       double ncov[4] = {-alp, 0., 0., 0.}, etacon[4];
@@ -806,6 +826,7 @@ KG_HD int check_floors_mhd(const Grid &G, double *pp, const Geom &g, double rhof
       double A = sqrt(qsqmax / qsq);
       for (int j = 1; j < 4; j++) pp[1 + j] *= A;
       ret = -1;
+      if (kvalid) *kvalid = false;
     }
   }
   if (ret < 0) pp[5] = calc_Sfromu(G.gamma, pp[0], pp[1]);
