@@ -37,6 +37,7 @@ extern "C" {
 #define KGPU_ECUDA (-2)       /* a CUDA runtime call failed                   */
 #define KGPU_ENOMEM (-3)      /* device allocation failed                     */
 #define KGPU_ESTATE (-4)      /* call out of order (e.g. no metric uploaded)  */
+#define KGPU_EIO (-5)         /* a restart file could not be read or written  */
 
 /* reconstruction / Riemann solver / time integrator choices
  * (INT_ORDER, FLUXMETHOD, TIMESTEPPING; choices.h:150-160, mnemonics.h:117-124) */
@@ -116,6 +117,18 @@ int kgpu_set_minkowski_metric(kgpu_ctx *ctx);
 int kgpu_upload_state(kgpu_ctx *ctx, const double *u, const double *p);
 int kgpu_download_state(kgpu_ctx *ctx, double *u, double *p);
 int kgpu_download_array(kgpu_ctx *ctx, int which, double *out);
+
+/* Restart files in the reference's serial format (fprint_restartfile_bin /
+ * fread_restartfile_bin, fileop.c:910-1111): folder/resNNNN.head holds
+ * "## nout1 nout2 t PROBLEM NX NY NZ", folder/resNNNN.dat the global indices
+ * of the domain cells (x outer, z inner, three ints each) followed by their
+ * primitives in the same order; reslast.* are made links to the newest.
+ * Reading (nout1 < 0: reslast) puts the primitives into the domain cells and
+ * recomputes their conserved variables (p2u), leaving the ghosts to set_bc;
+ * it returns the time, the next file number and nout2.  A file of another
+ * grid size is rejected. */
+int kgpu_write_restart(kgpu_ctx *ctx, const char *folder, int nout1, int nout2, double t, int problem);
+int kgpu_read_restart(kgpu_ctx *ctx, const char *folder, int nout1, double *t, int *nout1_next, int *nout2);
 
 /* Grid operators of KORAL's time loop. ------------------------------------ */
 /* op_explicit(t,dt), finite.c:646-1234 (set_bc, wavespeeds, reconstruction,

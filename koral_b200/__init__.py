@@ -116,6 +116,9 @@ def lib():
             "kgpu_fm_torus_floor": [ctypes.POINTER(TorusParams), ctypes.c_int, ctypes.c_int, _dp, _dp, _dp],
             "kgpu_init_fm_torus": [vp, ctypes.POINTER(TorusParams)],
             "kgpu_download_flux": [vp, ctypes.c_int, _dp],
+            "kgpu_write_restart": [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int],
+            "kgpu_read_restart": [vp, ctypes.c_char_p, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int)],
             "kgpu_download_emf": [vp, _dp],
         }
         for name, args in sig.items():
@@ -366,6 +369,19 @@ class Subdomain:
         self._warm = warm
         _check(self.L.kgpu_set_implicit_solver(self.h, int(mode), warm.h if warm is not None else None),
                "kgpu_set_implicit_solver")
+
+    def write_restart(self, folder, nout1, t, nout2=0, problem=0):
+        """res%04d.head/.dat in the reference's format (fprint_restartfile_bin)."""
+        _check(self.L.kgpu_write_restart(self.h, os.fsencode(folder), int(nout1), int(nout2), float(t), int(problem)),
+               "kgpu_write_restart")
+
+    def read_restart(self, folder, nout1=-1):
+        """Reads a restart file (nout1 < 0: reslast); returns (t, next nout1, nout2)."""
+        t = ctypes.c_double()
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _check(self.L.kgpu_read_restart(self.h, os.fsencode(folder), int(nout1), ctypes.byref(t), ctypes.byref(a),
+                                        ctypes.byref(b)), "kgpu_read_restart")
+        return t.value, a.value, b.value
 
     def implicit_buffers(self):
         """Device pointers of the last implicit step's buffers: n and a dict of

@@ -21,6 +21,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #include <vector>
 
@@ -1710,6 +1711,125 @@ extern "C" int kgpu_download_state(kgpu_ctx *c, double *u, double *p) {
 // operator launchers (all asynchronous on the context stream)
 // ---------------------------------------------------------------------------
 static Box domain_box(const Grid &G) { return Box{0, 0, 0, G.nx, G.ny, G.nz}; }
+
+// ---------------------------------------------------------------------------
+// restart files in the reference's serial binary format (fileop.c:910-1111)
+// ---------------------------------------------------------------------------
+// conserved variables of the domain cells from their primitives (the p2u
+// of fread_restartfile_bin, fileop.c:1078-1092)
+__global__ void k_p2u_domain(Grid G, Box b) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const long c = cell_index(G, ix, iy, iz);
+  double pp[NVR], uu[NVR];
+  load_cell(G.p, G.ncell, c, pp);
+  Geom g;
+  geom_centre(G, ix, iy, iz, g);
+  p2u_full(G, pp, uu, g);
+  store_cell(G.u, G.ncell, c, uu);
+  if (G.rad) {
+    load_rad(G.p, G.ncell, c, pp);
+    p2u_rad(pp, uu, g);
+    store_rad(G.u, G.ncell, c, uu);
+  }
+}
+
+// KORAL's cell-major index of a domain cell in the padded arrays
+static long aos_index(const Grid &G, int ix, int iy, int iz) {
+  long ky = (G.ny > 1 ? iy : 0) + G.ngcy, kz = (G.nz > 1 ? iz : 0) + G.ngcz;
+  return ((long)kz * G.sy + ky) * G.sx + ix + G.ngcx;
+}
+
+extern "C" int kgpu_write_restart(kgpu_ctx *c, const char *folder, int nout1, int nout2, double t, int problem) {
+  if (!c || !folder || nout1 < 0) return KGPU_EINVAL;
+  Grid &G = c->G;
+  std::vector<double> p(G.ncell * G.nv);
+  int r = kgpu_download_array(c, KGPU_ARR_P, p.data());
+  if (r) return r;
+  char name[4096];
+  snprintf(name, sizeof(name), "%s/res%04d.head", folder, nout1);
+  FILE *f = fopen(name, "w");
+  if (!f) return KGPU_EIO;
+  fprintf(f, "## %5d %5d %10.6e %5d %5d %5d %5d\n", nout1, nout2, t, problem, G.nx, G.ny, G.nz);
+  if (fclose(f)) return KGPU_EIO;
+  snprintf(name, sizeof(name), "%s/res%04d.dat", folder, nout1);
+  f = fopen(name, "wb");
+  if (!f) return KGPU_EIO;
+  bool ok = true;
+  // global indices first, x outer and z inner; then the primitives in the
+  // same order
+  for (int ix = 0; ix < G.nx && ok; ix++)
+    for (int iy = 0; iy < G.ny && ok; iy++)
+      for (int iz = 0; iz < G.nz && ok; iz++) {
+        int gi[3] = {ix, iy, iz};
+        ok = fwrite(gi, sizeof(int), 3, f) == 3;
+      }
+  for (int ix = 0; ix < G.nx && ok; ix++)
+    for (int iy = 0; iy < G.ny && ok; iy++)
+      for (int iz = 0; iz < G.nz && ok; iz++)
+        ok = fwrite(p.data() + aos_index(G, ix, iy, iz) * G.nv, sizeof(double), G.nv, f) == (size_t)G.nv;
+  if (fclose(f) || !ok) return KGPU_EIO;
+  // reslast.* point at the newest files, as the reference's links do
+  const char *ext[2] = {"dat", "head"};
+  for (int k = 0; k < 2; k++) {
+    char link[4096], target[64];
+    snprintf(link, sizeof(link), "%s/reslast.%s", folder, ext[k]);
+    snprintf(target, sizeof(target), "res%04d.%s", nout1, ext[k]);
+    unlink(link);
+    if (symlink(target, link)) return KGPU_EIO;
+  }
+  return 0;
+}
+
+extern "C" int kgpu_read_restart(kgpu_ctx *c, const char *folder, int nout1, double *t, int *nout1_next,
+                                 int *nout2) {
+  if (!c || !folder) return KGPU_EINVAL;
+  if (!c->have_grid || !c->have_metric) return KGPU_ESTATE;
+  int r;
+  Grid &G = c->G;
+  char name[4096], head[4096];
+  if (nout1 >= 0) {
+    snprintf(name, sizeof(name), "%s/res%04d.dat", folder, nout1);
+    snprintf(head, sizeof(head), "%s/res%04d.head", folder, nout1);
+  } else {
+    snprintf(name, sizeof(name), "%s/reslast.dat", folder);
+    snprintf(head, sizeof(head), "%s/reslast.head", folder);
+  }
+  FILE *f = fopen(head, "r");
+  if (!f) return KGPU_EIO;
+  int ip[6];
+  double tt = 0.;
+  int nr = fscanf(f, "## %d %d %lf %d %d %d %d\n", &ip[0], &ip[1], &tt, &ip[2], &ip[3], &ip[4], &ip[5]);
+  fclose(f);
+  if (nr != 7) return KGPU_EIO;
+  if (ip[3] != G.nx || ip[4] != G.ny || ip[5] != G.nz) return KGPU_EINVAL;
+  std::vector<double> u(G.ncell * G.nv), p(G.ncell * G.nv);
+  if ((r = kgpu_download_state(c, u.data(), p.data()))) return r;
+  f = fopen(name, "rb");
+  if (!f) return KGPU_EIO;
+  const long n = (long)G.nx * G.ny * G.nz;
+  std::vector<int> idx(3 * n);
+  bool ok = fread(idx.data(), sizeof(int), 3 * n, f) == (size_t)(3 * n);
+  for (long k = 0; k < n && ok; k++) {
+    const int gx = idx[3 * k], gy = idx[3 * k + 1], gz = idx[3 * k + 2];
+    if (gx < 0 || gx >= G.nx || gy < 0 || gy >= G.ny || gz < 0 || gz >= G.nz) {
+      ok = false;
+      break;
+    }
+    ok = fread(p.data() + aos_index(G, gx, gy, gz) * G.nv, sizeof(double), G.nv, f) == (size_t)G.nv;
+  }
+  fclose(f);
+  if (!ok) return KGPU_EIO;
+  if ((r = kgpu_upload_state(c, u.data(), p.data()))) return r;
+  Box db = domain_box(G);
+  k_p2u_domain<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db);
+  CKL("k_p2u_domain");
+  CK(cudaStreamSynchronize(c->stream));
+  if (t) *t = tt;
+  if (nout1_next) *nout1_next = ip[0] + 1;
+  if (nout2) *nout2 = ip[1];
+  return 0;
+}
 
 static int launch_bc(kgpu_ctx *c) {
   Grid &G = c->G;
