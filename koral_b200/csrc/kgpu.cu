@@ -403,11 +403,13 @@ __global__ void k_wavespeeds(Grid G, Box b) {
 // Per face the arithmetic is exactly that of the one-thread form.
 // blocks per SM the face-flux, update and first inversion kernels are
 // compiled for (registers per thread = 65536 / (128 x this)); they are
-// FP64-latency bound, so occupancy is traded against spills (measured: the
-// flux kernel at 8 blocks, 64 registers with spills, is 12% faster than at
-// 4 blocks, 128 registers)
+// FP64-latency bound, so occupancy is traded against spills (measured on the
+// 192x96x64 torus: the flux kernel takes 0.66 ms at 4 blocks, 128 registers
+// without DRAM spill traffic; 0.55 ms at 6 blocks, 80 registers; 0.56 ms at
+// 8 blocks, 64 registers, whose spills then reach DRAM: 1.2 GB written per
+// launch against 0.57 GB at 6 blocks)
 #ifndef KGPU_FLUX_MIN_BLOCKS
-#define KGPU_FLUX_MIN_BLOCKS 8
+#define KGPU_FLUX_MIN_BLOCKS 6
 #endif
 #ifndef KGPU_UPDATE_MIN_BLOCKS
 #define KGPU_UPDATE_MIN_BLOCKS 4
