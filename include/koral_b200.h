@@ -106,6 +106,10 @@ int kgpu_set_uniform_grid(kgpu_ctx *ctx, const double lo[3], const double hi[3])
 int kgpu_upload_metric(kgpu_ctx *ctx, const double *g, const double *G, const double *gKr,
                        const double *gbx, const double *gby, const double *gbz,
                        const double *Gbx, const double *Gby, const double *Gbz);
+/* The context's metric tables back in the same layout (KGPU_ESTATE before
+ * any metric was uploaded or computed). */
+int kgpu_download_metric(kgpu_ctx *ctx, double *g, double *G, double *gKr, double *gbx, double *gby,
+                         double *gbz, double *Gbx, double *Gby, double *Gbz);
 /* Radius-dependent density floor (RHOFLOOR_BH, u2p.c:546-557) tabulated per
  * x-index: at cell centres (SX values, ic in [-NG, NX+NG)) and at x-faces
  * (SX+1 values).  Pass null pointers to switch it off. */
@@ -216,8 +220,15 @@ int kgpu_fm_torus_state(const kgpu_torus_params *tp, const kgpu_config *cfg, con
 /* Density floor table of the torus (host-only), as kgpu_set_density_floor takes it. */
 int kgpu_fm_torus_floor(const kgpu_torus_params *tp, int nx, int ng, const double *xbx, double *centres,
                         double *xfaces);
-/* Whole set-up on a context: grid, metric, floor, state, boundaries, first dt. */
+/* Whole set-up on a context: grid, metric, floor, state, boundaries, first dt.
+ * The metric tables (calc_metric, metric.c:3866-4075) and the torus state
+ * (the problem's init.c with calc_BfromA, magn.c:380-586) are computed by
+ * kernels straight into device memory; only the grid faces and the floor
+ * table cross from the host.  The _host form computes both with the
+ * host-only functions above and uploads them (the same formulas; the
+ * results differ in the last places of sin, cos, tan, exp, log and pow). */
 int kgpu_init_fm_torus(kgpu_ctx *ctx, const kgpu_torus_params *tp);
+int kgpu_init_fm_torus_host(kgpu_ctx *ctx, const kgpu_torus_params *tp);
 
 /* Batched per-cell solvers (host arrays, n cells, one metric point each:
  * g and G hold 20 doubles per cell).  They replace per-cell calls of
@@ -437,12 +448,16 @@ int kgpu_get_implicit_buffers(kgpu_ctx *ctx, int *n, const double **pp_in, const
  * M1 radiation in thermal equilibrium at one temperature (radiation frame
  * comoving with the gas), the atmosphere with a radiation energy of eradatm
  * times its gas energy at rest with it; host-only state, and the whole
- * set-up on a context with radiation switched on (kgpu_set_radiation). */
+ * set-up on a context with radiation switched on (kgpu_set_radiation),
+ * computed on the device (or on the host by the _host form), as
+ * kgpu_init_fm_torus. */
 int kgpu_fm_radtorus_state(const kgpu_torus_params *tp, const kgpu_rad_params *rp, double eradatm,
                            const kgpu_config *cfg, const double *xbx, const double *xby, const double *xbz,
                            const double *g, const double *G, double *u, double *p);
 int kgpu_init_fm_radtorus(kgpu_ctx *ctx, const kgpu_torus_params *tp, const kgpu_rad_params *rp, double eradatm,
                           int wavespeed_limiter);
+int kgpu_init_fm_radtorus_host(kgpu_ctx *ctx, const kgpu_torus_params *tp, const kgpu_rad_params *rp,
+                               double eradatm, int wavespeed_limiter);
 
 /* Last CUDA error string of this thread's most recent failing call. */
 const char *kgpu_last_error(void);

@@ -115,6 +115,8 @@ def lib():
             "kgpu_fm_torus_state": [ctypes.POINTER(TorusParams), ctypes.POINTER(Config)] + [_dp] * 7,
             "kgpu_fm_torus_floor": [ctypes.POINTER(TorusParams), ctypes.c_int, ctypes.c_int, _dp, _dp, _dp],
             "kgpu_init_fm_torus": [vp, ctypes.POINTER(TorusParams)],
+            "kgpu_init_fm_torus_host": [vp, ctypes.POINTER(TorusParams)],
+            "kgpu_download_metric": [vp] + [_dp] * 9,
             "kgpu_download_flux": [vp, ctypes.c_int, _dp],
             "kgpu_write_restart": [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int],
             "kgpu_read_restart": [vp, ctypes.c_char_p, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int),
@@ -166,6 +168,8 @@ def lib():
                                                         ctypes.POINTER(Config)] + [_dp] * 7),
                            ("kgpu_init_fm_radtorus", [vp, ctypes.POINTER(TorusParams), rpp, ctypes.c_double,
                                                       ctypes.c_int]),
+                           ("kgpu_init_fm_radtorus_host", [vp, ctypes.POINTER(TorusParams), rpp, ctypes.c_double,
+                                                           ctypes.c_int]),
                            ("kgpu_get_implicit_buffers", [vp, ctypes.POINTER(ctypes.c_int)] +
                             [ctypes.POINTER(vp)] * 9),
                            ("kgpu_set_radiation", [vp, rpp, ctypes.c_int]),
@@ -264,9 +268,20 @@ class Subdomain:
         a = [np.ascontiguousarray(x, dtype=np.float64) for x in (g, G, gKr, gbx, gby, gbz, Gbx, Gby, Gbz)]
         _check(self.L.kgpu_upload_metric(self.h, *[_ptr(x) for x in a]), "kgpu_upload_metric")
 
-    def init_fm_torus(self, tp=None):
+    def download_metric(self):
+        """The metric tables in KORAL's layout, in the argument order of
+        upload_metric."""
+        out = [np.zeros(n) for n in _metric_sizes(self.cfg)]
+        _check(self.L.kgpu_download_metric(self.h, *[_ptr(o) for o in out]), "kgpu_download_metric")
+        return out
+
+    def init_fm_torus(self, tp=None, on_host=False):
+        """Grid, metric, density floor, torus state, boundaries and first dt.
+        The metric and the state are computed on the device; on_host=True
+        computes them with the host functions and uploads them."""
         tp = tp or torus_params()
-        _check(self.L.kgpu_init_fm_torus(self.h, ctypes.byref(tp)), "kgpu_init_fm_torus")
+        name = "kgpu_init_fm_torus_host" if on_host else "kgpu_init_fm_torus"
+        _check(getattr(self.L, name)(self.h, ctypes.byref(tp)), name)
 
     def init_orszag_tang(self):
         _check(self.L.kgpu_init_orszag_tang(self.h), "kgpu_init_orszag_tang")
@@ -534,24 +549,30 @@ def torus_config(nx=192, ny=96, nz=64):
                           uurhoratiomin=1e-10, uurhoratiomax=1e2, b2rhoratiomax=100.0)
 
 
-def fm_torus(nx=192, ny=96, nz=64, tp=None):
+def fm_torus(nx=192, ny=96, nz=64, tp=None, on_host=False):
     """The benchmark torus on the current GPU, initialised by the product's
-    own metric and Fishbone-Moncrief set-up."""
+    own metric and Fishbone-Moncrief set-up (computed on the device unless
+    on_host)."""
     s = Subdomain(torus_config(nx, ny, nz))
-    s.init_fm_torus(tp)
+    s.init_fm_torus(tp, on_host=on_host)
     return s
 
 
-def mks2_metric_tables(tp, cfg, xb):
-    """Host-side MKS2 metric tables (KORAL layout) for faces xb = (xbx, xby, xbz)."""
+def _metric_sizes(cfg):
+    """Sizes of the nine metric tables (g, G, Christoffels, g and G of the
+    x, y, z faces) in KORAL's layout."""
     sx = cfg.nx + 2 * cfg.ng
     sy = cfg.ny + 2 * cfg.ng if cfg.ny > 1 else 1
     sz = cfg.nz + 2 * cfg.ng if cfg.nz > 1 else 1
     sm = 1 if cfg.axisym_metric else sz
-    shapes = [sx * sy * sm * 20, sx * sy * sm * 20, sx * sy * sm * 64,
-              (sx + 1) * sy * sm * 20, sx * (sy + 1) * sm * 20, sx * sy * (sm + 1) * 20,
-              (sx + 1) * sy * sm * 20, sx * (sy + 1) * sm * 20, sx * sy * (sm + 1) * 20]
-    out = [np.zeros(n) for n in shapes]
+    return [sx * sy * sm * 20, sx * sy * sm * 20, sx * sy * sm * 64,
+            (sx + 1) * sy * sm * 20, sx * (sy + 1) * sm * 20, sx * sy * (sm + 1) * 20,
+            (sx + 1) * sy * sm * 20, sx * (sy + 1) * sm * 20, sx * sy * (sm + 1) * 20]
+
+
+def mks2_metric_tables(tp, cfg, xb):
+    """Host-side MKS2 metric tables (KORAL layout) for faces xb = (xbx, xby, xbz)."""
+    out = [np.zeros(n) for n in _metric_sizes(cfg)]
     xb = [np.ascontiguousarray(x, dtype=np.float64) for x in xb]
     _check(lib().kgpu_mks2_metric_tables(tp.spin, tp.r0, tp.h0, cfg.nx, cfg.ny, cfg.nz, cfg.ng, cfg.axisym_metric,
                                          *[_ptr(x) for x in xb], *[_ptr(o) for o in out]), "kgpu_mks2_metric_tables")
@@ -595,14 +616,17 @@ def radtorus_config(nx=256, ny=128, nz=64):
     return cfg
 
 
-def radtorus(nx=256, ny=128, nz=64, tp=None, rp=None, eradatm=RADTORUS_ERADATM, wavespeed_limiter=False):
-    """A Subdomain holding the radiative torus, radiation switched on."""
+def radtorus(nx=256, ny=128, nz=64, tp=None, rp=None, eradatm=RADTORUS_ERADATM, wavespeed_limiter=False,
+             on_host=False):
+    """A Subdomain holding the radiative torus, radiation switched on; metric
+    and state computed on the device unless on_host."""
     tp = tp or torus_params()
     rp = rp or rad_params(mass=RADTORUS_MASS, gamma=13.0 / 9.0)
     s = Subdomain(radtorus_config(nx, ny, nz))
     s._rp = rp
-    _check(lib().kgpu_init_fm_radtorus(s.h, ctypes.byref(tp), ctypes.byref(rp), float(eradatm),
-                                       int(bool(wavespeed_limiter))), "kgpu_init_fm_radtorus")
+    name = "kgpu_init_fm_radtorus_host" if on_host else "kgpu_init_fm_radtorus"
+    _check(getattr(lib(), name)(s.h, ctypes.byref(tp), ctypes.byref(rp), float(eradatm),
+                                int(bool(wavespeed_limiter))), name)
     return s
 
 

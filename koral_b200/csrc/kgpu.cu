@@ -27,6 +27,7 @@
 
 #include "../../include/koral_b200.h"
 #include "kgpu_rad.cuh"
+#include "kgpu_setup.cuh"
 
 using namespace kgpu;
 
@@ -2536,14 +2537,26 @@ extern "C" int kgpu_num_kernels(void) { return K_NKERNELS; }
 // ---------------------------------------------------------------------------
 // torus set-up on a context
 // ---------------------------------------------------------------------------
-extern "C" int kgpu_init_fm_torus(kgpu_ctx *c, const kgpu_torus_params *tp) {
-  if (!c || !tp) return KGPU_EINVAL;
-  const kgpu_config &k = c->cfg;
-  if (k.nz < 2 || k.ny < 2) return KGPU_EINVAL;
-  int r;
+// grid of the torus: uniform in x1 = ln(r - r0), x2 in [x2_lo, x2_hi], phi
+static int torus_grid(kgpu_ctx *c, const kgpu_torus_params *tp) {
   double lo[3] = {log(tp->r_lo - tp->r0), tp->x2_lo, 0.}, hi[3] = {log(tp->r_hi - tp->r0), tp->x2_hi, 2. * M_PI};
-  if ((r = kgpu_set_uniform_grid(c, lo, hi))) return r;
+  return kgpu_set_uniform_grid(c, lo, hi);
+}
+
+static int torus_floor(kgpu_ctx *c, const kgpu_torus_params *tp) {
+  const Grid &G = c->G;
+  std::vector<double> fc(G.sx), ff(G.sx + 1);
+  int r;
+  if ((r = kgpu_fm_torus_floor(tp, c->cfg.nx, c->cfg.ng, c->hxb[0].data(), fc.data(), ff.data()))) return r;
+  return kgpu_set_density_floor(c, fc.data(), ff.data());
+}
+
+// Host set-up: metric and state computed on the host (the functions the
+// set-up tests compare with the reference) and uploaded.
+static int init_torus_host(kgpu_ctx *c, const kgpu_torus_params *tp, const kgpu_rad_params *rp, double eradatm) {
+  const kgpu_config &k = c->cfg;
   Grid &G = c->G;
+  int r;
   std::vector<double> g(G.nmet * 20), Gi(G.nmet * 20), kr(G.nmet * 64);
   std::vector<double> gb[3], Gb[3];
   for (int d = 0; d < 3; d++) {
@@ -2558,17 +2571,61 @@ extern "C" int kgpu_init_fm_torus(kgpu_ctx *c, const kgpu_torus_params *tp) {
   if ((r = kgpu_upload_metric(c, g.data(), Gi.data(), kr.data(), gb[0].data(), gb[1].data(), gb[2].data(),
                               Gb[0].data(), Gb[1].data(), Gb[2].data())))
     return r;
-  std::vector<double> fc(G.sx), ff(G.sx + 1);
-  if ((r = kgpu_fm_torus_floor(tp, k.nx, k.ng, c->hxb[0].data(), fc.data(), ff.data()))) return r;
-  if ((r = kgpu_set_density_floor(c, fc.data(), ff.data()))) return r;
   std::vector<double> u(G.ncell * G.nv), p(G.ncell * G.nv);
-  if ((r = kgpu_fm_torus_state(tp, &k, c->hxb[0].data(), c->hxb[1].data(), c->hxb[2].data(), g.data(), Gi.data(),
-                               u.data(), p.data())))
+  r = rp ? kgpu_fm_radtorus_state(tp, rp, eradatm, &k, c->hxb[0].data(), c->hxb[1].data(), c->hxb[2].data(),
+                                  g.data(), Gi.data(), u.data(), p.data())
+         : kgpu_fm_torus_state(tp, &k, c->hxb[0].data(), c->hxb[1].data(), c->hxb[2].data(), g.data(), Gi.data(),
+                               u.data(), p.data());
+  if (r) return r;
+  return kgpu_upload_state(c, u.data(), p.data());
+}
+
+// Device set-up: metric tables and state computed by kernels straight into
+// the context's arrays; nothing but the grid faces and the floor table
+// (one value per x index) crosses from the host.
+static int init_torus_device(kgpu_ctx *c, const kgpu_torus_params *tp, const kgpu_rad_params *rp, double eradatm) {
+  Grid &G = c->G;
+  int r = setup_mks2_metric_device(G, tp->spin, tp->r0, tp->h0, c->stream);
+  if (r < 0) {
+    set_err("setup_mks2_metric_device", cudaGetLastError());
     return r;
-  if ((r = kgpu_upload_state(c, u.data(), p.data()))) return r;
+  }
+  c->launches += r;
+  c->have_metric = true;
+  c->metric_gen++;
+  TorusRadConsts rad{0, 0., 0., 0., 0., 0.};
+  if (rp) rad = TorusRadConsts{1, rp->sigma, rp->kb, rp->mu, rp->mp, eradatm};
+  // c->stage holds ncell * nv doubles: A_phi and the field maximum fit
+  r = setup_fm_torus_device(G, *tp, rad, c->stage, c->stream);
+  if (r < 0) {
+    set_err("setup_fm_torus_device", cudaGetLastError());
+    return r;
+  }
+  c->launches += r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+static int init_torus(kgpu_ctx *c, const kgpu_torus_params *tp, const kgpu_rad_params *rp, double eradatm,
+                      int wavespeed_limiter, bool on_device) {
+  if (!c || !tp) return KGPU_EINVAL;
+  const kgpu_config &k = c->cfg;
+  if (k.nz < 2 || k.ny < 2 || k.nv != (rp ? NVR : 9)) return KGPU_EINVAL;
+  int r;
+  if ((r = torus_grid(c, tp))) return r;
+  if ((r = torus_floor(c, tp))) return r;
+  if (rp && (r = kgpu_set_radiation(c, rp, wavespeed_limiter))) return r;
+  if ((r = on_device ? init_torus_device(c, tp, rp, eradatm) : init_torus_host(c, tp, rp, eradatm))) return r;
   if ((r = launch_bc(c))) return r;
   CK(cudaStreamSynchronize(c->stream));
   return kgpu_begin_run(c);
+}
+
+extern "C" int kgpu_init_fm_torus(kgpu_ctx *c, const kgpu_torus_params *tp) {
+  return init_torus(c, tp, nullptr, 0., 0, true);
+}
+extern "C" int kgpu_init_fm_torus_host(kgpu_ctx *c, const kgpu_torus_params *tp) {
+  return init_torus(c, tp, nullptr, 0., 0, false);
 }
 
 // The radiative torus: the same set-up with the torus pressure shared by gas
@@ -2576,39 +2633,44 @@ extern "C" int kgpu_init_fm_torus(kgpu_ctx *c, const kgpu_torus_params *tp) {
 // the atmosphere (eradatm times its gas energy), radiation switched on.
 extern "C" int kgpu_init_fm_radtorus(kgpu_ctx *c, const kgpu_torus_params *tp, const kgpu_rad_params *rp,
                                      double eradatm, int wavespeed_limiter) {
-  if (!c || !tp || !rp) return KGPU_EINVAL;
-  const kgpu_config &k = c->cfg;
-  if (k.nz < 2 || k.ny < 2 || k.nv != NVR) return KGPU_EINVAL;
-  int r;
-  double lo[3] = {log(tp->r_lo - tp->r0), tp->x2_lo, 0.}, hi[3] = {log(tp->r_hi - tp->r0), tp->x2_hi, 2. * M_PI};
-  if ((r = kgpu_set_uniform_grid(c, lo, hi))) return r;
-  Grid &G = c->G;
-  std::vector<double> g(G.nmet * 20), Gi(G.nmet * 20), kr(G.nmet * 64);
-  std::vector<double> gb[3], Gb[3];
-  for (int d = 0; d < 3; d++) {
-    gb[d].resize(G.nfmet[d] * 20);
-    Gb[d].resize(G.nfmet[d] * 20);
-  }
-  if ((r = kgpu_mks2_metric_tables(tp->spin, tp->r0, tp->h0, k.nx, k.ny, k.nz, k.ng, k.axisym_metric,
-                                   c->hxb[0].data(), c->hxb[1].data(), c->hxb[2].data(), g.data(), Gi.data(),
-                                   kr.data(), gb[0].data(), gb[1].data(), gb[2].data(), Gb[0].data(), Gb[1].data(),
-                                   Gb[2].data())))
-    return r;
-  if ((r = kgpu_upload_metric(c, g.data(), Gi.data(), kr.data(), gb[0].data(), gb[1].data(), gb[2].data(),
-                              Gb[0].data(), Gb[1].data(), Gb[2].data())))
-    return r;
-  std::vector<double> fc(G.sx), ff(G.sx + 1);
-  if ((r = kgpu_fm_torus_floor(tp, k.nx, k.ng, c->hxb[0].data(), fc.data(), ff.data()))) return r;
-  if ((r = kgpu_set_density_floor(c, fc.data(), ff.data()))) return r;
-  if ((r = kgpu_set_radiation(c, rp, wavespeed_limiter))) return r;
-  std::vector<double> u(G.ncell * G.nv), p(G.ncell * G.nv);
-  if ((r = kgpu_fm_radtorus_state(tp, rp, eradatm, &k, c->hxb[0].data(), c->hxb[1].data(), c->hxb[2].data(), g.data(),
-                                  Gi.data(), u.data(), p.data())))
-    return r;
-  if ((r = kgpu_upload_state(c, u.data(), p.data()))) return r;
-  if ((r = launch_bc(c))) return r;
+  if (!rp) return KGPU_EINVAL;
+  return init_torus(c, tp, rp, eradatm, wavespeed_limiter, true);
+}
+extern "C" int kgpu_init_fm_radtorus_host(kgpu_ctx *c, const kgpu_torus_params *tp, const kgpu_rad_params *rp,
+                                          double eradatm, int wavespeed_limiter) {
+  if (!rp) return KGPU_EINVAL;
+  return init_torus(c, tp, rp, eradatm, wavespeed_limiter, false);
+}
+
+// Metric tables back in KORAL's layout (the inverse of kgpu_upload_metric).
+static int download_met(kgpu_ctx *c, const double *src, double *g, double *Gi, long npts) {
+  std::vector<double> h(npts * 40);
+  CK(cudaMemcpyAsync(h.data(), src, npts * 40 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  return kgpu_begin_run(c);
+  for (long i = 0; i < npts; i++)
+    for (int k = 0; k < 20; k++) {
+      g[i * 20 + k] = h[k * npts + i];
+      Gi[i * 20 + k] = h[(20 + k) * npts + i];
+    }
+  return 0;
+}
+
+extern "C" int kgpu_download_metric(kgpu_ctx *c, double *g, double *Gi, double *gKr, double *gbx, double *gby,
+                                    double *gbz, double *Gbx, double *Gby, double *Gbz) {
+  if (!c || !g || !Gi || !gKr || !gbx || !gby || !gbz || !Gbx || !Gby || !Gbz) return KGPU_EINVAL;
+  if (!c->have_metric) return KGPU_ESTATE;
+  Grid &G = c->G;
+  int r;
+  if ((r = download_met(c, G.met_c, g, Gi, G.nmet))) return r;
+  double *gb[3] = {gbx, gby, gbz}, *Gb[3] = {Gbx, Gby, Gbz};
+  for (int d = 0; d < 3; d++)
+    if ((r = download_met(c, G.met_f[d], gb[d], Gb[d], G.nfmet[d]))) return r;
+  std::vector<double> h(G.nmet * 64);
+  CK(cudaMemcpyAsync(h.data(), G.gkr, G.nmet * 64 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (long i = 0; i < G.nmet; i++)
+    for (int k = 0; k < 64; k++) gKr[i * 64 + k] = h[k * G.nmet + i];
+  return 0;
 }
 
 // ---------------------------------------------------------------------------
