@@ -459,6 +459,41 @@ int kgpu_init_fm_radtorus(kgpu_ctx *ctx, const kgpu_torus_params *tp, const kgpu
 int kgpu_init_fm_radtorus_host(kgpu_ctx *ctx, const kgpu_torus_params *tp, const kgpu_rad_params *rp,
                                double eradatm, int wavespeed_limiter);
 
+/* ---------------------------------------------------------------------------
+ * Scalar diagnostics of a black-hole disk, computed on the device.  Replaces
+ *   int calc_scalars(ldouble *scalars, ldouble t)          postproc.c:996
+ * for the Kerr tori (MKS2 coordinates written in their own coordinates,
+ * OUTCOORDS = MYCOORDS), entry by entry:
+ *   [0]  total mass (calc_totalmass)            [1] -accretion rate at the
+ *   horizon (calc_mdot, type 0)                 [4] the same in Eddington units
+ *   [3]  magnetic flux through the horizon, [7] MAD parameter, [9] its
+ *        quadrupole form (calc_Bflux: phi-symmetric grids; 0 in 3D as there)
+ *   [5]  MRI resolution Q_theta (calc_resmri; -1 unless bhdisk)
+ *   [6]  rho-weighted temperature at r = 15 (calc_meantemp; -1 unless
+ *        bhdisk and phi-symmetric)
+ *   [8]  scale height: -1 unless bhdisk; 0 with it (CALCHRONTHEGO is not
+ *        configured and r = 15 lies beyond every x1 of these grids)
+ *   [11] local total luminosity (calc_local_lum at the radial index of
+ *        r = 5e3 and theta index 3; R^r_t is 0 without radiation, where the
+ *        reference adds an unset value)
+ *   [2], [10], [12]: 0 (calc_lum leaves [2] and [10] unset on 3D grids and
+ *        its phi-symmetric sum is not built; [12] is never written).
+ * Radius searches, like the reference's for OUTCOORDS = MYCOORDS, compare
+ * the x1 coordinate of cell centres with the radius.  Sums run on the
+ * device in a fixed order: repeated calls give the same bits.
+ * kgpu_calc_scalars copies the result to host memory and waits;
+ * kgpu_calc_scalars_device writes it to device memory on the context's
+ * stream without waiting (it may be captured into a graph after one call
+ * outside capture, which allocates the work arrays). */
+#define KGPU_NSCALARS 13
+typedef struct kgpu_scalars_params {
+  double spin;   /* BHSPIN                                             */
+  double mass;   /* MASS in solar masses: units of the accretion rate  */
+  int bhdisk;    /* BHDISK_PROBLEMTYPE: MRI resolution, mean temperature */
+} kgpu_scalars_params;
+int kgpu_calc_scalars(kgpu_ctx *ctx, const kgpu_scalars_params *sp, double t, double *scalars);
+int kgpu_calc_scalars_device(kgpu_ctx *ctx, const kgpu_scalars_params *sp, double t, double *scalars_dev);
+
 /* Last CUDA error string of this thread's most recent failing call. */
 const char *kgpu_last_error(void);
 int kgpu_abi_version(void);

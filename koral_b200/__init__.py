@@ -34,6 +34,13 @@ class RadParams(ctypes.Structure):
         "eeuuratiomax")]
 
 
+class ScalarsParams(ctypes.Structure):
+    _fields_ = [("spin", ctypes.c_double), ("mass", ctypes.c_double), ("bhdisk", ctypes.c_int)]
+
+
+NSCALARS = 13
+
+
 class KgpuError(RuntimeError):
     pass
 
@@ -117,6 +124,8 @@ def lib():
             "kgpu_init_fm_torus": [vp, ctypes.POINTER(TorusParams)],
             "kgpu_init_fm_torus_host": [vp, ctypes.POINTER(TorusParams)],
             "kgpu_download_metric": [vp] + [_dp] * 9,
+            "kgpu_calc_scalars": [vp, ctypes.POINTER(ScalarsParams), ctypes.c_double, _dp],
+            "kgpu_calc_scalars_device": [vp, ctypes.POINTER(ScalarsParams), ctypes.c_double, vp],
             "kgpu_download_flux": [vp, ctypes.c_int, _dp],
             "kgpu_write_restart": [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int],
             "kgpu_read_restart": [vp, ctypes.c_char_p, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int),
@@ -267,6 +276,14 @@ class Subdomain:
     def upload_metric(self, g, G, gKr, gbx, gby, gbz, Gbx, Gby, Gbz):
         a = [np.ascontiguousarray(x, dtype=np.float64) for x in (g, G, gKr, gbx, gby, gbz, Gbx, Gby, Gbz)]
         _check(self.L.kgpu_upload_metric(self.h, *[_ptr(x) for x in a]), "kgpu_upload_metric")
+
+    def calc_scalars(self, spin=0.9, mass=10.0, bhdisk=False, t=0.):
+        """calc_scalars of the black-hole disk computed on the device
+        (NSCALARS values; the header documents each entry)."""
+        sp = ScalarsParams(float(spin), float(mass), int(bool(bhdisk)))
+        out = np.zeros(NSCALARS)
+        _check(self.L.kgpu_calc_scalars(self.h, ctypes.byref(sp), float(t), _ptr(out)), "kgpu_calc_scalars")
+        return out
 
     def download_metric(self):
         """The metric tables in KORAL's layout, in the argument order of

@@ -28,6 +28,7 @@
 #include "../../include/koral_b200.h"
 #include "kgpu_rad.cuh"
 #include "kgpu_setup.cuh"
+#include "kgpu_diag.cuh"
 
 using namespace kgpu;
 
@@ -1324,6 +1325,7 @@ struct kgpu_ctx {
   kgpu_mlp *warm = nullptr;      // warm-start network, or none
   int warm_gate = -1;            // warm-start only cells whose previous solve took more than this (-1: all)
   long long metric_gen = 0, packed_gen = -1;
+  double *diag_work = nullptr, *diag_out = nullptr;   // calc_scalars on the device
 };
 
 static cudaEvent_t pool_event(kgpu_ctx *c) {
@@ -2640,6 +2642,94 @@ extern "C" int kgpu_init_fm_radtorus_host(kgpu_ctx *c, const kgpu_torus_params *
                                           double eradatm, int wavespeed_limiter) {
   if (!rp) return KGPU_EINVAL;
   return init_torus(c, tp, rp, eradatm, wavespeed_limiter, false);
+}
+
+// ---------------------------------------------------------------------------
+// scalar diagnostics (calc_scalars, postproc.c:996-1105) on the device
+// ---------------------------------------------------------------------------
+// ISCO radius of a Kerr hole in Boyer-Lindquist r (Bardeen, Press and
+// Teukolsky 1972, eq. 2.21), in the operation order of r_ISCO_BL
+// (metric.c:3838-3844)
+static double isco_bl(double ac) {
+  double Z1 = 1. + pow(1. - ac * ac, 1. / 3.) * (pow(1. + ac, 1. / 3.) + pow(1. - ac, 1. / 3.));
+  double Z2 = pow(3. * ac * ac + Z1 * Z1, 1. / 2.);
+  return (3. + Z2 - pow((3. - Z1) * (3. + Z1 + 2. * Z2), 1. / 2.));
+}
+
+// first centre whose x1 exceeds the radius (the loops of calc_mdot,
+// calc_Bflux, calc_resmri, calc_meantemp, calc_scalars), NX when none does
+static int radial_index(const kgpu_ctx *c, double radius) {
+  const int nx = c->cfg.nx, ng = c->cfg.ng;
+  const std::vector<double> &xb = c->hxb[0];
+  int ix;
+  for (ix = 0; ix < nx; ix++)
+    if (.5 * (xb[ix + ng] + xb[ix + 1 + ng]) > radius) break;
+  return ix;
+}
+
+static int diag_prepare(kgpu_ctx *c, const kgpu_scalars_params *sp, DiagIdx &I, DiagConsts &K) {
+  if (!c || !sp) return KGPU_EINVAL;
+  if (!c->have_grid || !c->have_metric) return KGPU_ESTATE;
+  if (!(sp->mass > 0.) || !(fabs(sp->spin) < 1.)) return KGPU_EINVAL;
+  if (c->cfg.ny < 4) return KGPU_EINVAL;   // the local luminosity reads theta index 3
+  if (!c->diag_work) {
+    void *p;
+    int r;
+    if ((r = dalloc(c, &p, DIAG_WORK * sizeof(double)))) return r;
+    c->diag_work = (double *)p;
+    if ((r = dalloc(c, &p, NSCALARS * sizeof(double)))) return r;
+    c->diag_out = (double *)p;
+  }
+  const double rhorizon = 1. + sqrt(1 - sp->spin * sp->spin);   // r_horizon_BL, metric.c:3831-3834
+  const int nx = c->cfg.nx, ng = c->cfg.ng;
+  const double x1last = .5 * (c->hxb[0][nx - 1 + ng] + c->hxb[0][nx + ng]);
+  I.ix_mdot = radial_index(c, rhorizon);
+  I.ix_mri = radial_index(c, x1last / 2.);
+  I.ix_temp = radial_index(c, 15.);
+  I.ix_lum = radial_index(c, 5.e3);
+  // units (ko.h:4-26, choices.h:340): G, c, the mass in cm
+  const double GGG = (6.674e-8 / (1.)), CCC = (2.998e10 / (1.)), MASSCM = (sp->mass * 147700.);
+  const double rho1 = (1. / GGG * CCC * CCC / MASSCM / MASSCM), vel1 = (1. * CCC), len1 = (1. * MASSCM);
+  K.mdotscale = rho1 * vel1 * len1 * len1;
+  const double etaNT = 1. - sqrt(1. - 2. / 3. / isco_bl(sp->spin));   // metric.c:4069
+  K.mdotedd = 1.09649 * 2.23e18 * sp->mass * (0.057 / etaNT);          // calc_mdotEdd, postproc.c:2151-2162
+  kgpu_rad_params rp;
+  int r = kgpu_rad_default_params(&rp, sp->mass, c->cfg.gamma, 6.4e22, 0.34);
+  if (r) return r;
+  K.kb = rp.kb;
+  K.mu = rp.mu;
+  K.mp = rp.mp;
+  K.bhdisk = sp->bhdisk ? 1 : 0;
+  K.rad = c->G.rad ? 1 : 0;
+  return 0;
+}
+
+extern "C" int kgpu_calc_scalars_device(kgpu_ctx *c, const kgpu_scalars_params *sp, double t, double *scalars_dev) {
+  (void)t;   // the scalars of this problem class do not depend on the time
+  DiagIdx I;
+  DiagConsts K;
+  int r = diag_prepare(c, sp, I, K);
+  if (r) return r;
+  if (!scalars_dev) return KGPU_EINVAL;
+  r = diag_scalars_enqueue(c->G, I, K, c->diag_work, scalars_dev, c->stream);
+  if (r < 0) return r;
+  c->launches += r;
+  return 0;
+}
+
+extern "C" int kgpu_calc_scalars(kgpu_ctx *c, const kgpu_scalars_params *sp, double t, double *scalars) {
+  (void)t;
+  if (!scalars) return KGPU_EINVAL;
+  DiagIdx I;
+  DiagConsts K;
+  int r = diag_prepare(c, sp, I, K);
+  if (r) return r;
+  r = diag_scalars_enqueue(c->G, I, K, c->diag_work, c->diag_out, c->stream);
+  if (r < 0) return r;
+  c->launches += r;
+  CK(cudaMemcpyAsync(scalars, c->diag_out, NSCALARS * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
 }
 
 // Metric tables back in KORAL's layout (the inverse of kgpu_upload_metric).
