@@ -65,9 +65,9 @@ RAD_METRIC = "implicit solves/s (1 B200)"
 # From the ncu capture of the x-face flux kernel on the 192x96x64 torus
 # (profiles/k_flux_x_torus_192x96x64.md): DRAM bytes per launch and FP64
 # operations per face (DADD + DMUL + 2 DFMA thread instructions / faces).
-FLUX_X_TRAFFIC_BYTES_192 = 698.94e6
+FLUX_X_TRAFFIC_BYTES_192 = 971.19e6
 FLUX_X_FACES_192 = 193 * 98 * 66
-FLUX_FP64_PER_FACE = 1890.7
+FLUX_FP64_PER_FACE = 1895.5
 
 
 def flux_roofline(prof, nx, ny, nz, hbm_peak, peak_src, fp64_peak):
@@ -87,7 +87,7 @@ def flux_roofline(prof, nx, ny, nz, hbm_peak, peak_src, fp64_peak):
                      "frac": (tflops / fp64_peak) if (tflops and fp64_peak) else None,
                      "flop_per_face": FLUX_FP64_PER_FACE,
                      "note": "the kernel is FP64-latency bound: 13.1 FLOP per algorithmic byte; the DRAM "
-                             "traffic above the algorithmic bytes is register spill of its 80-register build"}}
+                             "traffic above the algorithmic bytes is register spill of its 72-register build"}}
 
 
 def fp64_peak_tflops(k):

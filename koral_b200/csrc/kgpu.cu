@@ -406,12 +406,12 @@ __global__ void k_wavespeeds(Grid G, Box b) {
 // blocks per SM the face-flux, update and first inversion kernels are
 // compiled for (registers per thread = 65536 / (128 x this)); they are
 // FP64-latency bound, so occupancy is traded against spills (measured on the
-// 192x96x64 torus: the flux kernel takes 0.66 ms at 4 blocks, 128 registers
-// without DRAM spill traffic; 0.55 ms at 6 blocks, 80 registers; 0.56 ms at
-// 8 blocks, 64 registers, whose spills then reach DRAM: 1.2 GB written per
-// launch against 0.57 GB at 6 blocks)
+// 192x96x64 torus, x faces: 0.66 ms at 4 blocks, 128 registers without DRAM
+// spill traffic; 0.558 ms at 5 blocks, 96 registers; 0.538 ms at 6, 80
+// registers; 0.525 ms at 7, 72 registers; 0.56 ms at 8 blocks, 64
+// registers, whose spills then reach DRAM: 1.2 GB written per launch)
 #ifndef KGPU_FLUX_MIN_BLOCKS
-#define KGPU_FLUX_MIN_BLOCKS 6
+#define KGPU_FLUX_MIN_BLOCKS 7
 #endif
 #ifndef KGPU_UPDATE_MIN_BLOCKS
 #define KGPU_UPDATE_MIN_BLOCKS 4
