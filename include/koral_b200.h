@@ -389,6 +389,12 @@ int kgpu_rad_set_pass_iters(int k);
  * time (default 64; 0: never).  Results do not depend on it.  Process-wide;
  * a context's captured step keeps the value it was captured with. */
 int kgpu_rad_set_inner_cap(int cap);
+/* Tuning of the batched form: once the cells left after a pass fit in one
+ * wave of warps, each is run to its end by a whole warp that evaluates the
+ * base and the Jacobian columns of every Newton iteration together (default
+ * on; 0: the passes carry on one lane per cell).  Results and statistics do
+ * not depend on it.  Process-wide, like kgpu_rad_set_inner_cap. */
+int kgpu_rad_set_tail(int on);
 /* Learned warm start: how many attempts of the cascade a warm-started cell
  * runs from the predicted iterate (1..6, default 6) before the reference
  * cascade runs from the reference guess.  Every cell still converges to

@@ -155,6 +155,7 @@ def lib():
         L.kgpu_rad_p2u_cells.argtypes = [ctypes.c_int, rpp] + [_dp] * 4
         L.kgpu_rad_set_pass_iters.argtypes = [ctypes.c_int]
         L.kgpu_rad_set_inner_cap.argtypes = [ctypes.c_int]
+        L.kgpu_rad_set_tail.argtypes = [ctypes.c_int]
         L.kgpu_rad_set_warm_attempts.argtypes = [ctypes.c_int]
         L.kgpu_ks_metric.argtypes = [ctypes.c_double] * 3 + [_dp] * 2
         L.kgpu_ks_metric_batch.argtypes = [ctypes.c_double, ctypes.c_int] + [_dp] * 4

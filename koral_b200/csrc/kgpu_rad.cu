@@ -84,6 +84,7 @@ struct Work {
   unsigned long long *stats;  // [0] Newton iterations, [1] passes, [2] fallbacks of the warm start,
                               // [3] residual evaluations, [4] Newton steps of the nested MHD inversions,
                               // [5] their W-function evaluations, [6] evaluations handed to a warp
+  unsigned *tail_done;        // blocks of the running tail launch that have finished
 };
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -98,6 +99,8 @@ unsigned g_inner_cap = 64;
 // attempts of the cascade a warm-started cell runs from the predicted iterate
 // before the reference cascade from the reference guess
 int g_warm_attempts = IMP_NATTEMPTS;
+// the warp-per-cell tail of the batched form (k_rad_tail) is used
+int g_tail = 1;
 size_t work_layout(int n, int passes, Work *w, char *base) {
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -119,6 +122,7 @@ size_t work_layout(int n, int passes, Work *w, char *base) {
     }
   p = take((size_t)(passes + 2) * 3 * 4); if (w) w->count = (int *)p;
   p = take(8 * sizeof(unsigned long long)); if (w) w->stats = (unsigned long long *)p;
+  p = take(sizeof(unsigned)); if (w) w->tail_done = (unsigned *)p;
   const int slots = slow_slots(n);
   p = take((size_t)slots * 4); if (w) w->qs = (int *)p;
   p = take((size_t)slots * sizeof(ImpState)); if (w) w->ss = (ImpState *)p;
@@ -315,6 +319,86 @@ __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, i
   if (blockIdx.x == 0 && threadIdx.x == 0 && nin > 0) atomicAdd(W.stats + 1, 1ull);
 }
 
+// The tail of the batched form.  Launched after pass p (and its cooperative
+// part): when the cells those left unfinished fit in one wave of warps
+// (at most `limit`), each is taken by a whole warp and run to its end.  At
+// the start of every Newton iteration lanes 0..8 evaluate the base and the
+// four Jacobian columns on both sides together (imp_eval_entry), and the
+// state machine, run by every lane alike, takes those entries instead of
+// evaluating them one after another (ImpCache); damped trials and the final
+// inversion it evaluates itself.  The sequence of operations per cell, and
+// so its results and its statistics, are those of the passes; a cell's
+// latency falls from six evaluations per Newton iteration to about two.
+// The last block to finish empties the queue, so that the passes after
+// this one find no work.
+constexpr int TAIL_WARPS = 4;   // warps per block of 128
+__global__ void __launch_bounds__(128) k_rad_tail(RadParams R, Cell C, Work W, int n, int p, int limit,
+                                                  int warm_attempts) {
+  const int nq = p + 1;
+  const int n0 = W.count[nq * 3 + 0], n1 = W.count[nq * 3 + 1];
+  const int nin = n0 + n1;
+  if (nin == 0 || nin > limit) return;   // the same decision in every block
+  __shared__ ImpEval cache_sh[TAIL_WARPS][IMP_NCACHE];
+  const int par = nq & 1;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  ImpEval *ce = cache_sh[wib];
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nin; q += nwarps) {
+    const int k = q < n0 ? W.q[par][0][q] : W.q[par][1][q - n0];
+    RadGeom rg;
+    rad_geom(C.g + 20L * k, C.G + 20L * k, rg);
+    const double *u0 = C.uu + (long)k * NVR, *p0 = C.pp + (long)k * NVR;
+    const double dt = C.dt[k];
+    ImpState s;
+    s.phase = PH_BASE;
+    s.j = 0;
+    s.sign = -1.;
+    s.xiapp = 1.;
+    s.evals = 0;
+    s.inner[0] = s.inner[1] = 0;
+    s.sw = W.wsw[k];
+    s.att = W.watt[k];
+    s.iter = W.wit[k];
+    s.warm = W.wwarm[k];
+    for (int i = 0; i < NVR; i++) s.pp[i] = W.wpp[(long)k * NVR + i];
+    const int warm0 = s.warm;
+    const double *wg = W.wguess + (long)k * NVR;
+    ImpInner how{nullptr, 0u, false, warm_attempts};
+    int budget = 1 << 30;
+    int r;
+    while (true) {
+      if (s.phase == PH_BASE) {
+        if (lane < IMP_NCACHE) imp_eval_entry(R, u0, p0, dt, rg, s, lane, ce[lane]);
+        __syncwarp();
+      }
+      const ImpCache cache{ce, (1u << IMP_NCACHE) - 1u};
+      r = imp_advance(R, u0, p0, dt, rg, s, budget, wg, &how, &cache);
+      __syncwarp();   // every lane has read the entries before they are replaced
+      if (r != IMP_RUNNING) break;
+    }
+    if (lane == 0) {
+      if (r == IMP_DONE_OK) cell_success(R, C, k, rg, s.pp, s.att, s.iter);
+      else cell_failure(C, k);
+      atomicAdd(W.stats, (unsigned long long)((1 << 30) - budget));
+      if (warm0 && !s.warm) atomicAdd(W.stats + 2, 1ull);
+      atomicAdd(W.stats + 3, (unsigned long long)s.evals);
+      atomicAdd(W.stats + 4, (unsigned long long)s.inner[0]);
+      atomicAdd(W.stats + 5, (unsigned long long)s.inner[1]);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned prev = atomicAdd(W.tail_done, 1u);
+    if (prev == gridDim.x - 1) {   // every block has read the counts: the queue is done
+      W.count[nq * 3 + 0] = 0;
+      W.count[nq * 3 + 1] = 0;
+      *W.tail_done = 0u;
+      atomicAdd(W.stats + 1, 1ull);
+    }
+  }
+}
+
 // The cooperative part of pass p: each cell whose evaluation was handed
 // over is taken by a whole warp, which repeats that evaluation and goes on
 // with the cell for the rest of the pass's budget, every nested MHD
@@ -476,6 +560,11 @@ extern "C" int kgpu_rad_set_inner_cap(int cap) {
   return 0;
 }
 
+extern "C" int kgpu_rad_set_tail(int on) {
+  g_tail = on ? 1 : 0;
+  return 0;
+}
+
 extern "C" int kgpu_rad_set_pass_iters(int k) {
   if (k < 1) return KGPU_EINVAL;
   g_pass_iters = k;
@@ -529,6 +618,7 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
   Work W;
   work_layout(n, passes, &W, base);   // fits: the area is sized for kMaxPasses >= passes
   RCK(cudaMemsetAsync(W.count, 0, (size_t)(passes + 2) * 3 * 4, st));
+  RCK(cudaMemsetAsync(W.tail_done, 0, sizeof(unsigned), st));
   if (acc) W.stats = acc;
   else RCK(cudaMemsetAsync(W.stats, 0, 8 * sizeof(unsigned long long), st));
   const int grid = sm_count() * 8;
@@ -541,6 +631,11 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
     RCK(cudaGetLastError());
     if (g_inner_cap) {
       k_rad_slow<<<grid / 2, 128, 0, st>>>(R, C, W, n, p, Kp, g_warm_attempts);
+      RCK(cudaGetLastError());
+    }
+    if (g_tail && p < passes - 1) {
+      // one wave: two blocks of four warps per SM at this kernel's registers
+      k_rad_tail<<<sm_count() * 2, 128, 0, st>>>(R, C, W, n, p, sm_count() * 8, g_warm_attempts);
       RCK(cudaGetLastError());
     }
   }
@@ -559,7 +654,8 @@ int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, c
                            unsigned long long *acc, long long *launches, int gate) {
   if (launches) {
     RadParams R = to_dev(*rp);
-    *launches = mode == KGPU_RAD_PLAIN ? 1 : 1 + (g_inner_cap ? 2 : 1) * max_passes(R, g_pass_iters);
+    const int np = max_passes(R, g_pass_iters);
+    *launches = mode == KGPU_RAD_PLAIN ? 1 : 1 + (g_inner_cap ? 2 : 1) * np + (g_tail ? np - 1 : 0);
   }
   return rad_solve_device(n, rp, uu, pp, g, G, dt, ypred, pp_out, uu_out, status, attempt, iters, mode, work, stream,
                           nullptr, 0, acc, gate);

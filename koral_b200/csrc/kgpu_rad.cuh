@@ -634,6 +634,75 @@ KG_HD int imp_next_attempt(const double *pp00, const double *warm_guess, ImpStat
   return IMP_RUNNING;
 }
 
+// Evaluations done ahead of the state machine: the base evaluation of a
+// Newton iteration and its four Jacobian columns on either side depend only
+// on the iterate at the start of the iteration, so other lanes of a warp can
+// compute them together from the same inputs (imp_input) with the same code
+// (imp_eval_entry).  imp_advance then takes the entry for its phase, column
+// and side instead of evaluating, and counts it as the evaluation it
+// replaces; entries the sequence does not reach are dropped.
+struct ImpEval {
+  double pin[NVR];   // the input after the evaluation (the other component inverted into it)
+  double f[4];
+  double err;
+  int u2pret, corr, fret;
+  unsigned inner[2];
+};
+constexpr int IMP_NCACHE = 9;   // [0] base, [1+j] column j at sign -1, [5+j] column j at sign +1
+struct ImpCache {
+  const ImpEval *e;
+  unsigned valid;   // bit i: entry i present
+};
+
+// The input of an evaluation in phase PH_BASE or PH_JAC (column s.j on side
+// s.sign), as imp_advance forms it.
+KG_HD void imp_input(const RadParams &R, int sh, const ImpState &s, const RadGeom &rg, double *pin) {
+  if (s.phase == PH_BASE) {
+    for (int i = 0; i < NVR; i++) pin[i] = s.pp[i];
+    return;
+  }
+  for (int i = 0; i < NVR; i++) pin[i] = s.ppp[i];
+  const int j = s.j;
+  double del;
+  if (j == 0) {
+    del = s.sign * R.eps * s.ppp[sh];
+  } else {
+    double x = s.ppp[j + sh];
+    double sg = x > 0. ? 1. : (x < 0. ? -1. : (x == 0. ? 1. : 0.));
+    double lim = 1.e-6 / sqrt(rg.g.gg[j][j]);
+    double ax = fabs(x);
+    double veleps = R.eps * sg * (lim > ax ? lim : ax);
+    del = x >= 0. ? s.sign * veleps : -s.sign * veleps;
+  }
+  pin[j + sh] = s.ppp[j + sh] + del;
+}
+
+// Entry `slot` of the iteration that cell state s (in phase PH_BASE) is
+// about to start, evaluated without a cap on the nested inversion.
+KG_HD void imp_eval_entry(const RadParams &R, const double *uu0, const double *pp00, double dt, const RadGeom &rg,
+                          const ImpState &s, int slot, ImpEval &e) {
+  const ImpParams P = imp_attempt(s.att, s.sw);
+  const int sh = P.prim == IMP_MHD ? UU : EE0;
+  ImpState t = s;
+  for (int i = 0; i < NVR; i++) t.ppp[i] = t.pp[i];
+  if (slot == 0) {
+    t.phase = PH_BASE;
+  } else {
+    t.phase = PH_JAC;
+    t.j = (slot - 1) & 3;
+    t.sign = slot < 5 ? -1. : 1.;
+  }
+  imp_input(R, sh, t, rg, e.pin);
+  double uu[NVR];
+  e.inner[0] = e.inner[1] = 0;
+  ImpInner in{e.inner, 0u, false, IMP_NATTEMPTS};
+  e.corr = 0;
+  e.u2pret = imp_prepare(R, P, uu0, e.pin, uu, rg, e.corr, &in);
+  for (int i = 0; i < 4; i++) e.f[i] = 0.;
+  e.err = 0.;
+  e.fret = imp_residual(R, P, e.pin, uu, uu0, pp00, dt, rg, e.u2pret, e.corr, e.f, e.err);
+}
+
 // One evaluation and the transition that follows it.  `budget` counts the
 // Newton iterations the cell may still start in this call sequence; at the
 // start of an iteration with no budget left the cell pauses (IMP_PAUSE)
@@ -642,7 +711,8 @@ KG_HD int imp_next_attempt(const double *pp00, const double *warm_guess, ImpStat
 // inversion runs out the evaluation is abandoned with the state as before
 // the call (IMP_OVER_CAP), to be repeated in the cooperative form.
 KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00, double dt, const RadGeom &rg,
-                      ImpState &s, int &budget, const double *warm_guess = nullptr, const ImpInner *how = nullptr) {
+                      ImpState &s, int &budget, const double *warm_guess = nullptr, const ImpInner *how = nullptr,
+                      const ImpCache *cache = nullptr) {
   const ImpParams P = imp_attempt(s.att, s.sw);
   const int sh = P.prim == IMP_MHD ? UU : EE0;
   const double CONV = P.eq == IMP_ENTROPY ? R.entrconv : R.conv;
@@ -653,22 +723,9 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
     budget--;
     s.iter++;
     for (int i = 0; i < NVR; i++) s.ppp[i] = s.pp[i];
-    for (int i = 0; i < NVR; i++) pin[i] = s.pp[i];
+    imp_input(R, sh, s, rg, pin);
   } else if (s.phase == PH_JAC) {
-    for (int i = 0; i < NVR; i++) pin[i] = s.ppp[i];
-    const int j = s.j;
-    double del;
-    if (j == 0) {
-      del = s.sign * R.eps * s.ppp[sh];
-    } else {
-      double x = s.ppp[j + sh];
-      double sg = x > 0. ? 1. : (x < 0. ? -1. : (x == 0. ? 1. : 0.));
-      double lim = 1.e-6 / sqrt(rg.g.gg[j][j]);
-      double ax = fabs(x);
-      double veleps = R.eps * sg * (lim > ax ? lim : ax);
-      del = x >= 0. ? s.sign * veleps : -s.sign * veleps;
-    }
-    pin[j + sh] = s.ppp[j + sh] + del;
+    imp_input(R, sh, s, rg, pin);
   } else if (s.phase == PH_DAMP) {
     double xxx[4];
     for (int i = 0; i < 4; i++) xxx[i] = s.ppp[i + sh];
@@ -681,21 +738,37 @@ KG_HD int imp_advance(const RadParams &R, const double *uu0, const double *pp00,
     for (int i = 0; i < NVR; i++) pin[i] = s.pp[i];
   }
   // the evaluation: other component's inversion, residual where needed
-  ImpInner in{s.inner, how ? how->cap : 0u, how ? how->warp : false, IMP_NATTEMPTS};
   const int wa = how ? how->warm_attempts : IMP_NATTEMPTS;
-  int corr = 0;
-  int u2pret = imp_prepare(R, P, uu0, pin, uu, rg, corr, &in);
-  if (u2pret == U2P_OVER_CAP) {
-    if (s.phase == PH_BASE) {   // undo the start of the iteration
-      budget++;
-      s.iter--;
+  int slot = -1;
+  if (cache && s.phase == PH_BASE) slot = 0;
+  else if (cache && s.phase == PH_JAC) slot = (s.sign < 0. ? 1 : 5) + s.j;
+  if (slot >= 0 && !((cache->valid >> slot) & 1u)) slot = -1;
+  int corr = 0, u2pret, fret = 0;
+  if (slot >= 0) {   // evaluated ahead from the same input
+    const ImpEval &e = cache->e[slot];
+    for (int i = 0; i < NVR; i++) pin[i] = e.pin[i];
+    for (int i = 0; i < 4; i++) f[i] = e.f[i];
+    err = e.err;
+    u2pret = e.u2pret;
+    corr = e.corr;
+    fret = e.fret;
+    s.inner[0] += e.inner[0];
+    s.inner[1] += e.inner[1];
+    s.evals++;
+  } else {
+    ImpInner in{s.inner, how ? how->cap : 0u, how ? how->warp : false, IMP_NATTEMPTS};
+    u2pret = imp_prepare(R, P, uu0, pin, uu, rg, corr, &in);
+    if (u2pret == U2P_OVER_CAP) {
+      if (s.phase == PH_BASE) {   // undo the start of the iteration
+        budget++;
+        s.iter--;
+      }
+      return IMP_OVER_CAP;
     }
-    return IMP_OVER_CAP;
+    s.evals++;
+    if (s.phase == PH_BASE || s.phase == PH_JAC)
+      fret = imp_residual(R, P, pin, uu, uu0, pp00, dt, rg, u2pret, corr, f, err);
   }
-  s.evals++;
-  int fret = 0;
-  if (s.phase == PH_BASE || s.phase == PH_JAC)
-    fret = imp_residual(R, P, pin, uu, uu0, pp00, dt, rg, u2pret, corr, f, err);
   // transition
   if (s.phase == PH_BASE) {
     if (fret < 0) return imp_next_attempt(pp00, warm_guess, s, wa);

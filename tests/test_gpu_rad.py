@@ -111,14 +111,19 @@ def test_rad_implicit_matches_reference(kgpu, ref, cells):
 def test_rad_batched_equals_plain(kgpu, cells):
     """The work-queue form resumes each Newton solve exactly where it paused:
     its results are those of the one-thread-per-cell form, bit for bit, for
-    any number of iterations per pass."""
+    any number of iterations per pass, with the warp-per-cell tail (the
+    base and Jacobian evaluations of an iteration done by lanes together)
+    and without it."""
     rp, uu, pp, g, G, dt = cells
     a = kgpu.rad_implicit_cells(rp, uu, pp, g, G, dt, mode=kgpu.RAD_PLAIN)
     try:
-        for k in (1, 3, 8):
-            assert kgpu.lib().kgpu_rad_set_pass_iters(k) == 0
-            b = kgpu.rad_implicit_cells(rp, uu, pp, g, G, dt, mode=kgpu.RAD_BATCHED)
-            for x, y in zip(a, b):
-                assert np.array_equal(x, y), k
+        for tail in (1, 0):
+            assert kgpu.lib().kgpu_rad_set_tail(tail) == 0
+            for k in (1, 3, 8):
+                assert kgpu.lib().kgpu_rad_set_pass_iters(k) == 0
+                b = kgpu.rad_implicit_cells(rp, uu, pp, g, G, dt, mode=kgpu.RAD_BATCHED)
+                for x, y in zip(a, b):
+                    assert np.array_equal(x, y), (tail, k)
     finally:
         kgpu.lib().kgpu_rad_set_pass_iters(8)
+        kgpu.lib().kgpu_rad_set_tail(1)
