@@ -13,6 +13,13 @@ inversions with fixups and boundary conditions) of the workload.  Workloads:
           density floor 1e-4 r^-1.5, MP5 + HLL + flux-CT, RK2, CFL 0.5
   ot128   relativistic Orszag-Tang vortex, 128x128, PPM + LLF + flux-CT,
           Minkowski, Gamma = 5/3, CFL 0.5 (the reference's CPU-runnable case)
+  radcells  2^22 independent radiating cells: a step is one batched implicit
+          gas-radiation source solve (metric "implicit solves/s"); the line
+          adds the one-thread-per-cell form and the learned warm start
+  radtorus  the torus on 256x128x64 with M1 radiation: a step is one RK2IMEX
+          step (implicit source solve in every substep, batched solver with
+          the learned warm start, one CUDA graph per step); the line adds the
+          same steps without the network and with one thread per cell
 
 value  = cells x timed steps / device time (CUDA events on the library's own
          stream, L2 flushed between steps, inputs resident in HBM)
@@ -23,6 +30,10 @@ N > 1  : one process per GPU (torchrun), each rank runs its own replica of the
          time is the maximum over ranks, value counts the cells of all ranks.
 --impl reference times the reference KORAL sources themselves (oracle/_ref,
 OpenMP build) on the host cores, same workload and metric.
+The line also carries the roofline of the dominant kernel (HBM, and FP64
+for the face flux), the per-kernel shares, the clocks sampled during the
+timed region and the set-up time of the workload (metric and initial state
+computed on the device).
 """
 import argparse
 import ctypes
