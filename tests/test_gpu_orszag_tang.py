@@ -5,8 +5,8 @@ Tolerance: every conserved and primitive variable except the entropy
 contraction and keep the reference's operation order.  The entropy is
 rho*log(p^n/rho^(n+1)) (physics.c:899-917); CUDA's log/pow may differ from
 the host C library in the last place, so it is held to 1e-12 relative.
-The north-star bar (<=1e-12 relative per substep, <=1e-9 in L1 after 100
-steps) is implied by these.
+The parity bar of the path (<=1e-12 relative per substep, <=1e-9 in L1
+after 100 steps) is implied by these.
 """
 import os
 
@@ -80,7 +80,7 @@ def test_free_run_128_matches_oracle(kgpu, oracle, graph):
             d = dom(a, 3, 128)
             assert np.array_equal(d.min(axis=(0, 1))[NON_ENTR], gold[f"{nm}_min_{target}"][NON_ENTR])
             assert np.array_equal(d.max(axis=(0, 1))[NON_ENTR], gold[f"{nm}_max_{target}"][NON_ENTR])
-    # L1 difference after 100 steps (north-star bar 1e-9), all variables
+    # L1 difference after 100 steps (bar 1e-9), all variables
     l1 = np.abs(dom(u, 3, 128) - dom(G.array("u"), 3, 128)).mean(axis=(0, 1)) / \
         np.abs(dom(G.array("u"), 3, 128)).mean(axis=(0, 1)).clip(1e-300)
     assert l1.max() <= 1e-9
