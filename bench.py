@@ -108,6 +108,21 @@ def fp64_peak_tflops(k):
 RAD_UNIT = "solves/s"
 
 
+def max_over_ranks(x, dist, device):
+    """The largest value of x over all ranks (x itself on a single rank);
+    every rank takes part and receives the result."""
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, steps, world, ms_slowest):
+    """Units of all ranks per second, over the slowest rank's time."""
+    return units_per_rank * steps * world / (ms_slowest / 1e3)
+
+
 def make_subdomain(kgpu, name):
     """The workload's subdomain; its set-up time (context allocation, grid,
     metric tables and initial state computed on the device, boundaries,
@@ -366,11 +381,8 @@ def our_arm(args, wl, rank, world, local_rank):
         ms = timed_steps(args.steps)
     launches = s.launches - launches0
     torch.cuda.synchronize(dev)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = cells * args.steps * world / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, dist, dev)
+    value = whole_job_rate(cells, args.steps, world, ms_max)
 
     # per-kernel device times (events around each launch, separate pass)
     timed_steps(min(args.steps, 50), profile=True)
@@ -402,10 +414,7 @@ def our_arm(args, wl, rank, world, local_rank):
     with torch.cuda.stream(ext):
         e1.record(ext)
     torch.cuda.synchronize(dev)
-    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = cells * ke * world / (float(t.item()) / 1e3)
+    e2e_value = whole_job_rate(cells, ke, world, max_over_ranks(e0.elapsed_time(e1), dist, dev))
     state_bytes = 2 * int(np.prod(shape)) * 8
 
     if rank != 0:
@@ -505,10 +514,7 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
             dist.barrier()
 
     def dmax(ms):
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(ms, dist, dev)
 
     def timed_steps(kk, graph=True, profile=False):
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(kk)]
@@ -753,10 +759,7 @@ def our_arm_radcells(args, wl, rank, world, local_rank):
             b.record(stream)
         torch.cuda.synchronize(dev)
         ms = sum(a.elapsed_time(b) for a, b in ev)
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(ms, dist, dev)
 
     for _ in range(args.warmup):
         solve(k.RAD_BATCHED)
@@ -801,10 +804,7 @@ def our_arm_radcells(args, wl, rank, world, local_rank):
                                            ctypes.cast(hit.data_ptr(), ip), k.RAD_BATCHED), "kgpu_rad_implicit_cells")
     torch.cuda.synchronize(dev)
     e2e_s = time.perf_counter() - t0
-    t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = n * ke * world / float(t.item())
+    e2e_value = whole_job_rate(n, ke, world, 1e3 * max_over_ranks(e2e_s, dist, dev))
     if rank != 0:
         return
     ok = st == 0
