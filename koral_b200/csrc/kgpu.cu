@@ -1157,8 +1157,6 @@ __global__ void k_fixup(Grid G, Box b, int *fixmark) {
   int nb[6][3] = {{ix - 1, iy, iz}, {ix + 1, iy, iz}, {ix, iy - 1, iz}, {ix, iy + 1, iz}, {ix, iy, iz - 1}, {ix, iy, iz + 1}};
   bool inr[6] = {ix - 1 >= 0, ix + 1 < NX, iy - 1 >= 0, iy + 1 < NY, iz - 1 >= 0, iz + 1 < NZ};
   bool before[6] = {true, false, true, false, true, false};
-  double acc[NVMAX];
-  for (int iv = 0; iv < nv; iv++) acc[iv] = 0.;
   int in = 0;
   long nbc[6];
   for (int k = 0; k < 6; k++) {
