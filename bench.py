@@ -54,16 +54,18 @@ WORKLOADS = {
     "torus": dict(desc="3D magnetised Kerr torus 192x96x64 (a=0.9 MKS2, FM torus r_in=6 r_max=12, Gamma 13/9, "
                        "beta_min 100, 2% noise, MP5+HLL+flux-CT, RK2, CFL 0.5)",
                   shape=(192, 96, 64), ref_lib="libkref_fmtorus_omp.so", ref_serial="libkref_fmtorus.so",
-                  ref_sample_steps=4),
+                  ref_sample_steps=4, ref_max_steps=20, ref_max_warmup=5),
     "ot128": dict(desc="relativistic Orszag-Tang vortex 128x128 (Minkowski, PPM+LLF+flux-CT, RK2, CFL 0.5, Gamma 5/3)",
                   shape=(128, 128, 1), ref_lib="libkref_orszagrel_128_omp.so", ref_serial="libkref_orszagrel_128.so",
-                  ref_sample_steps=40),
+                  ref_sample_steps=40, ref_max_steps=100, ref_max_warmup=10),
     "radtorus": dict(desc="3D magnetised radiative Kerr torus 256x128x64 (the torus above plus M1 radiation in LTE "
                           "with the gas at one temperature, Kramers + electron scattering, M = 1e16 Msun, faint "
                           "atmosphere radiation 1e-6 u; MP5+HLL+flux-CT, RK2IMEX with the implicit source solve "
                           "every substep, batched solver + learned warm start, one CUDA graph per step, CFL 0.5)",
                      shape=(256, 128, 64), ref_lib="libkref_radtorus_omp.so", ref_serial="libkref_radtorus_omp.so",
-                     ref_sample_steps=1, radiation=True),
+                     ref_sample_lib="libkref_radtorus_wedge_omp.so", ref_sample_desc="a 256x128x8 phi wedge of the "
+                     "torus (its first 8 of 64 phi columns, same cells, periodic in phi)",
+                     ref_max_steps=40, ref_max_warmup=5, radiation=True),
     "radcells": dict(desc="batched implicit gas-radiation source solve, 2^22 independent cells (Kerr-Schild a=0.9, "
                           "r log-U[2,100] M, theta U[0.1,pi-0.1], log-U rho [1e-8,1], T [1e4,1e12] K, "
                           "E_rad/rho [1e-10,1e2], tau [1e-3,1e5], gas Lorentz factor [1,20], flux fraction [0,0.99], "
@@ -152,7 +154,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="torus", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="radtorus", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -295,6 +297,16 @@ def reference_arm_radcells(args, wl, threads):
     print(json.dumps(line))
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def reference_arm(args, wl, rank):
     if rank != 0:
         return
@@ -302,20 +314,29 @@ def reference_arm(args, wl, rank):
     if "ncells" in wl:
         reference_arm_radcells(args, wl, threads)
         return
-    # one full RK2 step of the reference on all host cores per step, at most
-    # ref_sample_steps of them (a full-size CPU step takes seconds)
-    nsteps = max(1, min(args.steps, wl["ref_sample_steps"]))
-    val, err = run_reference_cpu(wl, nsteps, min(max(0, args.warmup), 1), threads)
+    # The reference's own time steps on all host cores, from its own initial
+    # state: the same W warm-up steps as the GPU arm (capped where a CPU step
+    # takes long), then the timed steps, at most ref_max_steps of them;
+    # "steps" and "warmup" report what was run.  The radiative torus runs on
+    # a phi wedge (its first 8 of 64 phi columns, periodic in phi): a bounded
+    # sample of the same cells at the same resolution.
+    nsteps = max(1, min(args.steps, wl["ref_max_steps"]))
+    warm = max(0, min(args.warmup, wl["ref_max_warmup"]))
+    lib = wl.get("ref_sample_lib", wl["ref_lib"])
+    val, err = run_reference_cpu(dict(wl, ref_lib=lib), nsteps, warm, threads)
     if val is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
         return
+    sample = wl.get("ref_sample_desc", "the whole grid")
     line = {
         "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": cells_of(wl) / val * 1e3,
+        "steps": nsteps, "warmup": warm, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": cells_of(wl) / val * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wl["desc"], "parallelism": "openmp host threads"},
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"{nsteps} full RK2 steps after {min(max(0, args.warmup), 1)} warm-up step(s)"},
+        "config": {"workload": wl["desc"], "parallelism": "openmp host threads", "sample": sample},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "reference", "cpu": cpu_model(),
+                         "sample": f"{nsteps} time steps of {sample} after {warm} warm-up step(s), "
+                                   f"reference sources built with gcc -O3 -fopenmp"},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -481,7 +502,56 @@ def warmstart_network(k):
     return None, None
 
 
+# attempts of the cascade a warm-started torus cell runs from the prediction
+# before the reference cascade (the torus's solves start close to the
+# previous state: past the first two attempts a failed warm start is better
+# served by the reference cascade; measured 236 against 365 ms per implicit
+# step with all six)
 WARM_ATTEMPTS_RADTORUS = 2
+# the implicit solver of the timed radiative-torus steps
+MAIN_SOLVER = "batched"
+# FP64 work of one residual evaluation of the implicit solve on the torus's
+# own cells, nested MHD inversion included: DADD + DMUL + 2 DFMA thread
+# instructions of the one-thread-per-cell solver over its counted
+# evaluations (ncu capture, profiles/k_rad_radtorus_256x128x64.md)
+IMP_FP64_PER_EVAL = None
+
+CPU_REF_CHILD = r"""
+import json, sys, time
+import numpy as np
+sys.path.insert(0, {root!r})
+from oracle.koral_oracle import RefKoral
+R = RefKoral({lib!r}); R.init()
+st = np.load({state!r})
+u, p = R.array("u"), R.array("p")
+u[...] = st["u"][:u.shape[0]]
+p[...] = st["p"][:p.shape[0]]
+R.set_scalar("tstepdenmax", float(st["tsd"]))
+t0 = time.perf_counter(); R.step({steps}); t1 = time.perf_counter()
+print(json.dumps({{"seconds": t1 - t0, "cells": R.nx * R.ny * R.nz, "steps": {steps}}}))
+"""
+
+
+def cpu_baseline_from_state(wl, u, p, tsd, steps, threads):
+    """The reference's own time steps on the host cores, started from the
+    GPU run's state (its first phi columns, for the wedge build): a bounded
+    sample of the same steps the GPU timed."""
+    import tempfile
+    import numpy as np
+    lib = wl.get("ref_sample_lib", wl["ref_lib"])
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", lib)):
+        return None, f"{lib} not built (needs the reference tree at build time)"
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "state.npz")
+        np.savez(path, u=u, p=p, tsd=tsd)
+        code = CPU_REF_CHILD.format(root=ROOT, lib=lib, state=path, steps=steps)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=1800)
+    line = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    if r.returncode != 0 or not line:
+        return None, (r.stderr or r.stdout)[-300:]
+    d = json.loads(line[-1])
+    return d["cells"] * d["steps"] / d["seconds"], None
 
 
 def our_arm_radtorus(args, wl, rank, world, local_rank):
@@ -495,11 +565,10 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
     build.build()
     s = make_subdomain(k, args.workload)
     mlp, mlp_name = warmstart_network(k)
-    # the torus's own solves are close to the previous state: past the first
-    # two attempts a failed warm start is better served by the reference
-    # cascade than by further attempts from the prediction (measured: 236 ms
-    # per implicit step against 365 ms with all six)
-    k.lib().kgpu_rad_set_warm_attempts(WARM_ATTEMPTS_RADTORUS)
+    s.set_implicit_options(warm_attempts=WARM_ATTEMPTS_RADTORUS)
+    main_mode = {"persistent": k.RAD_PERSISTENT, "batched": k.RAD_BATCHED}[MAIN_SOLVER]
+    other_mode, other_name = ((k.RAD_BATCHED, "batched") if main_mode == k.RAD_PERSISTENT
+                              else (k.RAD_PERSISTENT, "persistent"))
     ext = torch.cuda.ExternalStream(s.stream, device=dev)
     nx, ny, nz = wl["shape"]
     cells = nx * ny * nz
@@ -534,13 +603,16 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
             s.profile(False)
         return sum(a.elapsed_time(b) for a, b in zip(starts, ends))
 
+    def restart():
+        s.upload_state(u_start.copy(), p_start.copy())
+        s.tstepdenmax = tsd_start
+        s.reset_counters()
+
     def leg(mode, warm, kk):
         """kk steps from the saved state with the given solver; device ms,
         solver statistics and the end state"""
         s.set_implicit_solver(mode, warm)
-        s.upload_state(u_start.copy(), p_start.copy())
-        s.tstepdenmax = tsd_start
-        s.reset_counters()
+        restart()
         barrier()
         ms = dmax(timed_steps(kk))
         c = s.counters()
@@ -552,36 +624,40 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
                 "mean_evaluations_per_solve": c["imp_evals"] / max(1, c["imp_solves"]),
                 "mean_nested_inversion_iterations_per_solve": c["imp_inner"] / max(1, c["imp_solves"]),
                 "failed_solves": int(c["radimp_failed"]), "fallbacks": int(c["imp_fallbacks"]),
+                "evaluations_handed_to_a_warp": int(c["imp_cooperative"]),
                 "radiation_corrections": int(c["rad_corrected"])}
 
-    # warm-up from the initial torus, then the timed run from the state reached
-    s.set_implicit_solver(k.RAD_BATCHED, mlp)
+    # warm-up from the initial torus (graph capture included), then every leg
+    # times the same K steps from the state reached
+    s.set_implicit_solver(main_mode, mlp)
     s.rk2imex_steps(max(1, args.warmup), graph=True)
     u_start, p_start = s.download_state()
     tsd_start = s.tstepdenmax
     launches0 = s.launches
     with ClockSampler(local_rank) as clk:
-        ms, c_main, u_main = leg(k.RAD_BATCHED, mlp, args.steps)
+        ms, c_main, u_main = leg(main_mode, mlp, args.steps)
     launches = s.launches - launches0
     value = cells * args.steps * world / (ms / 1e3)
-    # the same steps from the same state without the network and with the
-    # one-thread-per-cell solver (the cost per step falls by several times
-    # over the first tens of steps, so every leg times the same steps)
-    ms_b, c_b, u_b = leg(k.RAD_BATCHED, None, args.steps)
-    kp = args.steps
-    ms_p, c_p, u_p = leg(k.RAD_PLAIN, None, kp)
+    # the same steps without the network, with the other queued solver and
+    # with one thread per cell (the cost per step falls by several times over
+    # the first tens of steps, so every leg times the same steps)
+    ms_n, c_n, u_n = leg(main_mode, None, args.steps)
+    ms_o, c_o, u_o = leg(other_mode, mlp, args.steps)
+    ms_p, c_p, u_p = leg(k.RAD_PLAIN, None, args.steps)
     g = s.cfg.ng
 
     def l1(a, b):
         a, b = a[g:-g, g:-g, g:-g], b[g:-g, g:-g, g:-g]
         return [float(np.abs(a[..., v] - b[..., v]).sum() / (np.abs(b[..., v]).sum() + 1e-300)) for v in range(13)]
 
-    # per-kernel device times (events around each launch, stream replay)
-    s.set_implicit_solver(k.RAD_BATCHED, mlp)
-    s.upload_state(u_start.copy(), p_start.copy())
-    s.tstepdenmax = tsd_start
-    timed_steps(min(args.steps, 3), profile=True)
+    # per-kernel device times (events around each launch, stream replay) and
+    # the solver's counters over the same steps
+    s.set_implicit_solver(main_mode, mlp)
+    restart()
+    kprof = min(args.steps, 5)
+    timed_steps(kprof, profile=True)
     prof = s.profile_read()
+    c_prof = s.counters()
     total = sum(v[0] for v in prof.values())
     top = max(prof.items(), key=lambda kv: kv[1][0])
 
@@ -613,31 +689,39 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
     state_bytes = 2 * int(np.prod(shape)) * 8
     if rank != 0:
         return
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    fp64_peak = fp64_peak_tflops(k)
+    solve_ms = prof["k_imp_solve"][0]
+    roof = {"kernel": "k_imp_solve (" + MAIN_SOLVER + " implicit source solve)", "bound": "fp64",
+            "peak": fp64_peak, "unit": "TFLOP/s", "peak_source": "measured live (DMUL+DADD chains, no FMA)",
+            "traffic": None, "evaluations": int(c_prof["imp_evals"]), "solve_ms": solve_ms,
+            "share_of_step": solve_ms / total if total else None}
+    if IMP_FP64_PER_EVAL and solve_ms > 0:
+        tf = IMP_FP64_PER_EVAL * c_prof["imp_evals"] / (solve_ms / 1e3) / 1e12
+        roof.update(achieved=tf, frac=tf / fp64_peak, flop_per_evaluation=IMP_FP64_PER_EVAL)
+    else:
+        roof.update(achieved=None, frac=None)
     it_main = c_main["imp_iters"] / max(1, c_main["imp_solves"])
-    it_b = c_b["imp_iters"] / max(1, c_b["imp_solves"])
+    it_n = c_n["imp_iters"] / max(1, c_n["imp_solves"])
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": wl["desc"], "cells_per_gpu": cells, "l2": "flushed (256 MB write) before every step",
                    "parallelism": "replicas" if world > 1 else "single subdomain",
-                   "graph": "one CUDA graph per RK2IMEX step", "warm_start_weights": mlp_name,
-                   "warm_attempts": WARM_ATTEMPTS_RADTORUS},
-        "newton": {"learned": newton(c_main), "batched_no_network": newton(c_b),
-                   "iteration_ratio": it_b / it_main if it_main > 0 else None},
-        "batched_no_network": {"value": cells * args.steps * world / (ms_b / 1e3), "unit": UNIT,
-                               "ms_per_step": ms_b / args.steps,
-                               "end_state_l1_vs_learned": l1(u_main, u_b)},
-        "plain": {"value": cells * kp * world / (ms_p / 1e3), "unit": UNIT, "ms_per_step": ms_p / kp,
-                  "steps": kp, "newton": newton(c_p)},
-        "roofline": flux_roofline(prof, nx, ny, nz, hbm_peak, peak_src, fp64_peak_tflops(k)),
+                   "graph": "one CUDA graph per RK2IMEX step", "solver": MAIN_SOLVER,
+                   "warm_start_weights": mlp_name, "warm_attempts": WARM_ATTEMPTS_RADTORUS,
+                   "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps} from the initial torus"},
+        "newton": {"learned": newton(c_main), "no_network": newton(c_n),
+                   "iteration_ratio_no_network_over_learned": it_n / it_main if it_main > 0 else None},
+        "no_network": {"value": cells * args.steps * world / (ms_n / 1e3), "unit": UNIT,
+                       "ms_per_step": ms_n / args.steps, "end_state_l1_vs_learned": l1(u_main, u_n)},
+        other_name: {"value": cells * args.steps * world / (ms_o / 1e3), "unit": UNIT,
+                     "ms_per_step": ms_o / args.steps, "with_network": mlp_name is not None,
+                     "same_state_as_main": bool(np.array_equal(u_o, u_main)), "newton": newton(c_o)},
+        "plain": {"value": cells * args.steps * world / (ms_p / 1e3), "unit": UNIT,
+                  "ms_per_step": ms_p / args.steps, "newton": newton(c_p)},
+        "roofline": roof,
+        "flux_roofline": flux_roofline(prof, nx, ny, nz, *hbm_peak_of(), fp64_peak),
         "kernels": {kk: {"ms_per_launch": v[0] / max(1, v[1]), "share": v[0] / total if total else 0.}
                     for kk, v in prof.items() if v[1]},
         "top_kernel": top[0],
@@ -648,11 +732,27 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
     }
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        val, err = run_reference_cpu(wl, 1, 0, threads)
+        sample = wl.get("ref_sample_desc", "the whole grid")
+        nz_s = 8 + 2 * g
+        us, ps = u_start[:nz_s].copy(), p_start[:nz_s].copy()
+        val, err = cpu_baseline_from_state(wl, us, ps, tsd_start, 2, threads)
+        val1, err1 = cpu_baseline_from_state(wl, us, ps, tsd_start, 1, 1)
         line["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": threads, "kind": "reference",
-                                "sample": ("1 full RK2IMEX step of the same workload from its initial state"
+                                "cpu": cpu_model(), "value_1_thread": val1,
+                                "sample": (f"2 time steps (and 1 on one thread) of {sample}, from the state the "
+                                           f"GPU run reached after {args.warmup} steps: the reference sources "
+                                           f"(gcc -O3 -fopenmp) on the host cores"
                                            if val is not None else f"unavailable: {err}")}
     print(json.dumps(line))
+
+
+def hbm_peak_of():
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    return peaks.get("hbm_gbs", 6650.0), ("measured" if "hbm_gbs" in peaks else "fallback")
 
 
 # ---------------------------------------------------------------------------

@@ -314,8 +314,40 @@ typedef struct {
 int kgpu_rad_default_params(kgpu_rad_params *rp, double mass, double gamma, double kramers, double kes);
 
 /* Solver variants of kgpu_rad_implicit_cells. */
-#define KGPU_RAD_PLAIN 0    /* one thread runs a cell's whole cascade        */
-#define KGPU_RAD_BATCHED 1  /* passes over a work queue of unfinished cells  */
+#define KGPU_RAD_PLAIN 0       /* one thread runs a cell's whole cascade        */
+#define KGPU_RAD_BATCHED 1     /* passes over a work queue of unfinished cells  */
+#define KGPU_RAD_PERSISTENT 2  /* one resident kernel whose lanes take cells    */
+                               /* from a work list as they finish, then a       */
+                               /* warp-per-cell kernel for the cells left over  */
+
+/* Tuning of the batched and persistent forms.  Results and statistics
+ * (Newton iterations, evaluations) do not depend on any field except
+ * warm_attempts, which chooses how long a warm-started cell trusts its
+ * prediction.
+ *  pass_iters     batched: Newton iterations a cell may take per pass (8)
+ *  inner_cap      W-function evaluations the MHD inversion nested in one
+ *                 residual evaluation may take in a single lane before that
+ *                 evaluation is repeated by a whole warp with the damped
+ *                 trials tried 32 at a time (64; 0: never)
+ *  tail           batched: once the cells left after a pass fit in one wave
+ *                 of warps, each is run to its end by a whole warp (1; 0: off)
+ *  warm_attempts  learned warm start: attempts of the cascade a warm-started
+ *                 cell runs from the predicted iterate before the reference
+ *                 cascade runs from the reference guess (1..6, default 6)
+ *  thin           persistent: once the work list is empty, a warp hands the
+ *                 cells it still holds to the warp-per-cell kernel when at
+ *                 most this many of its 32 lanes hold one (0..32, default 8)
+ *  blocks_per_sm  persistent: resident blocks of 128 threads per SM
+ *                 (0: as many as the kernel's registers allow) */
+typedef struct {
+  int pass_iters;
+  int inner_cap;
+  int tail;
+  int warm_attempts;
+  int thin;
+  int blocks_per_sm;
+} kgpu_rad_solver_opts;
+int kgpu_rad_default_solver_opts(kgpu_rad_solver_opts *opts);
 
 /* Batched solve_implicit_lab (rad.c:1225-1570): for each of n cells, the
  * conserved state uu after the explicit update, the primitive guess pp,
@@ -332,8 +364,9 @@ int kgpu_rad_implicit_cells(int n, const kgpu_rad_params *rp, const double *uu, 
 /* The same on device pointers, asynchronously on `stream` (a cudaStream_t,
  * or null for the default stream).  stats, when not null, receives after
  * completion: [0] Newton iterations over all attempts, [1] passes run.
- * Temporary device memory of the batched variant is taken from `work`,
- * which must hold kgpu_rad_work_bytes(n) bytes (null for the plain one). */
+ * Temporary device memory of the batched and persistent variants is taken
+ * from `work`, which must hold kgpu_rad_work_bytes(n) bytes (null for the
+ * plain one). */
 size_t kgpu_rad_work_bytes(int n);
 int kgpu_rad_implicit_cells_device(int n, const kgpu_rad_params *rp, const double *uu, const double *pp,
                                    const double *g, const double *G, const double *dt, double *pp_out,
@@ -351,6 +384,18 @@ int kgpu_rad_implicit_cells_warm_device(int n, const kgpu_rad_params *rp, const 
                                         const double *g, const double *G, const double *dt, const float *ypred,
                                         double *pp_out, double *uu_out, int *status, int *attempt, int *iters,
                                         void *work, void *stream, unsigned long long *stats);
+/* The general device form: any solver variant, an optional prediction
+ * ypred (null: the reference guess; not with KGPU_RAD_PLAIN), the solver
+ * tuning opts (null: the process-wide values), and up to nstats (<= 8)
+ * counters: [0] Newton iterations over all attempts, [1] launches that had
+ * work, [2] warm-start fallbacks, [3] residual evaluations, [4] Newton steps
+ * and [5] W-function evaluations of the nested MHD inversions, [6]
+ * evaluations handed to a whole warp. */
+int kgpu_rad_implicit_cells_device_ex(int n, const kgpu_rad_params *rp, const double *uu, const double *pp,
+                                      const double *g, const double *G, const double *dt, const float *ypred,
+                                      double *pp_out, double *uu_out, int *status, int *attempt, int *iters,
+                                      int mode, const kgpu_rad_solver_opts *opts, void *work, void *stream,
+                                      unsigned long long *stats, int nstats);
 /* Network inputs (float [n][16]) of cells before a solve, and training
  * targets (float [n][5]: ln of the gas and radiation energy ratios, change
  * of the iterated velocity) from the states before and after; NaN where
@@ -380,26 +425,16 @@ int kgpu_mlp_gradient(kgpu_mlp *mlp, const float *X, const float *T, int n, floa
 int kgpu_mlp_train_epoch(kgpu_mlp *mlp, const float *X, const float *T, int n, int batch, float lr,
                          unsigned long long seed, double *mean_loss);
 
-/* Tuning of the batched form: Newton iterations a cell may take per pass
- * (default 8; results do not depend on it).  Process-wide. */
+/* Solver tuning of the context-free entry points (kgpu_rad_implicit_cells*):
+ * process-wide values, one field of kgpu_rad_solver_opts each (see there).
+ * A context does not read them: it holds its own options
+ * (kgpu_set_implicit_options). */
 int kgpu_rad_set_pass_iters(int k);
-/* Tuning of the batched form: W-function evaluations the MHD inversion
- * nested in one residual evaluation may take in a single lane before that
- * evaluation is repeated by a whole warp with the damped trials tried 32 at a
- * time (default 64; 0: never).  Results do not depend on it.  Process-wide;
- * a context's captured step keeps the value it was captured with. */
 int kgpu_rad_set_inner_cap(int cap);
-/* Tuning of the batched form: once the cells left after a pass fit in one
- * wave of warps, each is run to its end by a whole warp that evaluates the
- * base and the Jacobian columns of every Newton iteration together (default
- * on; 0: the passes carry on one lane per cell).  Results and statistics do
- * not depend on it.  Process-wide, like kgpu_rad_set_inner_cap. */
 int kgpu_rad_set_tail(int on);
-/* Learned warm start: how many attempts of the cascade a warm-started cell
- * runs from the predicted iterate (1..6, default 6) before the reference
- * cascade runs from the reference guess.  Every cell still converges to
- * RADIMPCONV or fails as the reference would.  Process-wide. */
 int kgpu_rad_set_warm_attempts(int k);
+int kgpu_rad_set_solver_opts(const kgpu_rad_solver_opts *opts);
+int kgpu_rad_get_solver_opts(kgpu_rad_solver_opts *opts);
 /* M1 closure u2p_rad (u2prad.c:485) and p2u (p2u.c:40) of n cells, host
  * pointers; corrected[i] is u2p_rad's corrected flag. */
 int kgpu_rad_u2p_cells(int n, const kgpu_rad_params *rp, const double *uu, double *pp, const double *g,
@@ -425,10 +460,17 @@ int kgpu_fp64_peak(double *ops_per_s);
  * the RADIMP fixup.  rp->gamma must equal the grid's adiabatic index.
  * Allocates the solver's buffers for the domain cells once. */
 int kgpu_set_radiation(kgpu_ctx *ctx, const kgpu_rad_params *rp, int wavespeed_limiter);
-/* Solver of op_implicit: KGPU_RAD_PLAIN or KGPU_RAD_BATCHED (default), and
- * the warm-start network (batched only; null for the reference's guess).
- * The network is borrowed: it must outlive its use by the context. */
+/* Solver of op_implicit: KGPU_RAD_PLAIN, KGPU_RAD_BATCHED (default) or
+ * KGPU_RAD_PERSISTENT, and the warm-start network (batched and
+ * persistent only; null for the reference's guess).  The network is
+ * borrowed: it must outlive its use by the context. */
 int kgpu_set_implicit_solver(kgpu_ctx *ctx, int mode, kgpu_mlp *warm);
+/* The context's own solver tuning (kgpu_rad_solver_opts; defaults from
+ * kgpu_rad_default_solver_opts at kgpu_set_radiation).  Setting it drops the
+ * context's captured step graph, so the next graph step runs with the new
+ * values. */
+int kgpu_set_implicit_options(kgpu_ctx *ctx, const kgpu_rad_solver_opts *opts);
+int kgpu_get_implicit_options(kgpu_ctx *ctx, kgpu_rad_solver_opts *opts);
 /* With a warm-start network: start from the prediction only the cells whose
  * previous implicit solve in this context needed a later attempt of the
  * cascade or more than `iters` Newton iterations (the others start from the

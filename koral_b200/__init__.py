@@ -34,6 +34,16 @@ class RadParams(ctypes.Structure):
         "eeuuratiomax")]
 
 
+class SolverOpts(ctypes.Structure):
+    """kgpu_rad_solver_opts (include/koral_b200.h): tuning of the batched and
+    persistent implicit solvers."""
+    _fields_ = [(n, ctypes.c_int) for n in ("pass_iters", "inner_cap", "tail", "warm_attempts", "thin",
+                                            "blocks_per_sm")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class ScalarsParams(ctypes.Structure):
     _fields_ = [("spin", ctypes.c_double), ("mass", ctypes.c_double), ("bhdisk", ctypes.c_int)]
 
@@ -162,6 +172,14 @@ def lib():
         L.kgpu_fp64_peak.argtypes = [_dp]
         L.kgpu_rad_implicit_cells_warm_device.argtypes = [ctypes.c_int, rpp] + [vp] * 13 + [
             ctypes.POINTER(ctypes.c_ulonglong)]
+        sop = ctypes.POINTER(SolverOpts)
+        L.kgpu_rad_implicit_cells_device_ex.argtypes = [ctypes.c_int, rpp] + [vp] * 11 + [
+            ctypes.c_int, sop, vp, vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]
+        L.kgpu_rad_default_solver_opts.argtypes = [sop]
+        L.kgpu_rad_set_solver_opts.argtypes = [sop]
+        L.kgpu_rad_get_solver_opts.argtypes = [sop]
+        L.kgpu_set_implicit_options.argtypes = [vp, sop]
+        L.kgpu_get_implicit_options.argtypes = [vp, sop]
         L.kgpu_rad_features_device.argtypes = [ctypes.c_int, rpp] + [vp] * 6
         L.kgpu_rad_targets_device.argtypes = [ctypes.c_int, rpp] + [vp] * 7
         fp = ctypes.POINTER(ctypes.c_float)
@@ -396,8 +414,9 @@ class Subdomain:
                "kgpu_set_radiation")
 
     def set_implicit_solver(self, mode=None, warm=None):
-        """Solver of op_implicit (RAD_PLAIN or RAD_BATCHED) and the warm-start
-        network (an Mlp, kept alive by this object), or None."""
+        """Solver of op_implicit (RAD_PLAIN, RAD_BATCHED or RAD_PERSISTENT)
+        and the warm-start network (an Mlp, kept alive by this object), or
+        None."""
         mode = RAD_BATCHED if mode is None else mode
         self._warm = warm
         _check(self.L.kgpu_set_implicit_solver(self.h, int(mode), warm.h if warm is not None else None),
@@ -442,6 +461,20 @@ class Subdomain:
                                               vp(b["G20"]), vp(b["status"]), _vp(T), _stream()),
                "kgpu_rad_targets_device")
         return X, T
+
+    def implicit_options(self):
+        """This context's solver tuning (a SolverOpts)."""
+        o = SolverOpts()
+        _check(self.L.kgpu_get_implicit_options(self.h, ctypes.byref(o)), "kgpu_get_implicit_options")
+        return o
+
+    def set_implicit_options(self, opts=None, **kw):
+        """Set this context's solver tuning: a SolverOpts, or fields changed
+        by keyword from the current values."""
+        o = self.implicit_options() if opts is None else opts
+        for k, v in kw.items():
+            setattr(o, k, int(v))
+        _check(self.L.kgpu_set_implicit_options(self.h, ctypes.byref(o)), "kgpu_set_implicit_options")
 
     def set_warm_gate(self, iters):
         """Warm-start only cells whose previous solve took a later attempt or
@@ -651,8 +684,17 @@ def radtorus(nx=256, ny=128, nz=64, tp=None, rp=None, eradatm=RADTORUS_ERADATM, 
 # ---------------------------------------------------------------------------
 # radiation: per-cell implicit gas-radiation source solve
 # ---------------------------------------------------------------------------
-RAD_PLAIN, RAD_BATCHED = 0, 1
+RAD_PLAIN, RAD_BATCHED, RAD_PERSISTENT = 0, 1, 2
 NVR = 13
+
+
+def solver_opts(**kw):
+    """kgpu_rad_default_solver_opts with fields changed by keyword."""
+    o = SolverOpts()
+    _check(lib().kgpu_rad_default_solver_opts(ctypes.byref(o)), "kgpu_rad_default_solver_opts")
+    for k, v in kw.items():
+        setattr(o, k, int(v))
+    return o
 
 
 def rad_params(mass=10.0, gamma=13.0 / 9.0, kramers=6.4e22, kes=0.34):
@@ -854,9 +896,13 @@ def rad_targets_device(rp, pp, pp1, g, G, status):
     return T
 
 
-def rad_solve_device(rp, uu, pp, g, G, dt, mode=RAD_BATCHED, ypred=None, work=None):
-    """Batched implicit solve on device tensors; with ypred, the learned warm
-    start.  Returns (pp, uu, status, attempt, iters, stats)."""
+def rad_solve_device(rp, uu, pp, g, G, dt, mode=RAD_BATCHED, ypred=None, work=None, opts=None, nstats=3):
+    """Implicit solve on device tensors (kgpu_rad_implicit_cells_device_ex);
+    with ypred, the learned warm start; opts a SolverOpts or None for the
+    process-wide values.  Returns (pp, uu, status, attempt, iters, stats)
+    with nstats counters (Newton iterations, launches with work, warm-start
+    fallbacks, evaluations, nested Newton steps, nested W evaluations,
+    evaluations handed to a warp)."""
     import torch
     n = uu.shape[0]
     dev = uu.device
@@ -864,17 +910,14 @@ def rad_solve_device(rp, uu, pp, g, G, dt, mode=RAD_BATCHED, ypred=None, work=No
     uo = torch.empty_like(uu)
     st, at, it = (torch.empty(n, dtype=torch.int32, device=dev) for _ in range(3))
     L = lib()
-    if work is None and (mode == RAD_BATCHED or ypred is not None):
+    if work is None and mode != RAD_PLAIN:
         work = torch.empty(int(L.kgpu_rad_work_bytes(n)), dtype=torch.uint8, device=dev)
-    stats = (ctypes.c_ulonglong * 3)()
-    if ypred is None:
-        _check(L.kgpu_rad_implicit_cells_device(n, ctypes.byref(rp), _vp(uu), _vp(pp), _vp(g), _vp(G), _vp(dt),
-                                                _vp(po), _vp(uo), _vp(st), _vp(at), _vp(it), mode, _vp(work),
-                                                _stream(), stats), "kgpu_rad_implicit_cells_device")
-    else:
-        _check(L.kgpu_rad_implicit_cells_warm_device(n, ctypes.byref(rp), _vp(uu), _vp(pp), _vp(g), _vp(G),
-                                                     _vp(dt), _vp(ypred), _vp(po), _vp(uo), _vp(st), _vp(at),
-                                                     _vp(it), _vp(work), _stream(), stats),
-               "kgpu_rad_implicit_cells_warm_device")
+    stats = (ctypes.c_ulonglong * nstats)()
+    _check(L.kgpu_rad_implicit_cells_device_ex(n, ctypes.byref(rp), _vp(uu), _vp(pp), _vp(g), _vp(G), _vp(dt),
+                                               _vp(ypred) if ypred is not None else None, _vp(po), _vp(uo),
+                                               _vp(st), _vp(at), _vp(it), mode,
+                                               ctypes.byref(opts) if opts is not None else None,
+                                               _vp(work) if work is not None else None, _stream(), stats, nstats),
+           "kgpu_rad_implicit_cells_device_ex")
     return po, uo, st, at, it, list(stats)
 

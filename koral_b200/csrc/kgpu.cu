@@ -1277,8 +1277,10 @@ static const char *kKernelNames[K_NKERNELS] = {"k_bc", "k_wavespeeds", "k_flux_x
 int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
                            const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
                            int *status, int *attempt, int *iters, int mode, void *work, void *stream,
-                           unsigned long long *acc, long long *launches, int gate);
+                           unsigned long long *acc, long long *launches, int gate,
+                           const kgpu_rad_solver_opts *opts);
 kgpu::RadParams kgpu_rad_device_params(const kgpu_rad_params &p);
+bool kgpu_rad_opts_valid(const kgpu_rad_solver_opts &o);
 
 struct ProfRec {
   int id;
@@ -1320,6 +1322,7 @@ struct kgpu_ctx {
   void *imp_work = nullptr;
   float *imp_X = nullptr, *imp_Y = nullptr;
   int imp_mode = KGPU_RAD_BATCHED;
+  kgpu_rad_solver_opts imp_opts;  // this context's solver tuning
   kgpu_mlp *warm = nullptr;      // warm-start network, or none
   int warm_gate = -1;            // warm-start only cells whose previous solve took more than this (-1: all)
   long long metric_gen = 0, packed_gen = -1;
@@ -1436,6 +1439,7 @@ extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
     return KGPU_EINVAL;
   kgpu_ctx *c = new kgpu_ctx();
   c->cfg = *cfg;
+  kgpu_rad_default_solver_opts(&c->imp_opts);
   fill_grid_params(c->G, *cfg);
   Grid &G = c->G;
   c->have_grid = c->have_metric = false;
@@ -2139,9 +2143,23 @@ extern "C" int kgpu_set_radiation(kgpu_ctx *c, const kgpu_rad_params *rp, int wa
   return 0;
 }
 
+extern "C" int kgpu_set_implicit_options(kgpu_ctx *c, const kgpu_rad_solver_opts *o) {
+  if (!c || !o) return KGPU_EINVAL;
+  if (!kgpu_rad_opts_valid(*o)) return KGPU_EINVAL;
+  c->imp_opts = *o;
+  drop_graph(c);
+  return 0;
+}
+
+extern "C" int kgpu_get_implicit_options(kgpu_ctx *c, kgpu_rad_solver_opts *o) {
+  if (!c || !o) return KGPU_EINVAL;
+  *o = c->imp_opts;
+  return 0;
+}
+
 extern "C" int kgpu_set_implicit_solver(kgpu_ctx *c, int mode, kgpu_mlp *warm) {
-  if (!c || (mode != KGPU_RAD_PLAIN && mode != KGPU_RAD_BATCHED)) return KGPU_EINVAL;
-  if (warm && mode != KGPU_RAD_BATCHED) return KGPU_EINVAL;   // the warm start runs in the batched solver
+  if (!c || (mode != KGPU_RAD_PLAIN && mode != KGPU_RAD_BATCHED && mode != KGPU_RAD_PERSISTENT)) return KGPU_EINVAL;
+  if (warm && mode == KGPU_RAD_PLAIN) return KGPU_EINVAL;   // the warm start runs in the queued solvers
   if (!c->G.rad) return KGPU_ESTATE;
   if (warm && !c->imp_X) {
     void *p;
@@ -2197,7 +2215,7 @@ static int enqueue_implicit(kgpu_ctx *c, const double *dtp, double fac) {
     long long nl = 0;
     int r = kgpu_rad_solve_enqueue(n, &c->rp, c->imp_uu, c->imp_pp, c->imp_g, c->imp_G, c->imp_dt, ypred, c->imp_ppo,
                                    c->imp_uuo, c->imp_status, c->imp_att, c->imp_it, c->imp_mode, c->imp_work,
-                                   c->stream, G.cnt + C_IMP_ITERS, &nl, c->warm_gate);
+                                   c->stream, G.cnt + C_IMP_ITERS, &nl, c->warm_gate, &c->imp_opts);
     if (r) return r;
     c->launches += nl - 1;
   }

@@ -17,12 +17,17 @@
 //    exits (KGPU_STATIC_MAX_CELLS * 472 bytes, about 3.9 MB).
 //  - The first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (that device current); make that first call before
-//    any stream capture.
+//    any stream capture.  The address is kept per device together with the
+//    identity of the device's CUDA context: after cudaDeviceReset (or any
+//    other teardown and re-creation of the context, which reloads the module
+//    and moves the array) the next call looks the address up again, so
+//    that call, too, belongs before any stream capture.
 //  - All calls share the one array, which keeps the last call's contents.
 //    Every word the kernel reads is written by the same call's copies, so no
 //    clearing is needed; calls that overlap on the GPU (from several host
 //    threads) race on the array and must be serialised by the caller.
 //  - Copies are synchronous on the legacy default stream.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -65,9 +70,40 @@ static __device__ __align__(256) unsigned char kgpu_static_scratch[kScratchBytes
 namespace {
 
 constexpr int kMaxDevices = 64;
-void *g_scratch_addr[kMaxDevices];   // device address per device ordinal, set once
+void *g_scratch_addr[kMaxDevices];            // device address per device ordinal ...
+unsigned long long g_scratch_ctx[kMaxDevices];  // ... and the context it was looked up in
 std::mutex g_setup_mutex;
 thread_local char g_err[200];
+
+// Unique identity of the current context (cuCtxGetId: unique over the
+// process's lifetime, unlike the context handle, which a re-created context
+// may reuse), through the runtime's driver entry points so that the
+// library needs no link to the driver library.
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext *);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long *);
+int current_context_id(unsigned long long *id) {
+  static PfnCtxGetCurrent get_current = nullptr;
+  static PfnCtxGetId get_id = nullptr;
+  if (!get_current || !get_id) {
+    cudaDriverEntryPointQueryResult q1, q2;
+    void *f1 = nullptr, *f2 = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || !f1 ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+        q2 != cudaDriverEntryPointSuccess || !f2) {
+      snprintf(g_err, sizeof(g_err), "driver entry points cuCtxGetCurrent/cuCtxGetId not found");
+      return KGPU_ECUDA;
+    }
+    get_current = (PfnCtxGetCurrent)f1;
+    get_id = (PfnCtxGetId)f2;
+  }
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, id) != CUDA_SUCCESS) {
+    snprintf(g_err, sizeof(g_err), "no current CUDA context");
+    return KGPU_ECUDA;
+  }
+  return 0;
+}
 
 int scratch_for_current_device(unsigned char **out) {
   int dev = -1;
@@ -80,8 +116,17 @@ int scratch_for_current_device(unsigned char **out) {
     snprintf(g_err, sizeof(g_err), "device ordinal %d beyond %d", dev, kMaxDevices);
     return KGPU_EINVAL;
   }
+  // makes the device's primary context current (and creates it on first use)
+  e = cudaSetDevice(dev);
+  if (e != cudaSuccess) {
+    snprintf(g_err, sizeof(g_err), "context set-up: %s", cudaGetErrorString(e));
+    return KGPU_ECUDA;
+  }
+  unsigned long long ctx = 0;
+  int r = current_context_id(&ctx);
+  if (r) return r;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
+  if (!g_scratch_addr[dev] || g_scratch_ctx[dev] != ctx) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, kgpu_static_scratch);
     if (e != cudaSuccess || !p) {
@@ -89,6 +134,7 @@ int scratch_for_current_device(unsigned char **out) {
       return KGPU_ECUDA;
     }
     g_scratch_addr[dev] = p;
+    g_scratch_ctx[dev] = ctx;
   }
   *out = (unsigned char *)g_scratch_addr[dev];
   return 0;

@@ -11,6 +11,13 @@
 //    that finish leave the queue, so warps stay full of live work.  The
 //    iterations a cell takes are the same in both forms (the solve resumes
 //    exactly where it stopped), so both give the same results.
+//  - persistent: one resident kernel (k_rad_persist) whose lanes take cells
+//    from a work list and take the next one as soon as theirs finishes, so
+//    no lane waits for a pass to end; cells whose nested inversion runs
+//    over its cap, and those still running in warps that have thinned out
+//    once the list is empty, are handed with their whole state to a
+//    warp-per-cell kernel (k_rad_finish) that runs them to their end.  Three
+//    launches per solve instead of one per pass; the same bits.
 // Both run the cascade as the one-evaluation state machine of
 // kgpu_rad.cuh (imp_advance), so the lanes of a warp perform their
 // expensive evaluations together whatever phase each cell is in.
@@ -23,6 +30,11 @@
 #include "kgpu_mlp.cuh"
 
 using namespace kgpu;
+
+// resident blocks of 128 threads per SM the solver kernels are compiled for
+#ifndef KGPU_RAD_MIN_BLOCKS
+#define KGPU_RAD_MIN_BLOCKS 1
+#endif
 
 int kgpu_report_cuda(const char *what, cudaError_t e);   // kgpu.cu: records the error for kgpu_last_error
 
@@ -51,7 +63,42 @@ RadParams to_dev(const kgpu_rad_params &p) {
   return R;
 }
 
-int g_pass_iters = 8;   // Newton iterations per cell and pass of the batched form
+// Tuning of the batched and persistent forms (kgpu_rad_solver_opts)
+struct Opts {
+  int pass_iters = 8;       // Newton iterations per cell and pass of the batched form
+  int inner_cap = 64;       // W-function evaluations of a nested inversion in one lane (0: no cap)
+  int tail = 1;             // batched: warp-per-cell tail
+  int warm_attempts = IMP_NATTEMPTS;
+  int thin = 8;             // persistent: hand-off threshold of live lanes once the list is empty
+  int blocks_per_sm = 0;    // persistent: resident blocks per SM (0: occupancy limit)
+};
+Opts g_opts;   // the context-free entry points' values
+
+Opts from_api(const kgpu_rad_solver_opts &o) {
+  Opts r;
+  r.pass_iters = o.pass_iters;
+  r.inner_cap = o.inner_cap;
+  r.tail = o.tail;
+  r.warm_attempts = o.warm_attempts;
+  r.thin = o.thin;
+  r.blocks_per_sm = o.blocks_per_sm;
+  return r;
+}
+kgpu_rad_solver_opts to_api(const Opts &o) {
+  kgpu_rad_solver_opts r;
+  r.pass_iters = o.pass_iters;
+  r.inner_cap = o.inner_cap;
+  r.tail = o.tail;
+  r.warm_attempts = o.warm_attempts;
+  r.thin = o.thin;
+  r.blocks_per_sm = o.blocks_per_sm;
+  return r;
+}
+bool opts_valid(const kgpu_rad_solver_opts &o) {
+  return o.pass_iters >= 1 && o.inner_cap >= 0 && (o.tail == 0 || o.tail == 1) && o.warm_attempts >= 1 &&
+         o.warm_attempts <= IMP_NATTEMPTS && o.thin >= 0 && o.thin <= 32 && o.blocks_per_sm >= 0 &&
+         o.blocks_per_sm <= 16;
+}
 
 // upper bound of the passes a cell can need: six attempts of at most
 // RADIMPMAXITER + 1 iterations each (the queue-length array of the work
@@ -85,6 +132,9 @@ struct Work {
                               // [3] residual evaluations, [4] Newton steps of the nested MHD inversions,
                               // [5] their W-function evaluations, [6] evaluations handed to a warp
   unsigned *tail_done;        // blocks of the running tail launch that have finished
+  unsigned *ctl;              // persistent form: [0] next work-list entry, [1] cells handed over paused
+                              // (listed in q[1][0]), [2] next hand-over taken by k_rad_finish,
+                              // [3] evaluations handed over with their state (qs/ss)
 };
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -92,15 +142,6 @@ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 // finds the queue full carries on alone, without the cap)
 inline int slow_slots(int n) { return n / 8 > 1024 ? n / 8 : 1024; }
 
-// W-function evaluations a nested MHD inversion may take in one lane before
-// the evaluation is handed to a whole warp (a converged inversion typically
-// takes 3-6); 0 turns the cooperative pass off
-unsigned g_inner_cap = 64;
-// attempts of the cascade a warm-started cell runs from the predicted iterate
-// before the reference cascade from the reference guess
-int g_warm_attempts = IMP_NATTEMPTS;
-// the warp-per-cell tail of the batched form (k_rad_tail) is used
-int g_tail = 1;
 size_t work_layout(int n, int passes, Work *w, char *base) {
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -123,6 +164,7 @@ size_t work_layout(int n, int passes, Work *w, char *base) {
   p = take((size_t)(passes + 2) * 3 * 4); if (w) w->count = (int *)p;
   p = take(8 * sizeof(unsigned long long)); if (w) w->stats = (unsigned long long *)p;
   p = take(sizeof(unsigned)); if (w) w->tail_done = (unsigned *)p;
+  p = take(4 * sizeof(unsigned)); if (w) w->ctl = (unsigned *)p;
   const int slots = slow_slots(n);
   p = take((size_t)slots * 4); if (w) w->qs = (int *)p;
   p = take((size_t)slots * sizeof(ImpState)); if (w) w->ss = (ImpState *)p;
@@ -176,7 +218,7 @@ __device__ inline void cell_failure(const Cell &C, int k) {
   C.iters[k] = 0;
 }
 
-__global__ void __launch_bounds__(128) k_rad_plain(RadParams R, Cell C, int n, unsigned long long *stats) {
+__global__ void __launch_bounds__(128, KGPU_RAD_MIN_BLOCKS) k_rad_plain(RadParams R, Cell C, int n, unsigned long long *stats) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   RadGeom rg;
@@ -251,7 +293,7 @@ __device__ inline int warp_slot(int *qcount, bool pred) {
 // Pass p: the cells of queue p may start up to K Newton iterations;
 // unfinished ones keep their state (the iterate, its iteration count, the
 // attempt) and go to queue p+1, by the primitives of their running attempt.
-__global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, int n, int p, int K,
+__global__ void __launch_bounds__(128, KGPU_RAD_MIN_BLOCKS) k_rad_pass(RadParams R, Cell C, Work W, int n, int p, int K,
                                                   unsigned inner_cap, int warm_attempts) {
   const int n0 = W.count[p * 3 + 0], n1 = W.count[p * 3 + 1];
   const int nin = n0 + n1;
@@ -332,7 +374,7 @@ __global__ void __launch_bounds__(128) k_rad_pass(RadParams R, Cell C, Work W, i
 // The last block to finish empties the queue, so that the passes after
 // this one find no work.
 constexpr int TAIL_WARPS = 4;   // warps per block of 128
-__global__ void __launch_bounds__(128) k_rad_tail(RadParams R, Cell C, Work W, int n, int p, int limit,
+__global__ void __launch_bounds__(128, KGPU_RAD_MIN_BLOCKS) k_rad_tail(RadParams R, Cell C, Work W, int n, int p, int limit,
                                                   int warm_attempts) {
   const int nq = p + 1;
   const int n0 = W.count[nq * 3 + 0], n1 = W.count[nq * 3 + 1];
@@ -404,7 +446,7 @@ __global__ void __launch_bounds__(128) k_rad_tail(RadParams R, Cell C, Work W, i
 // with the cell for the rest of the pass's budget, every nested MHD
 // inversion run by the 32 lanes together; the arithmetic is the same, so
 // the cell's results are too.  Unfinished cells join the next pass.
-__global__ void __launch_bounds__(128) k_rad_slow(RadParams R, Cell C, Work W, int n, int p, int K,
+__global__ void __launch_bounds__(128, KGPU_RAD_MIN_BLOCKS) k_rad_slow(RadParams R, Cell C, Work W, int n, int p, int K,
                                                   int warm_attempts) {
   const int ns0 = W.count[p * 3 + 2];
   const int ns = ns0 < W.nslots ? ns0 : W.nslots;
@@ -451,6 +493,203 @@ __global__ void __launch_bounds__(128) k_rad_slow(RadParams R, Cell C, Work W, i
     (void)it0;
     __syncwarp();
   }
+}
+
+// The persistent form.  A lane's cell state at the start of a Newton
+// iteration: what the per-cell work arrays hold (k_rad_start, or a cell
+// paused at an iteration boundary).
+__device__ inline void load_paused(const Work &W, int k, ImpState &s) {
+  s.phase = PH_BASE;
+  s.j = 0;
+  s.sign = -1.;
+  s.xiapp = 1.;
+  s.evals = 0;
+  s.inner[0] = s.inner[1] = 0;
+  s.sw = W.wsw[k];
+  s.att = W.watt[k];
+  s.iter = W.wit[k];
+  s.warm = W.wwarm[k];
+  for (int i = 0; i < NVR; i++) s.pp[i] = W.wpp[(long)k * NVR + i];
+}
+
+// k_rad_persist: as many blocks as are resident at once.  Each lane takes a
+// cell from the work list (the two start queues of k_rad_start, cells whose
+// first attempt iterates radiation primitives first), runs its cascade one
+// evaluation per loop trip (imp_advance) and, when the cell finishes, takes
+// the next entry of the list: a warp stays full until the list is empty.
+// Cells leave the kernel in three ways: finished (outputs written); with
+// an evaluation whose nested inversion ran over its cap (the whole state is
+// handed to k_rad_finish, which repeats that evaluation with the warp's 32
+// lanes); or, once the list is empty and at most `thin` lanes of the warp
+// still hold a cell, paused at the next iteration boundary and handed to
+// k_rad_finish, which runs each such cell with a whole warp.  Every cell
+// performs the same sequence of evaluations as in the one-thread form.
+__global__ void __launch_bounds__(128, KGPU_RAD_MIN_BLOCKS) k_rad_persist(RadParams R, Cell C, Work W, unsigned inner_cap,
+                                                     int warm_attempts, int thin) {
+  const unsigned FULL = 0xffffffffu;
+  const int n0 = W.count[0], n1 = W.count[1];
+  const int nin = n0 + n1;
+  const int lane = threadIdx.x & 31;
+  bool have = false, drained = false;
+  int k = 0, budget = 0, warm0 = 0;
+  double dt = 0.;
+  const double *u0 = C.uu, *p0 = C.pp, *wg = W.wguess;
+  RadGeom rg;
+  ImpState s;
+  ImpInner how{nullptr, inner_cap, false, warm_attempts};
+  unsigned st_it = 0, st_fb = 0, st_ev = 0, st_in0 = 0, st_in1 = 0, st_coop = 0;
+  while (true) {
+    // lanes without a cell take the next entries of the list together
+    const unsigned need = __ballot_sync(FULL, !have && !drained);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      int base = 0;
+      if (lane == leader) base = (int)atomicAdd(W.ctl, (unsigned)__popc(need));
+      base = __shfl_sync(FULL, base, leader);
+      if (base + __popc(need) >= nin) drained = true;   // the same in every lane
+      if ((need >> lane) & 1u) {
+        const int q = base + __popc(need & ((1u << lane) - 1u));
+        if (q < nin) {
+          k = q < n0 ? W.q[0][0][q] : W.q[0][1][q - n0];
+          rad_geom(C.g + 20L * k, C.G + 20L * k, rg);
+          u0 = C.uu + (long)k * NVR;
+          p0 = C.pp + (long)k * NVR;
+          wg = W.wguess + (long)k * NVR;
+          dt = C.dt[k];
+          load_paused(W, k, s);
+          warm0 = s.warm;
+          budget = 1 << 30;
+          how.cap = inner_cap;
+          have = true;
+        }
+      }
+    }
+    const unsigned live = __ballot_sync(FULL, have);
+    if (!live) break;
+    // a thinned warp hands its cells over at their next iteration boundary
+    if (drained && __popc(live) <= thin) budget = 0;
+    if (have) {
+      const int b0 = budget;
+      const int r = imp_advance(R, u0, p0, dt, rg, s, budget, wg, &how);
+      st_it += (unsigned)(b0 - budget);
+      if (r == IMP_OVER_CAP) {
+        const unsigned slot = atomicAdd(W.ctl + 3, 1u);
+        if (slot < (unsigned)W.nslots) {
+          W.qs[slot] = k;
+          W.ss[slot] = s;
+          st_coop++;
+        } else {
+          how.cap = 0;   // no room: the lane repeats the evaluation alone, without the cap
+        }
+        if (slot < (unsigned)W.nslots) {
+          st_ev += s.evals;
+          st_in0 += s.inner[0];
+          st_in1 += s.inner[1];
+          st_fb += (unsigned)(warm0 && !s.warm);
+          have = false;
+        }
+      } else if (r != IMP_RUNNING) {
+        if (r == IMP_PAUSE) {
+          W.watt[k] = s.att;
+          W.wit[k] = s.iter;
+          W.wwarm[k] = s.warm;
+          for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = s.pp[i];
+          const unsigned at = atomicAdd(W.ctl + 1, 1u);
+          W.q[1][0][at] = k;
+        } else if (r == IMP_DONE_OK) {
+          cell_success(R, C, k, rg, s.pp, s.att, s.iter);
+        } else {
+          cell_failure(C, k);
+        }
+        st_ev += s.evals;
+        st_in0 += s.inner[0];
+        st_in1 += s.inner[1];
+        st_fb += (unsigned)(warm0 && !s.warm);
+        have = false;
+      }
+    }
+  }
+  // every lane is here (the loop ends on a warp-wide ballot)
+  warp_add(W.stats, st_it);
+  warp_add(W.stats + 2, st_fb);
+  warp_add(W.stats + 3, st_ev);
+  warp_add(W.stats + 4, st_in0);
+  warp_add(W.stats + 5, st_in1);
+  warp_add(W.stats + 6, st_coop);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && nin > 0) atomicAdd(W.stats + 1, 1ull);
+}
+
+// k_rad_finish: the cells k_rad_persist handed over, each run to its end by
+// a whole warp that takes them from a counter.  At the start of every
+// Newton iteration lanes 0..8 evaluate the base and the Jacobian columns on
+// both sides together (imp_eval_entry, as k_rad_tail does), each with the
+// cap on its nested inversion; the entries that ran over the cap, and the
+// remaining evaluations (damped trials, the final inversion, and the
+// evaluation a handed-over state stopped in), run their nested MHD
+// inversion with all 32 lanes (the damped trials tried 32 at a time, as
+// k_rad_slow does).  The sequence of operations per cell is that of the
+// one-thread form.
+__global__ void __launch_bounds__(128, KGPU_RAD_MIN_BLOCKS) k_rad_finish(RadParams R, Cell C, Work W, int warm_attempts,
+                                                    unsigned inner_cap) {
+  const unsigned FULL = 0xffffffffu;
+  const int ncoop0 = (int)W.ctl[3];
+  const int ncoop = ncoop0 < W.nslots ? ncoop0 : W.nslots;
+  const int total = ncoop + (int)W.ctl[1];
+  __shared__ ImpEval cache_sh[TAIL_WARPS][IMP_NCACHE];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  ImpEval *ce = cache_sh[wib];
+  while (true) {
+    int q = 0;
+    if (lane == 0) q = (int)atomicAdd(W.ctl + 2, 1u);
+    q = __shfl_sync(FULL, q, 0);
+    if (q >= total) break;
+    int k;
+    ImpState s;
+    if (q < ncoop) {
+      k = W.qs[q];
+      s = W.ss[q];
+      s.evals = 0;
+      s.inner[0] = s.inner[1] = 0;
+    } else {
+      k = W.q[1][0][q - ncoop];
+      load_paused(W, k, s);
+    }
+    RadGeom rg;
+    rad_geom(C.g + 20L * k, C.G + 20L * k, rg);
+    const double *u0 = C.uu + (long)k * NVR, *p0 = C.pp + (long)k * NVR;
+    const double dt = C.dt[k];
+    const double *wg = W.wguess + (long)k * NVR;
+    const int warm0 = s.warm;
+    ImpInner how{nullptr, 0u, true, warm_attempts};
+    int budget = 1 << 30;
+    int r;
+    // a handed-over state may stop inside an iteration: its entries are
+    // not in the cache until the next iteration starts
+    unsigned valid = 0u;
+    while (true) {
+      if (s.phase == PH_BASE) {
+        bool ok = false;
+        if (lane < IMP_NCACHE) ok = imp_eval_entry(R, u0, p0, dt, rg, s, lane, ce[lane], inner_cap);
+        valid = __ballot_sync(FULL, ok) & ((1u << IMP_NCACHE) - 1u);
+        __syncwarp();   // the entries written are visible to every lane
+      }
+      const ImpCache cache{ce, valid};
+      r = imp_advance(R, u0, p0, dt, rg, s, budget, wg, &how, &cache);
+      __syncwarp();   // every lane has read the entries before they are replaced
+      if (r != IMP_RUNNING) break;
+    }
+    if (lane == 0) {
+      if (r == IMP_DONE_OK) cell_success(R, C, k, rg, s.pp, s.att, s.iter);
+      else cell_failure(C, k);
+      atomicAdd(W.stats, (unsigned long long)((1 << 30) - budget));
+      if (warm0 && !s.warm) atomicAdd(W.stats + 2, 1ull);
+      atomicAdd(W.stats + 3, (unsigned long long)s.evals);
+      atomicAdd(W.stats + 4, (unsigned long long)s.inner[0]);
+      atomicAdd(W.stats + 5, (unsigned long long)s.inner[1]);
+    }
+    __syncwarp();
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && total > 0) atomicAdd(W.stats + 1, 1ull);
 }
 
 __global__ void k_rad_u2p(RadParams R, int n, const double *uu, double *pp, const double *g, const double *G,
@@ -548,26 +787,44 @@ extern "C" int kgpu_rad_default_params(kgpu_rad_params *rp, double mass, double 
   return 0;
 }
 
+extern "C" int kgpu_rad_default_solver_opts(kgpu_rad_solver_opts *o) {
+  if (!o) return KGPU_EINVAL;
+  *o = to_api(Opts());
+  return 0;
+}
+
+extern "C" int kgpu_rad_set_solver_opts(const kgpu_rad_solver_opts *o) {
+  if (!o || !opts_valid(*o)) return KGPU_EINVAL;
+  g_opts = from_api(*o);
+  return 0;
+}
+
+extern "C" int kgpu_rad_get_solver_opts(kgpu_rad_solver_opts *o) {
+  if (!o) return KGPU_EINVAL;
+  *o = to_api(g_opts);
+  return 0;
+}
+
 extern "C" int kgpu_rad_set_warm_attempts(int k) {
   if (k < 1 || k > IMP_NATTEMPTS) return KGPU_EINVAL;
-  g_warm_attempts = k;
+  g_opts.warm_attempts = k;
   return 0;
 }
 
 extern "C" int kgpu_rad_set_inner_cap(int cap) {
   if (cap < 0) return KGPU_EINVAL;
-  g_inner_cap = (unsigned)cap;
+  g_opts.inner_cap = cap;
   return 0;
 }
 
 extern "C" int kgpu_rad_set_tail(int on) {
-  g_tail = on ? 1 : 0;
+  g_opts.tail = on ? 1 : 0;
   return 0;
 }
 
 extern "C" int kgpu_rad_set_pass_iters(int k) {
   if (k < 1) return KGPU_EINVAL;
-  g_pass_iters = k;
+  g_opts.pass_iters = k;
   return 0;
 }
 
@@ -576,19 +833,40 @@ extern "C" size_t kgpu_rad_work_bytes(int n) {
   return work_layout(n, kMaxPasses, nullptr, nullptr) + 256;
 }
 
+// resident blocks of k_rad_persist per SM
+static int persist_blocks_per_sm(const Opts &o) {
+  if (o.blocks_per_sm > 0) return o.blocks_per_sm;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_rad_persist, 128, 0) != cudaSuccess || nb < 1) nb = 1;
+  return nb;
+}
+
+// kernels one solve launches (for the launch counters)
+static long long solve_launches(const RadParams &R, int mode, const Opts &o) {
+  if (mode == KGPU_RAD_PLAIN) return 1;
+  if (mode == KGPU_RAD_PERSISTENT) return 3;
+  const int np = max_passes(R, o.pass_iters);
+  return 1 + (o.inner_cap ? 2 : 1) * np + (o.tail ? np - 1 : 0);
+}
+
 // acc (device, optional): counters the solve adds to instead of reporting
 // through stats: [0] Newton iterations, [1] passes with work, [2] warm-start
-// fallbacks.  Launches only (no allocation, no synchronisation) when stats
-// is null, so that a time step can be captured in a CUDA graph.
+// fallbacks, [3] residual evaluations, [4] nested Newton steps, [5] their
+// W-function evaluations, [6] evaluations handed to a whole warp.
+// Launches only (no allocation, no synchronisation) when stats is null, so
+// that a time step can be captured in a CUDA graph.
 static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
                             const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
                             int *status, int *attempt, int *iters, int mode, void *work, void *stream,
-                            unsigned long long *stats, int nstats, unsigned long long *acc = nullptr,
+                            unsigned long long *stats, int nstats, const Opts &o, unsigned long long *acc = nullptr,
                             int gate = -1) {
-  if (n < 0 || !rp || (mode != KGPU_RAD_PLAIN && mode != KGPU_RAD_BATCHED)) return KGPU_EINVAL;
+  if (n < 0 || !rp || (mode != KGPU_RAD_PLAIN && mode != KGPU_RAD_BATCHED && mode != KGPU_RAD_PERSISTENT))
+    return KGPU_EINVAL;
   if (n > 0 && (!uu || !pp || !g || !G || !dt || !pp_out || !uu_out || !status || !attempt || !iters))
     return KGPU_EINVAL;
-  if (mode == KGPU_RAD_BATCHED && n > 0 && !work) return KGPU_EINVAL;
+  if (mode != KGPU_RAD_PLAIN && n > 0 && !work) return KGPU_EINVAL;
+  if (ypred && mode == KGPU_RAD_PLAIN) return KGPU_EINVAL;
+  if (nstats < 0 || nstats > 8) return KGPU_EINVAL;
   if (stats)
     for (int i = 0; i < nstats; i++) stats[i] = 0;
   if (n == 0) return 0;
@@ -606,37 +884,48 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
     k_rad_plain<<<(n + 127) / 128, 128, 0, st>>>(R, C, n, dstats);
     RCK(cudaGetLastError());
     if (stats) {
-      RCK(cudaMemcpyAsync(stats, dstats, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+      unsigned long long h[8];
+      RCK(cudaMemcpyAsync(h, dstats, sizeof(h), cudaMemcpyDeviceToHost, st));
       RCK(cudaStreamSynchronize(st));
-      stats[1] = 1;
+      h[1] = 1;
+      for (int i = 0; i < nstats; i++) stats[i] = h[i];
     }
     return 0;
   }
-  const int K = g_pass_iters;
-  const int passes = max_passes(R, K);
+  const int K = o.pass_iters;
+  const int passes = mode == KGPU_RAD_BATCHED ? max_passes(R, K) : 1;
   char *base = (char *)(((uintptr_t)work + 255) & ~(uintptr_t)255);
   Work W;
   work_layout(n, passes, &W, base);   // fits: the area is sized for kMaxPasses >= passes
   RCK(cudaMemsetAsync(W.count, 0, (size_t)(passes + 2) * 3 * 4, st));
   RCK(cudaMemsetAsync(W.tail_done, 0, sizeof(unsigned), st));
+  RCK(cudaMemsetAsync(W.ctl, 0, 4 * sizeof(unsigned), st));
   if (acc) W.stats = acc;
   else RCK(cudaMemsetAsync(W.stats, 0, 8 * sizeof(unsigned long long), st));
-  const int grid = sm_count() * 8;
   k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n, ypred, gate);
   RCK(cudaGetLastError());
-  for (int p = 0; p < passes; p++) {
-    const int Kp = p == passes - 1 ? (1 << 30) : K;   // the last pass finishes whatever is left
-    const int blocks = p == 0 ? (n + 127) / 128 : grid;
-    k_rad_pass<<<blocks, 128, 0, st>>>(R, C, W, n, p, Kp, g_inner_cap, g_warm_attempts);
+  if (mode == KGPU_RAD_PERSISTENT) {
+    const int grid = sm_count() * persist_blocks_per_sm(o);
+    k_rad_persist<<<grid, 128, 0, st>>>(R, C, W, (unsigned)o.inner_cap, o.warm_attempts, o.thin);
     RCK(cudaGetLastError());
-    if (g_inner_cap) {
-      k_rad_slow<<<grid / 2, 128, 0, st>>>(R, C, W, n, p, Kp, g_warm_attempts);
+    k_rad_finish<<<grid, 128, 0, st>>>(R, C, W, o.warm_attempts, (unsigned)o.inner_cap);
+    RCK(cudaGetLastError());
+  } else {
+    const int grid = sm_count() * 8;
+    for (int p = 0; p < passes; p++) {
+      const int Kp = p == passes - 1 ? (1 << 30) : K;   // the last pass finishes whatever is left
+      const int blocks = p == 0 ? (n + 127) / 128 : grid;
+      k_rad_pass<<<blocks, 128, 0, st>>>(R, C, W, n, p, Kp, (unsigned)o.inner_cap, o.warm_attempts);
       RCK(cudaGetLastError());
-    }
-    if (g_tail && p < passes - 1) {
-      // one wave: two blocks of four warps per SM at this kernel's registers
-      k_rad_tail<<<sm_count() * 2, 128, 0, st>>>(R, C, W, n, p, sm_count() * 8, g_warm_attempts);
-      RCK(cudaGetLastError());
+      if (o.inner_cap) {
+        k_rad_slow<<<grid / 2, 128, 0, st>>>(R, C, W, n, p, Kp, o.warm_attempts);
+        RCK(cudaGetLastError());
+      }
+      if (o.tail && p < passes - 1) {
+        // one wave: two blocks of four warps per SM at this kernel's registers
+        k_rad_tail<<<sm_count() * 2, 128, 0, st>>>(R, C, W, n, p, sm_count() * 8, o.warm_attempts);
+        RCK(cudaGetLastError());
+      }
     }
   }
   if (stats) {
@@ -651,15 +940,14 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
 int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
                            const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
                            int *status, int *attempt, int *iters, int mode, void *work, void *stream,
-                           unsigned long long *acc, long long *launches, int gate) {
-  if (launches) {
-    RadParams R = to_dev(*rp);
-    const int np = max_passes(R, g_pass_iters);
-    *launches = mode == KGPU_RAD_PLAIN ? 1 : 1 + (g_inner_cap ? 2 : 1) * np + (g_tail ? np - 1 : 0);
-  }
+                           unsigned long long *acc, long long *launches, int gate, const kgpu_rad_solver_opts *opts) {
+  const Opts o = opts ? from_api(*opts) : g_opts;
+  if (launches) *launches = solve_launches(to_dev(*rp), mode, o);
   return rad_solve_device(n, rp, uu, pp, g, G, dt, ypred, pp_out, uu_out, status, attempt, iters, mode, work, stream,
-                          nullptr, 0, acc, gate);
+                          nullptr, 0, o, acc, gate);
 }
+
+bool kgpu_rad_opts_valid(const kgpu_rad_solver_opts &o) { return opts_valid(o); }
 
 // Device form of the radiation constants, for the grid step.
 kgpu::RadParams kgpu_rad_device_params(const kgpu_rad_params &p) { return to_dev(p); }
@@ -669,7 +957,7 @@ extern "C" int kgpu_rad_implicit_cells_device(int n, const kgpu_rad_params *rp, 
                                               double *uu_out, int *status, int *attempt, int *iters, int mode,
                                               void *work, void *stream, unsigned long long *stats) {
   return rad_solve_device(n, rp, uu, pp, g, G, dt, nullptr, pp_out, uu_out, status, attempt, iters, mode, work,
-                          stream, stats, 2);
+                          stream, stats, 2, g_opts);
 }
 
 extern "C" int kgpu_rad_implicit_cells_warm_device(int n, const kgpu_rad_params *rp, const double *uu,
@@ -679,7 +967,18 @@ extern "C" int kgpu_rad_implicit_cells_warm_device(int n, const kgpu_rad_params 
                                                    void *work, void *stream, unsigned long long *stats) {
   if (n > 0 && !ypred) return KGPU_EINVAL;
   return rad_solve_device(n, rp, uu, pp, g, G, dt, ypred, pp_out, uu_out, status, attempt, iters,
-                          KGPU_RAD_BATCHED, work, stream, stats, 3);
+                          KGPU_RAD_BATCHED, work, stream, stats, 3, g_opts);
+}
+
+extern "C" int kgpu_rad_implicit_cells_device_ex(int n, const kgpu_rad_params *rp, const double *uu,
+                                                 const double *pp, const double *g, const double *G,
+                                                 const double *dt, const float *ypred, double *pp_out,
+                                                 double *uu_out, int *status, int *attempt, int *iters, int mode,
+                                                 const kgpu_rad_solver_opts *opts, void *work, void *stream,
+                                                 unsigned long long *stats, int nstats) {
+  if (opts && !opts_valid(*opts)) return KGPU_EINVAL;
+  return rad_solve_device(n, rp, uu, pp, g, G, dt, ypred, pp_out, uu_out, status, attempt, iters, mode, work,
+                          stream, stats, nstats, opts ? from_api(*opts) : g_opts);
 }
 
 // network inputs of n cells (float [n][16])
@@ -735,7 +1034,7 @@ extern "C" int kgpu_rad_implicit_cells(int n, const kgpu_rad_params *rp, const d
   if (n == 0) return 0;
   if (!uu || !pp || !g || !G || !dt || !pp_out || !uu_out || !status || !attempt || !iters) return KGPU_EINVAL;
   const size_t cell_bytes = (size_t)n * (4 * NVR + 40 + 1) * 8 + (size_t)n * 3 * 4;
-  const size_t work = mode == KGPU_RAD_BATCHED ? kgpu_rad_work_bytes(n) : 0;
+  const size_t work = mode != KGPU_RAD_PLAIN ? kgpu_rad_work_bytes(n) : 0;
   DevMem m;
   RCK(cudaMalloc(&m.p, cell_bytes + work + 16 * 256));   // room for the 256-byte alignment of 11 regions
   char *b = (char *)m.p;

@@ -14,6 +14,15 @@
 
 #include "kgpu_physics.cuh"
 
+// Large routines of the implicit solve that are called from several places
+// of its evaluation: out of line with -DKGPU_RAD_NOINLINE (one copy of each
+// in the instruction stream), inlined by default.
+#ifdef KGPU_RAD_NOINLINE
+#define KG_RAD_CALL __noinline__
+#else
+#define KG_RAD_CALL
+#endif
+
 namespace kgpu {
 
 constexpr int NVR = 13;
@@ -105,14 +114,14 @@ KG_HD void p2u_rad(const double *pp, double *uu, const Geom &g) {
   uu[FZ0] = gdetu * Rt[3];
 }
 // p2u for the full 13-variable state (p2u.c:40-48)
-KG_HD void p2u_rad_full(const Grid &G, const double *pp, double *uu, const Geom &g) {
+KG_RAD_CALL KG_HD void p2u_rad_full(const Grid &G, const double *pp, double *uu, const Geom &g) {
   p2u_full(G, pp, uu, g);
   p2u_rad(pp, uu, g);
 }
 
 // fluid-frame radiation energy density -R^t_t and the gas four-velocity
 // (calc_ff_Rtt, rad.c:2833-2860)
-KG_HD void calc_ff_Rtt(const double *pp, const Geom &g, double &Rtt, double ucon[4]) {
+KG_RAD_CALL KG_HD void calc_ff_Rtt(const double *pp, const Geom &g, double &Rtt, double ucon[4]) {
   double ut[4] = {0., pp[VX], pp[VY], pp[VZ]}, ucov[4];
   velr_to_vel4(ut, ucon, ucov, g);
   double Rij[4][4], Rl[4][4];
@@ -161,7 +170,7 @@ KG_HD void boost2_lab2ff(double A[4], const double *pp, const Geom &g) {
 
 // radiative four-force G^mu, lab frame (labframe = 1) or fluid frame with
 // the time component rewritten (calc_Gi, rad.c:1787-1888; no Comptonisation)
-KG_HD void calc_Gi(const RadParams &R, const double *pp, const Geom &g, double Gi[4], int labframe) {
+KG_RAD_CALL KG_HD void calc_Gi(const RadParams &R, const double *pp, const Geom &g, double Gi[4], int labframe) {
   double Rij[4][4];
   calc_Rij_M1(pp, g, Rij);
   double ut[4] = {0., pp[2], pp[3], pp[4]}, ucon[4], ucov[4];
@@ -196,7 +205,7 @@ KG_HD void calc_Gi(const RadParams &R, const double *pp, const Geom &g, double G
 KG_HD double m1_pow2(double x) { return pow(x, 2.); }
 
 // lab-frame gamma^2 of the radiation frame from R_t_mu (u2prad.c:116-250)
-KG_HD double m1_gammarel2(const RadParams &R, const RadGeom &rg, const double Avcov[4]) {
+KG_RAD_CALL KG_HD double m1_gammarel2(const RadParams &R, const RadGeom &rg, const double Avcov[4]) {
   const auto &GG = rg.g.GG;
   double gn11 = GG[0][0], gn12 = GG[0][1], gn13 = GG[0][2], gn14 = GG[0][3], gn22 = GG[1][1], gn23 = GG[1][2],
          gn24 = GG[1][3], gn33 = GG[2][2], gn34 = GG[2][3], gn44 = GG[3][3];
@@ -244,7 +253,7 @@ KG_HD double m1_gammarel2(const RadParams &R, const RadGeom &rg, const double Av
 
 // cold solution at a prescribed gamma^2 (u2prad.c:9-105): new R_t, R^t, Erf
 // and the relative four-velocity
-KG_HD void m1_cold(const RadGeom &rg, double Avcon[4], double Avcov[4], double gammarel2, double &Erf,
+KG_RAD_CALL KG_HD void m1_cold(const RadGeom &rg, double Avcon[4], double Avcov[4], double gammarel2, double &Erf,
                    double urfconrel[4]) {
   const auto &GG = rg.g.GG;
   double alpha = rg.alpha;
@@ -274,7 +283,7 @@ KG_HD void m1_cold(const RadGeom &rg, double Avcon[4], double Avcov[4], double g
 
 // u2p_rad (u2prad.c:485-520 with get_m1closure_* 116-411).  Returns 0 or -1;
 // corrected = 1 when the closure fell back to a cold solution.
-KG_HD int u2p_rad(const RadParams &R, const double *uu, double *pp, const RadGeom &rg, int &corrected) {
+KG_RAD_CALL KG_HD int u2p_rad(const RadParams &R, const double *uu, double *pp, const RadGeom &rg, int &corrected) {
   corrected = 0;
   const auto &GG = rg.g.GG;
   const double gdetu = rg.g.gdet;
@@ -325,7 +334,7 @@ KG_HD int u2p_rad(const RadParams &R, const double *uu, double *pp, const RadGeo
 
 // 4x4 inverse by cofactors (misc.c:500-602), the same products and sums in
 // the same order; returns -1 on a NaN determinant or entry.
-KG_HD int inverse_44(const double a[4][4], double ia[4][4]) {
+KG_RAD_CALL KG_HD int inverse_44(const double a[4][4], double ia[4][4]) {
   double s[16], d[16], t[12];
   for (int i = 0; i < 4; i++) {
     s[i] = a[i][0];
@@ -387,7 +396,7 @@ struct ImpInner {
 };
 
 // inner: where and how the nested inversion runs (see ImpInner)
-KG_HD int imp_u2p_hot(const RadParams &R, const double *uu, double *pp, const Geom &g, const ImpInner *inner = nullptr) {
+KG_RAD_CALL KG_HD int imp_u2p_hot(const RadParams &R, const double *uu, double *pp, const Geom &g, const ImpInner *inner = nullptr) {
   Grid G;
   G.gamma = R.gamma;
   G.u2pconv = R.u2pconv;
@@ -396,13 +405,10 @@ KG_HD int imp_u2p_hot(const RadParams &R, const double *uu, double *pp, const Ge
 #ifdef __CUDA_ARCH__
   if (inner && inner->warp) return u2p_solver_W_warp(G, uu, pp, g, 0, st, st ? st + 1 : nullptr);
 #endif
-  if (inner && inner->cap) {
-    unsigned used = 0;
-    int r = u2p_solver_W(G, uu, pp, g, 0, st, &used, inner->cap);
-    if (st) st[1] += used;
-    return r;
-  }
-  return u2p_solver_W(G, uu, pp, g, 0, st, st ? st + 1 : nullptr);
+  unsigned used = 0;
+  const int r = u2p_solver_W(G, uu, pp, g, 0, st, &used, inner ? inner->cap : 0u);
+  if (st) st[1] += used;
+  return r;
 }
 
 KG_HD double rad_Sfromu(const RadParams &R, double rho, double u) { return calc_Sfromu(R.gamma, rho, u); }
@@ -458,7 +464,7 @@ KG_HD int imp_prepare(const RadParams &R, const ImpParams &P, const double *uu0,
 // residual f[4] and its relative size from a prepared state (the rest of
 // f_implicit_lab_4dprim, rad.c:199-351).  Returns -1 on failure, 1 when the
 // closure was corrected, else 0.
-KG_HD int imp_residual(const RadParams &R, const ImpParams &P, double *pp, const double *uu, const double *uu0,
+KG_RAD_CALL KG_HD int imp_residual(const RadParams &R, const ImpParams &P, double *pp, const double *uu, const double *uu0,
                        const double *pp00, double dt, const RadGeom &rg, int u2pret, int corr, double f[4],
                        double &err0) {
   const Geom &g = rg.g;
@@ -678,9 +684,11 @@ KG_HD void imp_input(const RadParams &R, int sh, const ImpState &s, const RadGeo
 }
 
 // Entry `slot` of the iteration that cell state s (in phase PH_BASE) is
-// about to start, evaluated without a cap on the nested inversion.
-KG_HD void imp_eval_entry(const RadParams &R, const double *uu0, const double *pp00, double dt, const RadGeom &rg,
-                          const ImpState &s, int slot, ImpEval &e) {
+// about to start.  With cap > 0 a nested inversion that passes cap
+// W-function evaluations is abandoned and false returned: the entry is not
+// valid, and the state machine evaluates it itself.
+KG_HD bool imp_eval_entry(const RadParams &R, const double *uu0, const double *pp00, double dt, const RadGeom &rg,
+                          const ImpState &s, int slot, ImpEval &e, unsigned cap = 0u) {
   const ImpParams P = imp_attempt(s.att, s.sw);
   const int sh = P.prim == IMP_MHD ? UU : EE0;
   ImpState t = s;
@@ -695,12 +703,14 @@ KG_HD void imp_eval_entry(const RadParams &R, const double *uu0, const double *p
   imp_input(R, sh, t, rg, e.pin);
   double uu[NVR];
   e.inner[0] = e.inner[1] = 0;
-  ImpInner in{e.inner, 0u, false, IMP_NATTEMPTS};
+  ImpInner in{e.inner, cap, false, IMP_NATTEMPTS};
   e.corr = 0;
   e.u2pret = imp_prepare(R, P, uu0, e.pin, uu, rg, e.corr, &in);
+  if (e.u2pret == U2P_OVER_CAP) return false;
   for (int i = 0; i < 4; i++) e.f[i] = 0.;
   e.err = 0.;
   e.fret = imp_residual(R, P, e.pin, uu, uu0, pp00, dt, rg, e.u2pret, e.corr, e.f, e.err);
+  return true;
 }
 
 // One evaluation and the transition that follows it.  `budget` counts the

@@ -2,8 +2,9 @@
 # Builds the reference KORAL path into a shared library for the parity
 # oracle.  Test infrastructure.
 #
-# The reference sources are compiled where they lie (read-only tree, default
-# /root/reference, override with KORAL_REF_DIR); nothing is copied.  Problem
+# The reference sources are compiled where they lie (a read-only tree given
+# by KORAL_REF_DIR, or else by the one-line file reference_tree beside this
+# script); nothing is copied.  Problem
 # selection is done with the reference's own plug-in mechanism: the
 # directory oracle/ref/problems/<PROBLEM> holds a problem.h selector plus the
 # plug-in files, and is put in front of the quote-include search path with
@@ -23,7 +24,7 @@
 set -euo pipefail
 PROBLEM="$1"; OUTLIB="$2"; shift 2
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${KORAL_REF_DIR:-/root/reference}"
+REF="${KORAL_REF_DIR:-$(head -n 1 "$HERE/reference_tree")}"
 PROBDIR="$HERE/problems/$PROBLEM"
 [ -d "$REF" ] || { echo "reference tree $REF not present" >&2; exit 3; }
 [ -f "$PROBDIR/problem.h" ] || { echo "no plug-in $PROBDIR" >&2; exit 2; }
@@ -32,7 +33,7 @@ OUTDIR="$(dirname "$OUTLIB")"
 OBJDIR="$OUTLIB.objs"
 mkdir -p "$OUTDIR" "$OBJDIR"
 
-CFLAGS=(-O2 -fPIC -fcommon -ffp-contract=off -fno-fast-math -DNOSILO -w)
+CFLAGS=(-O3 -fPIC -fcommon -ffp-contract=off -fno-fast-math -DNOSILO -w)
 if [ "${KORAL_REF_OPENMP:-0}" = "1" ]; then CFLAGS+=(-fopenmp); fi
 INC=(-I "$PROBDIR" -I- -I "$HERE/gsl_shim" -I "$REF")
 
@@ -57,4 +58,5 @@ if [ "$FAIL" = 1 ]; then grep -h -v "obsolete option '-I-'" "$OBJDIR"/*.log >&2;
 LINK=(-shared -Wl,-Bsymbolic -Wl,--no-undefined)
 if [ "${KORAL_REF_OPENMP:-0}" = "1" ]; then LINK+=(-fopenmp); fi
 gcc "${LINK[@]}" -o "$OUTLIB" "${OBJS[@]}" "$OBJDIR/harness.o" "$OBJDIR/gsl_shim.o" -lm
+rm -r "$OBJDIR"   # objects are rebuilt on every call; only the library is kept
 echo "built $OUTLIB"

@@ -87,7 +87,14 @@
 #define MINY 0.005
 #define MAXY 0.995
 #define MINZ 0.
-#define MAXZ (2. * M_PI)
+/* a phi wedge [0, TORUS_MAXZ] with TNZ cells and periodic phi boundaries
+ * (e.g. -DTNZ=8 -DTORUS_MAXZ='(M_PI/4.)' keeps the phi cell size of the
+ * 64-cell torus and the same cells, noise included, as its first 8 phi
+ * columns) */
+#ifndef TORUS_MAXZ
+#define TORUS_MAXZ (2. * M_PI)
+#endif
+#define MAXZ TORUS_MAXZ
 #ifndef TNX
 #define TNX 192
 #endif

@@ -92,7 +92,7 @@ def test_rad_implicit_matches_reference(kgpu, ref, cells):
     un = uu.copy()
     un[:, 1] = np.nextafter(un[:, 1], np.inf)
     pn, _, sn, _, inn = ref.implicit(un, pp, g, G, dt)
-    pg, ug, sg, ag, ig = kgpu.rad_implicit_cells(rp, uu, pp, g, G, dt, mode=kgpu.RAD_BATCHED)
+    pg, ug, sg, ag, ig = kgpu.rad_implicit_cells(rp, uu, pp, g, G, dt, mode=kgpu.RAD_PERSISTENT)
     q = [0.5, 0.9, 0.99]
     bg, bn = (sg == 0) & (sr == 0), (sn == 0) & (sr == 0)
     dg, dn = np.quantile(scaled_difference(pg[bg], pr[bg]), q), np.quantile(scaled_difference(pn[bn], pr[bn]), q)
@@ -109,21 +109,42 @@ def test_rad_implicit_matches_reference(kgpu, ref, cells):
 
 
 def test_rad_batched_equals_plain(kgpu, cells):
-    """The work-queue form resumes each Newton solve exactly where it paused:
-    its results are those of the one-thread-per-cell form, bit for bit, for
-    any number of iterations per pass, with the warp-per-cell tail (the
-    base and Jacobian evaluations of an iteration done by lanes together)
-    and without it."""
+    """The work-queue forms resume each Newton solve exactly where it paused:
+    their results are those of the one-thread-per-cell form, bit for bit.
+    Batched: any number of iterations per pass, with the warp-per-cell tail
+    (the base and Jacobian evaluations of an iteration done by lanes
+    together) and without it.  Persistent: any hand-off threshold of a
+    thinned warp, with and without the cap on nested inversions, at one
+    block per SM and at the occupancy limit.  The tuning is passed per call;
+    the process-wide values are not touched."""
+    import torch
     rp, uu, pp, g, G, dt = cells
-    a = kgpu.rad_implicit_cells(rp, uu, pp, g, G, dt, mode=kgpu.RAD_PLAIN)
-    try:
-        for tail in (1, 0):
-            assert kgpu.lib().kgpu_rad_set_tail(tail) == 0
-            for k in (1, 3, 8):
-                assert kgpu.lib().kgpu_rad_set_pass_iters(k) == 0
-                b = kgpu.rad_implicit_cells(rp, uu, pp, g, G, dt, mode=kgpu.RAD_BATCHED)
-                for x, y in zip(a, b):
-                    assert np.array_equal(x, y), (tail, k)
-    finally:
-        kgpu.lib().kgpu_rad_set_pass_iters(8)
-        kgpu.lib().kgpu_rad_set_tail(1)
+    d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (uu, pp, g, G, dt)]
+    a = [x.cpu().numpy() for x in kgpu.rad_solve_device(rp, *d, mode=kgpu.RAD_PLAIN)[:5]]
+    host = kgpu.rad_implicit_cells(rp, uu, pp, g, G, dt, mode=kgpu.RAD_PLAIN)
+    for x, y in zip(a, host):
+        assert np.array_equal(x, y)
+    variants = [(kgpu.RAD_BATCHED, dict(tail=tail, pass_iters=k)) for tail in (1, 0) for k in (1, 3, 8)]
+    variants += [(kgpu.RAD_PERSISTENT, dict(thin=thin, inner_cap=cap, blocks_per_sm=b))
+                 for thin, cap, b in ((8, 64, 0), (0, 64, 0), (32, 64, 1), (8, 0, 0), (16, 4, 1))]
+    stats = {}
+    for mode, kw in variants:
+        out = kgpu.rad_solve_device(rp, *d, mode=mode, opts=kgpu.solver_opts(**kw), nstats=7)
+        b = [x.cpu().numpy() for x in out[:5]]
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y), (mode, kw)
+        stats[(mode, tuple(kw.items()))] = out[5]
+    # the Newton iterations and evaluations are the same in every variant
+    its = {v[0] for v in stats.values()}
+    evs = {v[3] for v in stats.values()}
+    assert len(its) == 1 and len(evs) == 1, stats
+
+
+def test_rad_persistent_launches(kgpu, cells):
+    """The persistent form runs a solve in three launches (start, the
+    resident kernel, the warp-per-cell finish), whatever the cells need."""
+    import torch
+    rp, uu, pp, g, G, dt = cells
+    d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (uu, pp, g, G, dt)]
+    out = kgpu.rad_solve_device(rp, *d, mode=kgpu.RAD_PERSISTENT, nstats=7)
+    assert out[5][1] in (1, 2)   # launches that had work: the resident kernel, and the finish if cells were handed on

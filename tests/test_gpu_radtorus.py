@@ -180,7 +180,8 @@ def test_radtorus_solver_variants_and_graph_identical(kgpu, oracle):
     R.init()
     u, p, tsd = R.array("u").copy(), R.array("p").copy(), R.scalar("tstepdenmax")
     out = []
-    for mode, graph in ((kgpu.RAD_BATCHED, False), (kgpu.RAD_BATCHED, True), (kgpu.RAD_PLAIN, True)):
+    for mode, graph in ((kgpu.RAD_BATCHED, False), (kgpu.RAD_BATCHED, True), (kgpu.RAD_PLAIN, True),
+                        (kgpu.RAD_PERSISTENT, False), (kgpu.RAD_PERSISTENT, True)):
         s = make_gpu(kgpu, R)
         s.set_implicit_solver(mode, None)
         s.upload_state(u.copy(), p.copy())
@@ -188,8 +189,42 @@ def test_radtorus_solver_variants_and_graph_identical(kgpu, oracle):
         s.rk2imex_steps(3, graph=graph)
         out.append(s.download_state())
         s.close()
-    for k in (1, 2):
+    for k in range(1, len(out)):
         assert np.array_equal(out[0][0], out[k][0]) and np.array_equal(out[0][1], out[k][1]), k
+
+
+def test_radtorus_solver_options_per_context(kgpu, oracle):
+    """Two contexts in one process hold their own solver tuning: setting one
+    leaves the other alone, a captured step graph is re-captured when its
+    context's options change (its launch count follows them), and the
+    results stay the same bits."""
+    R = oracle.RefKoral(LIB)
+    R.init()
+    u, p, tsd = R.array("u").copy(), R.array("p").copy(), R.scalar("tstepdenmax")
+    a, b = make_gpu(kgpu, R), make_gpu(kgpu, R)
+    for s in (a, b):
+        s.set_implicit_solver(kgpu.RAD_BATCHED, None)
+        s.upload_state(u.copy(), p.copy())
+        s.tstepdenmax = tsd
+    a.set_implicit_options(pass_iters=1)
+    assert b.implicit_options().pass_iters == 8 and a.implicit_options().pass_iters == 1
+    la = a.launches
+    a.rk2imex_steps(1, graph=True)
+    la = a.launches - la
+    lb = b.launches
+    b.rk2imex_steps(1, graph=True)
+    lb = b.launches - lb
+    assert la > lb   # one Newton iteration per pass: more pass launches
+    b.set_implicit_options(pass_iters=1)   # between two graph steps: re-captured
+    lb2 = b.launches
+    b.rk2imex_steps(1, graph=True)
+    assert b.launches - lb2 == la
+    a.rk2imex_steps(1, graph=True)
+    ua, pa = a.download_state()
+    ub, pb = b.download_state()
+    assert np.array_equal(ua, ub) and np.array_equal(pa, pb)
+    with pytest.raises(kgpu.KgpuError):
+        a.set_implicit_options(thin=33)
 
 
 def test_radtorus_two_steps_within_reference_sensitivity(kgpu, oracle, tmp_path):
