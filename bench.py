@@ -156,7 +156,56 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="radtorus", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-solve", choices=["plain", "batched", "persistent"], default=None,
+                    help="radtorus only, a profiling aid: after the warm-up steps solve the cells of the last "
+                         "implicit step again with this solver and print its counters as JSON (no bench line)")
+    ap.add_argument("--profile-cells", type=int, default=0,
+                    help="with --profile-solve: solve only the first this many cells (0: all)")
     return ap.parse_args()
+
+
+def profile_solve(args):
+    """A profiling aid for the radiative torus: after the warm-up steps, the
+    cells of the last implicit step (their inputs, as the step gathered
+    them; the first --profile-cells of them, or all) are solved once more
+    with the given solver through kgpu_rad_implicit_cells_device_ex, for an
+    ncu capture of its kernels; prints the solver's counters (solves, Newton
+    iterations, residual evaluations, nested inversion work) and its event
+    time as JSON, so that per-evaluation figures can be formed from the
+    capture."""
+    import torch
+    import koral_b200 as k
+    from koral_b200 import build
+    build.build()
+    torch.cuda.set_device(0)
+    s = make_subdomain(k, "radtorus")
+    mlp, _ = warmstart_network(k)
+    s.set_implicit_options(warm_attempts=WARM_ATTEMPTS_RADTORUS, skip=SKIP_RADTORUS)
+    s.set_implicit_solver(k.RAD_BATCHED, mlp)
+    s.rk2imex_steps(max(1, args.warmup), graph=True)
+    n, b = s.implicit_buffers()
+    m = min(n, args.profile_cells) if args.profile_cells > 0 else n
+
+    class Dev:
+        def __init__(self, ptr, shape):
+            self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f8", "data": (ptr, False), "version": 3}
+
+    d = [torch.as_tensor(Dev(b[key], shape), device="cuda")[:m].clone()
+         for key, shape in (("uu_in", (n, 13)), ("pp_in", (n, 13)), ("g20", (n, 20)), ("G20", (n, 20)), ("dt", (n,)))]
+    rp = s._rp
+    s.close()
+    mode = {"plain": k.RAD_PLAIN, "batched": k.RAD_BATCHED, "persistent": k.RAD_PERSISTENT}[args.profile_solve]
+    torch.cuda.synchronize()
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    out = k.rad_solve_device(rp, *d, mode=mode, nstats=7)
+    e.record()
+    torch.cuda.synchronize()
+    st = out[5]
+    print(json.dumps({"solver": args.profile_solve, "warmup_steps": args.warmup, "cells": m, "ms": a.elapsed_time(e),
+                      "newton_iterations": int(st[0]), "launches_with_work": int(st[1]), "evaluations": int(st[3]),
+                      "nested_newton_steps": int(st[4]), "nested_w_evaluations": int(st[5]),
+                      "evaluations_handed_to_a_warp": int(st[6])}))
 
 
 # ---------------------------------------------------------------------------
@@ -508,13 +557,17 @@ def warmstart_network(k):
 # served by the reference cascade; measured 236 against 365 ms per implicit
 # step with all six)
 WARM_ATTEMPTS_RADTORUS = 2
+# on the torus only the cells the network expects to fail their first
+# attempt start from its prediction (kgpu_rad_solver_opts.skip = 2): the
+# others are already close to their solution at the previous state
+SKIP_RADTORUS = 2
 # the implicit solver of the timed radiative-torus steps
 MAIN_SOLVER = "batched"
 # FP64 work of one residual evaluation of the implicit solve on the torus's
 # own cells, nested MHD inversion included: DADD + DMUL + 2 DFMA thread
 # instructions of the one-thread-per-cell solver over its counted
 # evaluations (ncu capture, profiles/k_rad_radtorus_256x128x64.md)
-IMP_FP64_PER_EVAL = None
+IMP_FP64_PER_EVAL = 2972.0
 
 CPU_REF_CHILD = r"""
 import json, sys, time
@@ -565,7 +618,7 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
     build.build()
     s = make_subdomain(k, args.workload)
     mlp, mlp_name = warmstart_network(k)
-    s.set_implicit_options(warm_attempts=WARM_ATTEMPTS_RADTORUS)
+    s.set_implicit_options(warm_attempts=WARM_ATTEMPTS_RADTORUS, skip=SKIP_RADTORUS)
     main_mode = {"persistent": k.RAD_PERSISTENT, "batched": k.RAD_BATCHED}[MAIN_SOLVER]
     other_mode, other_name = ((k.RAD_BATCHED, "batched") if main_mode == k.RAD_PERSISTENT
                               else (k.RAD_PERSISTENT, "persistent"))
@@ -710,6 +763,7 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
                    "parallelism": "replicas" if world > 1 else "single subdomain",
                    "graph": "one CUDA graph per RK2IMEX step", "solver": MAIN_SOLVER,
                    "warm_start_weights": mlp_name, "warm_attempts": WARM_ATTEMPTS_RADTORUS,
+                   "warm_start_skip": SKIP_RADTORUS,
                    "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps} from the initial torus"},
         "newton": {"learned": newton(c_main), "no_network": newton(c_n),
                    "iteration_ratio_no_network_over_learned": it_n / it_main if it_main > 0 else None},
@@ -758,7 +812,7 @@ def hbm_peak_of():
 # ---------------------------------------------------------------------------
 # our arm, batched implicit solve
 # ---------------------------------------------------------------------------
-def learned_leg(k, rp, d_in, work, stream, n, st_plain, it_plain, args, dev):
+def learned_leg(k, rp, d_in, work, stream, n, st_plain, it_plain, all_plain, args, dev):
     """The same solve with the learned warm start (features, network on the
     tensor cores, warm batched solve), timed as a whole, against the plain
     batched solve's iterations on the same cells."""
@@ -807,11 +861,17 @@ def learned_leg(k, rp, d_in, work, stream, n, st_plain, it_plain, args, dev):
     except Exception:
         pass
     bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    at = out[3].cpu().numpy()
     return {"value": n / (ms / 1e3), "unit": RAD_UNIT, "ms_per_step": ms,
+            "mean_iterations_all_attempts": stats[0] / n, "plain_mean_iterations_all_attempts": all_plain / n,
+            "iteration_ratio": all_plain / max(1, stats[0]),
+            "iteration_ratio_note": "Newton iterations per implicit solve over every attempt (failed attempts "
+                                    "and the fallback to the reference cascade included), plain over learned",
             "mean_iterations_successful_attempt": float(it[ok].mean()),
             "plain_mean_iterations_successful_attempt": float(it_plain[ok].mean()),
-            "iteration_ratio": float(it_plain[ok].mean() / it[ok].mean()),
-            "mean_iterations_all_attempts": stats[0] / n, "fallback_rate": stats[2] / n,
+            "iteration_ratio_successful_attempt": float(it_plain[ok].mean() / it[ok].mean()),
+            "succeeding_attempt_histogram": {int(a): int((at == a).sum()) for a in np.unique(at)},
+            "fallback_rate": stats[2] / n,
             "status_agreement": float(np.mean(st == st_plain)),
             "guess_error_median": {"u_gas": float(np.median(gerr[ok, 0])), "E_rad": float(np.median(gerr[ok, 1]))},
             "mlp": {"ms": ms_mlp, "achieved_tflops": flop / (ms_mlp / 1e3) / 1e12, "peak_tflops": bf16_peak,
@@ -881,7 +941,7 @@ def our_arm_radcells(args, wl, rank, world, local_rank):
     at = d_at.cpu().numpy()
     peak = ctypes.c_double()
     k._check(L.kgpu_fp64_peak(ctypes.byref(peak)), "kgpu_fp64_peak")
-    learned = learned_leg(k, rp, d_in, work, stream, n, st, it, args, dev)
+    learned = learned_leg(k, rp, d_in, work, stream, n, st, it, stats[0], args, dev)
 
     # e2e: the host-pointer entry point with pinned buffers, copies included
     hin = []
@@ -948,6 +1008,9 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         reference_arm(args, wl, rank)
+        return
+    if args.profile_solve:
+        profile_solve(args)
         return
     if world > 1:
         import datetime

@@ -51,6 +51,7 @@ extern "C" {
 #define KGPU_ARR_P 1
 #define KGPU_ARR_UT0 2
 #define KGPU_ARR_UT1 3
+#define KGPU_ARR_UT2 4   /* RK2's k2 (ko.c:614-615: addi_u(1.,u,-1.,ut1,ut2)) */
 
 /* boundary conditions per axis (set_bc_core finite.c:2673-2748 and the
  * problem plug-ins' calc_bc):
@@ -147,9 +148,25 @@ int kgpu_calc_u2p(kgpu_ctx *ctx);
 int kgpu_set_bc(kgpu_ctx *ctx, double t, int ifinit);
 /* save_timesteps(), finite.c:404-496 (no SELFTIMESTEP: nothing to store). */
 int kgpu_save_timesteps(kgpu_ctx *ctx);
-/* copyi_u(factor,src,dst), finite.c:2492; addi_u(f1,a,f2,b,c), finite.c:2545. */
+/* copyi_u(factor,src,dst), finite.c:2492; addi_u(f1,a,f2,b,c), finite.c:2545;
+ * addi_u_3(f1,a,f2,b,f3,c,d), finite.c:2603: d = f1 a + f2 b + f3 c.  Domain
+ * cells, all NV variables, arrays named by KGPU_ARR_*. */
 int kgpu_copyi_u(kgpu_ctx *ctx, double factor, int src, int dst);
 int kgpu_addi_u(kgpu_ctx *ctx, double f1, int a, double f2, int b, int c);
+int kgpu_addi_u_3(kgpu_ctx *ctx, double f1, int a, double f2, int b, double f3, int c, int d);
+/* do_correct(), finite.c:605: the polar-axis corrections it can run are
+ * compiled only with CORRECT_POLARAXIS(_3D) or SMOOTH_POLARAXIS, which no
+ * configuration of this library defines, so it returns 0; the problem's
+ * my_finger hook stays host code. */
+int kgpu_do_correct(kgpu_ctx *ctx);
+/* flux_ct(), magn.c:199-339: corner EMFs from the face fluxes of the last
+ * op_explicit and the magnetic components of those fluxes rewritten from
+ * them, as the reference leaves flbx/flby/flbz (kgpu_download_flux reads
+ * them).  kgpu_op_explicit applies flux-CT inside its update without
+ * storing the rewritten fluxes; this call stores them.  KGPU_ESTATE when
+ * called twice for one op_explicit (the EMFs need the fluxes before the
+ * rewrite). */
+int kgpu_flux_ct(kgpu_ctx *ctx);
 
 /* Time-step bookkeeping of solve_the_problem (ko.c:290-313, 399-425). ----- */
 /* Initial 1/dt from max_ws = 10000 (ko.c:290-300). */
@@ -338,7 +355,15 @@ int kgpu_rad_default_params(kgpu_rad_params *rp, double mass, double gamma, doub
  *                 cells it still holds to the warp-per-cell kernel when at
  *                 most this many of its 32 lanes hold one (0..32, default 8)
  *  blocks_per_sm  persistent: resident blocks of 128 threads per SM
- *                 (0: as many as the kernel's registers allow) */
+ *                 (0: as many as the kernel's registers allow)
+ *  skip           learned warm start: 1 (default): a warm-started cell
+ *                 begins with the energy-equation attempt the network expects
+ *                 to be the first that succeeds (outputs 5 and 6), skipping
+ *                 those it expects to fail; 2: besides, only the cells the
+ *                 network expects to fail their first attempt start from the
+ *                 prediction, the others from their own guess; 0: every
+ *                 warm-started cell begins with attempt 0.  Every cell still
+ *                 converges to RADIMPCONV or runs the reference cascade */
 typedef struct {
   int pass_iters;
   int inner_cap;
@@ -346,6 +371,7 @@ typedef struct {
   int warm_attempts;
   int thin;
   int blocks_per_sm;
+  int skip;
 } kgpu_rad_solver_opts;
 int kgpu_rad_default_solver_opts(kgpu_rad_solver_opts *opts);
 
@@ -397,19 +423,22 @@ int kgpu_rad_implicit_cells_device_ex(int n, const kgpu_rad_params *rp, const do
                                       int mode, const kgpu_rad_solver_opts *opts, void *work, void *stream,
                                       unsigned long long *stats, int nstats);
 /* Network inputs (float [n][16]) of cells before a solve, and training
- * targets (float [n][5]: ln of the gas and radiation energy ratios, change
- * of the iterated velocity) from the states before and after; NaN where
- * status is not 0.  Device pointers, asynchronous on stream. */
+ * targets (float [n][7]: ln of the gas and radiation energy ratios, change
+ * of the iterated velocity, then 1/0 for "the first attempt failed" and
+ * "the first two attempts failed") from the states before and after and
+ * the attempt that succeeded; the first five NaN where status is not 0.
+ * Device pointers, asynchronous on stream. */
 int kgpu_rad_features_device(int n, const kgpu_rad_params *rp, const double *pp, const double *g, const double *G,
                              const double *dt, float *X, void *stream);
 int kgpu_rad_targets_device(int n, const kgpu_rad_params *rp, const double *pp, const double *pp1,
-                            const double *g, const double *G, const int *status, float *T, void *stream);
+                            const double *g, const double *G, const int *status, const int *attempt, float *T,
+                            void *stream);
 
-/* The warm-start network: 16 -> 128 -> 128 -> 5, SiLU, BF16 weights and
+/* The warm-start network: 16 -> 128 -> 128 -> 7, SiLU, BF16 weights and
  * activations with FP32 accumulation on the tensor cores; trained and run on
  * the device.  The parameter blob (kgpu_mlp_blob_size() floats) holds
- * W1[16][128], b1[128], W2[128][128], b2[128], W3[128][8], b3[8] (outputs
- * 5..7 unused), then the output standardisation mean[8] and scale[8]. */
+ * W1[16][128], b1[128], W2[128][128], b2[128], W3[128][8], b3[8] (output 7
+ * unused), then the output standardisation mean[8] and scale[8]. */
 typedef struct kgpu_mlp kgpu_mlp;
 int kgpu_mlp_blob_size(void);
 int kgpu_mlp_create(kgpu_mlp **mlp, unsigned long long seed);
@@ -441,6 +470,15 @@ int kgpu_rad_u2p_cells(int n, const kgpu_rad_params *rp, const double *uu, doubl
                        const double *G, int *status, int *corrected);
 int kgpu_rad_p2u_cells(int n, const kgpu_rad_params *rp, const double *pp, double *uu, const double *g,
                        const double *G);
+/* The per-cell u2p of the reference with all its outputs (u2p.c:176-485,
+ * type 0): the MHD inversion with its entropy fallback and, when rp is
+ * given (cfg->nv = 13), the M1 inversion u2p_rad.  n cells in KORAL's
+ * cell-major layout with cfg->nv variables; per cell status (u2p's return
+ * value), corrected[3] (hydro corrected, radiation corrected, entropy
+ * balance not applied: always 0 here) and fixups[2] (hydro fixup requested,
+ * radiation fixup requested: DORADFIXUPS).  rp must be null for nv = 9. */
+int kgpu_u2p_cells_full(int n, const kgpu_config *cfg, const kgpu_rad_params *rp, const double *uu, double *pp,
+                        const double *g, const double *G, int *status, int *corrected, int *fixups);
 /* Kerr-Schild metric point (r, theta) of spin a in the 20 + 20 layout
  * (g_{mu nu}, d ln sqrt(-g)/dx^i, sqrt(-g); g^{mu nu}, g_tt + 1).  Host. */
 int kgpu_ks_metric(double a, double r, double th, double *g20, double *G20);
@@ -449,6 +487,12 @@ int kgpu_ks_metric_batch(double a, int n, const double *r, const double *th, dou
  * contraction, as the library's kernels are built): the denominator of the
  * FP64 roofline of the solver kernels. */
 int kgpu_fp64_peak(double *ops_per_s);
+/* The device's powers and logarithm of the hot path on n host values, for
+ * checks against the host C library: kind 0 x^2, 1 x^4, 2 x^-3.5 (the
+ * Planck and Kramers terms), 3 x^y with 4y an integer (the entropy),
+ * 4 log(x), 5 the device library's pow(x, y).  Kinds 0-3 are products and
+ * square roots carried to double-double accuracy and rounded once. */
+int kgpu_eval_powers(int n, int kind, double y, const double *x, double *out);
 
 /* Radiation in the grid step (nv = 13: the nine MHD variables, then E and
  * the radiation frame's relative four-velocity; conserved R^t_t, R^t_i).
@@ -477,6 +521,55 @@ int kgpu_get_implicit_options(kgpu_ctx *ctx, kgpu_rad_solver_opts *opts);
  * reference guess, which the time step's own evolution keeps close);
  * -1 (default): every cell. */
 int kgpu_set_warm_gate(kgpu_ctx *ctx, int iters);
+/* Launch shapes and solver settings of a context.  None changes results:
+ * every choice performs the same arithmetic (the kernels' variants differ
+ * in the registers they are compiled for, the solver settings in how work
+ * is scheduled).
+ *  flux_blocks     blocks of 128 threads per SM the face-flux kernels are
+ *                  compiled for: 5..8 (default 7)
+ *  flux_split      1: the face states are reconstructed by a kernel of
+ *                  their own (one thread per face and variable) and read by
+ *                  the flux kernel; 0 (default): reconstructed inside it
+ *  update_blocks   the same for the update kernel: 3..5 (default 4)
+ *  u2p_blocks      the same for the first inversion pass: 4..6 (default 5)
+ *  u2p_pass_iters  Newton steps of the first inversion pass before a solve
+ *                  is queued for resumption (default 8)
+ *  implicit_mode   solver of op_implicit (KGPU_RAD_*; default batched)
+ *  implicit        its tuning (kgpu_rad_solver_opts) */
+typedef struct {
+  int flux_blocks;
+  int flux_split;
+  int update_blocks;
+  int u2p_blocks;
+  int u2p_pass_iters;
+  int implicit_mode;
+  kgpu_rad_solver_opts implicit;
+} kgpu_tuning;
+int kgpu_get_tuning(kgpu_ctx *ctx, kgpu_tuning *t);
+/* Applies a tuning (drops the captured step graph; the network of the
+ * implicit solver is kept; a plain implicit mode with a network set is
+ * KGPU_EINVAL). */
+int kgpu_set_tuning(kgpu_ctx *ctx, const kgpu_tuning *t);
+/* The autotuner.  Times candidate values of each field of kgpu_tuning, one
+ * field after another (coordinate descent from the current tuning), on
+ * this context's own state: each trial restores the state, runs `steps`
+ * whole time steps (RK2, or RK2IMEX with radiation) from the stream and
+ * times them with CUDA events; the state, the time step and the counters
+ * are restored afterwards, and the choice is applied.  Candidates: the
+ * fused or split face flux, flux 5..8, update 3..5, u2p 4..6 blocks; u2p_pass_iters 4, 8, 16; with
+ * radiation the batched and the persistent solver, pass_iters 4, 8, 16,
+ * inner_cap 32, 64, 128, tail on/off or thin 4, 8, 16.  A candidate
+ * replaces the incumbent only when it is faster by min_gain (a fraction,
+ * e.g. 0.02) in the same round of trials.  The choice is cached per device
+ * and grid configuration for the process: with reuse = 1 a cached choice
+ * is applied without trials.  Outputs (optional): the chosen tuning and
+ * the time per step of the starting and of the chosen tuning (ms[2]). */
+int kgpu_autotune(kgpu_ctx *ctx, int steps, double min_gain, int reuse, kgpu_tuning *chosen, double *ms);
+/* The autotuner's selection rule on its own: index of the fastest of n
+ * timings if it beats timings[incumbent] by the fraction min_gain, else
+ * incumbent.  Negative or non-finite timings (failed trials) never win. */
+int kgpu_tune_select(int n, const double *ms, int incumbent, double min_gain);
+
 /* Whole RK2IMEX steps (ko.c:444-570), dt in device memory; and the same
  * replayed from a CUDA graph captured on the first call. */
 int kgpu_rk2imex_steps(kgpu_ctx *ctx, int nsteps);

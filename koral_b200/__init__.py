@@ -20,7 +20,7 @@ LIB_PATH = os.environ.get("KORAL_B200_LIB") or os.path.join(HERE, "_lib", "libko
 PPM, MP5 = 2, 4
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECT, BC_PERIODIC_COPY = 0, 1, 2, 3
 LAXF, HLL = 0, 1
-ARR_U, ARR_P, ARR_UT0, ARR_UT1 = 0, 1, 2, 3
+ARR_U, ARR_P, ARR_UT0, ARR_UT1, ARR_UT2 = 0, 1, 2, 3, 4
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -38,10 +38,23 @@ class SolverOpts(ctypes.Structure):
     """kgpu_rad_solver_opts (include/koral_b200.h): tuning of the batched and
     persistent implicit solvers."""
     _fields_ = [(n, ctypes.c_int) for n in ("pass_iters", "inner_cap", "tail", "warm_attempts", "thin",
-                                            "blocks_per_sm")]
+                                            "blocks_per_sm", "skip")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class Tuning(ctypes.Structure):
+    """kgpu_tuning (include/koral_b200.h): launch shapes and solver settings
+    of a context."""
+    _fields_ = [("flux_blocks", ctypes.c_int), ("flux_split", ctypes.c_int), ("update_blocks", ctypes.c_int),
+                ("u2p_blocks", ctypes.c_int),
+                ("u2p_pass_iters", ctypes.c_int), ("implicit_mode", ctypes.c_int), ("implicit", SolverOpts)]
+
+    def as_dict(self):
+        d = {n: getattr(self, n) for n, _ in self._fields_ if n != "implicit"}
+        d["implicit"] = self.implicit.as_dict()
+        return d
 
 
 class ScalarsParams(ctypes.Structure):
@@ -170,6 +183,7 @@ def lib():
         L.kgpu_ks_metric.argtypes = [ctypes.c_double] * 3 + [_dp] * 2
         L.kgpu_ks_metric_batch.argtypes = [ctypes.c_double, ctypes.c_int] + [_dp] * 4
         L.kgpu_fp64_peak.argtypes = [_dp]
+        L.kgpu_eval_powers.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp]
         L.kgpu_rad_implicit_cells_warm_device.argtypes = [ctypes.c_int, rpp] + [vp] * 13 + [
             ctypes.POINTER(ctypes.c_ulonglong)]
         sop = ctypes.POINTER(SolverOpts)
@@ -180,8 +194,13 @@ def lib():
         L.kgpu_rad_get_solver_opts.argtypes = [sop]
         L.kgpu_set_implicit_options.argtypes = [vp, sop]
         L.kgpu_get_implicit_options.argtypes = [vp, sop]
+        tup = ctypes.POINTER(Tuning)
+        L.kgpu_get_tuning.argtypes = [vp, tup]
+        L.kgpu_set_tuning.argtypes = [vp, tup]
+        L.kgpu_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, tup, _dp]
+        L.kgpu_tune_select.argtypes = [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_double]
         L.kgpu_rad_features_device.argtypes = [ctypes.c_int, rpp] + [vp] * 6
-        L.kgpu_rad_targets_device.argtypes = [ctypes.c_int, rpp] + [vp] * 7
+        L.kgpu_rad_targets_device.argtypes = [ctypes.c_int, rpp] + [vp] * 8
         fp = ctypes.POINTER(ctypes.c_float)
         L.kgpu_mlp_create.argtypes = [ctypes.POINTER(vp), ctypes.c_ulonglong]
         L.kgpu_mlp_destroy.argtypes = [vp]
@@ -192,6 +211,12 @@ def lib():
         L.kgpu_mlp_train_epoch.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                            ctypes.c_ulonglong, _dp]
         L.kgpu_u2p_cells_static.argtypes = sig["kgpu_u2p_cells"]
+        L.kgpu_u2p_cells_full.argtypes = [ctypes.c_int, ctypes.POINTER(Config), rpp, _dp, _dp, _dp, _dp,
+                                          ip_, ip_, ip_]
+        L.kgpu_addi_u_3.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                    ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        L.kgpu_do_correct.argtypes = [vp]
+        L.kgpu_flux_ct.argtypes = [vp]
         for name, args in (("kgpu_fm_radtorus_state", [ctypes.POINTER(TorusParams), rpp, ctypes.c_double,
                                                         ctypes.POINTER(Config)] + [_dp] * 7),
                            ("kgpu_init_fm_radtorus", [vp, ctypes.POINTER(TorusParams), rpp, ctypes.c_double,
@@ -374,6 +399,17 @@ class Subdomain:
         _check(self.L.kgpu_addi_u(self.h, f1, a, f2, b, c), "kgpu_addi_u")
 
     # time-step bookkeeping
+    def addi_u_3(self, f1, a, f2, b, f3, c, d):
+        _check(self.L.kgpu_addi_u_3(self.h, f1, a, f2, b, f3, c, d), "kgpu_addi_u_3")
+
+    def do_correct(self):
+        _check(self.L.kgpu_do_correct(self.h), "kgpu_do_correct")
+
+    def flux_ct(self):
+        """flux_ct (magn.c:199): stores the rewritten magnetic face fluxes
+        of the last op_explicit (kgpu_flux_ct)."""
+        _check(self.L.kgpu_flux_ct(self.h), "kgpu_flux_ct")
+
     def begin_run(self):
         _check(self.L.kgpu_begin_run(self.h), "kgpu_begin_run")
 
@@ -453,12 +489,12 @@ class Subdomain:
         import torch
         n, b = self.implicit_buffers()
         X = torch.empty((n, 16), dtype=torch.float32, device="cuda")
-        T = torch.empty((n, 5), dtype=torch.float32, device="cuda")
+        T = torch.empty((n, MLP_OUT), dtype=torch.float32, device="cuda")
         vp = ctypes.c_void_p
         _check(self.L.kgpu_rad_features_device(n, ctypes.byref(rp), vp(b["pp_in"]), vp(b["g20"]), vp(b["G20"]),
                                                vp(b["dt"]), _vp(X), _stream()), "kgpu_rad_features_device")
         _check(self.L.kgpu_rad_targets_device(n, ctypes.byref(rp), vp(b["pp_in"]), vp(b["pp_out"]), vp(b["g20"]),
-                                              vp(b["G20"]), vp(b["status"]), _vp(T), _stream()),
+                                              vp(b["G20"]), vp(b["status"]), vp(b["attempt"]), _vp(T), _stream()),
                "kgpu_rad_targets_device")
         return X, T
 
@@ -475,6 +511,24 @@ class Subdomain:
         for k, v in kw.items():
             setattr(o, k, int(v))
         _check(self.L.kgpu_set_implicit_options(self.h, ctypes.byref(o)), "kgpu_set_implicit_options")
+
+    def tuning(self):
+        t = Tuning()
+        _check(self.L.kgpu_get_tuning(self.h, ctypes.byref(t)), "kgpu_get_tuning")
+        return t
+
+    def set_tuning(self, t):
+        _check(self.L.kgpu_set_tuning(self.h, ctypes.byref(t)), "kgpu_set_tuning")
+
+    def autotune(self, steps=2, min_gain=0.02, reuse=False):
+        """kgpu_autotune: times candidate launch shapes and solver settings
+        on this context's state (restored afterwards), applies and returns
+        the choice with the time per step before and after (ms)."""
+        t = Tuning()
+        ms = (ctypes.c_double * 2)()
+        _check(self.L.kgpu_autotune(self.h, int(steps), float(min_gain), int(bool(reuse)), ctypes.byref(t), ms),
+               "kgpu_autotune")
+        return t, (ms[0], ms[1])
 
     def set_warm_gate(self, iters):
         """Warm-start only cells whose previous solve took a later attempt or
@@ -571,6 +625,39 @@ def u2p_cells_static(cfg, uu, pp, g, G):
         msg = L.kgpu_u2p_cells_static_error().decode(errors="replace")
         raise KgpuError(f"kgpu_u2p_cells_static failed with code {rc}: {msg}")
     return pp, st, fx
+
+
+def u2p_cells_full(cfg, uu, pp, g, G, rp=None):
+    """The reference's per-cell u2p with all outputs (kgpu_u2p_cells_full):
+    returns (pp, status, corrected [n][3], fixups [n][2])."""
+    uu, pp, g, G = (np.ascontiguousarray(a, dtype=np.float64) for a in (uu, pp, g, G))
+    n = uu.shape[0]
+    pp = pp.copy()
+    st = np.zeros(n, np.int32)
+    co, fx = np.zeros((n, 3), np.int32), np.zeros((n, 2), np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    _check(lib().kgpu_u2p_cells_full(n, ctypes.byref(cfg), ctypes.byref(rp) if rp is not None else None, _ptr(uu),
+                                     _ptr(pp), _ptr(g), _ptr(G), st.ctypes.data_as(ip), co.ctypes.data_as(ip),
+                                     fx.ctypes.data_as(ip)), "kgpu_u2p_cells_full")
+    return pp, st, co, fx
+
+
+def eval_powers(kind, x, y=0.0):
+    """kgpu_eval_powers on the device: kind 0 x^2, 1 x^4, 2 x^-3.5, 3 x^y
+    (quarter exponents), 4 log, 5 the device library's pow."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    _check(lib().kgpu_eval_powers(len(x), int(kind), float(y), _ptr(x), _ptr(out)), "kgpu_eval_powers")
+    return out
+
+
+def tune_select(ms, incumbent, min_gain=0.02):
+    """The autotuner's selection rule (kgpu_tune_select)."""
+    a = np.ascontiguousarray(ms, dtype=np.float64)
+    r = lib().kgpu_tune_select(len(a), _ptr(a), int(incumbent), float(min_gain))
+    if r < 0:
+        _check(r, "kgpu_tune_select")
+    return r
 
 
 def p2u_cells(cfg, pp, g, G):
@@ -888,11 +975,15 @@ def rad_features_device(rp, pp, g, G, dt):
     return X
 
 
-def rad_targets_device(rp, pp, pp1, g, G, status):
+MLP_OUT = 7   # network outputs: five for the initial iterate, two attempt scores
+
+
+def rad_targets_device(rp, pp, pp1, g, G, status, attempt):
+    """Training targets [n][7] of solved cells (kgpu_rad_targets_device)."""
     import torch
-    T = torch.empty((pp.shape[0], 5), dtype=torch.float32, device=pp.device)
+    T = torch.empty((pp.shape[0], MLP_OUT), dtype=torch.float32, device=pp.device)
     _check(lib().kgpu_rad_targets_device(pp.shape[0], ctypes.byref(rp), _vp(pp), _vp(pp1), _vp(g), _vp(G),
-                                         _vp(status), _vp(T), _stream()), "kgpu_rad_targets_device")
+                                         _vp(status), _vp(attempt), _vp(T), _stream()), "kgpu_rad_targets_device")
     return T
 
 

@@ -23,6 +23,10 @@
 #include <string.h>
 #include <unistd.h>
 
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "../../include/koral_b200.h"
@@ -61,7 +65,7 @@ extern "C" int kgpu_abi_version(void) { return KGPU_ABI_VERSION; }
 // ---------------------------------------------------------------------------
 struct Box {
   int x0, y0, z0, nx, ny, nz;
-  long n() const { return (long)nx * ny * nz; }
+  __host__ __device__ long n() const { return (long)nx * ny * nz; }
 };
 __device__ inline bool box_coord(const Box &b, long t, int &ix, int &iy, int &iz) {
   if (t >= (long)b.nx * b.ny * b.nz) return false;
@@ -419,8 +423,46 @@ __global__ void k_wavespeeds(Grid G, Box b) {
 #ifndef KGPU_U2P_MIN_BLOCKS
 #define KGPU_U2P_MIN_BLOCKS 5
 #endif
+// The face states of direction D (avg2point, finite.c:89-289) on their
+// own: one thread per face of box b and variable, both sides (the left
+// state is the right value of cell i-1, the right state the left value of
+// cell i), stored [variable][face of the box] for k_flux<.., true>.  The
+// same functions and operations as the reconstruction inside k_flux.
 template <int D>
-__global__ void __launch_bounds__(128, KGPU_FLUX_MIN_BLOCKS) k_flux(Grid G, Box b) {
+__global__ void __launch_bounds__(256) k_recon(Grid G, Box b, double *sl, double *sr) {
+  const long nb = b.n();
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= nb * NVMAX) return;
+  const int iv = (int)(t / nb);
+  const long fi = t - (long)iv * nb;
+  int ix, iy, iz;
+  box_coord(b, fi, ix, iy, iz);
+  const int i = D == 0 ? ix : (D == 1 ? iy : iz);
+  const long stride = D == 0 ? 1 : (D == 1 ? (long)G.sx : (long)G.sx * G.sy);
+  const long cR = cell_index(G, ix, iy, iz);
+  const double *pv = G.p + iv * G.ncell + cR;
+  double left, right;
+  if (G.int_order == 4) {
+    left = mp5_face(pv[-3 * stride], pv[-2 * stride], pv[-stride], pv[0], pv[stride]);
+    right = mp5_face(pv[2 * stride], pv[stride], pv[0], pv[-stride], pv[-2 * stride]);
+  } else {
+    double dx[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) dx[k] = size_x(G, i - 3 + k, D);
+    double ul, ur;
+    ppm(pv[-3 * stride], pv[-2 * stride], pv[-stride], pv[0], pv[stride], dx[0], dx[1], dx[2], dx[3], dx[4], ul, ur);
+    left = ur;
+    ppm(pv[-2 * stride], pv[-stride], pv[0], pv[stride], pv[2 * stride], dx[1], dx[2], dx[3], dx[4], dx[5], ul, ur);
+    right = ul;
+  }
+  sl[(long)iv * nb + fi] = left;
+  sr[(long)iv * nb + fi] = right;
+}
+
+// SPLIT: the face states come from k_recon (sl, sr) instead of being
+// reconstructed here; the rest is the same.
+template <int D, int MB = KGPU_FLUX_MIN_BLOCKS, bool SPLIT = false>
+__global__ void __launch_bounds__(128, MB) k_flux(Grid G, Box b, const double *sl, const double *sr) {
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const int side = (int)(t & 1);
   int ix, iy, iz;
@@ -435,7 +477,12 @@ __global__ void __launch_bounds__(128, KGPU_FLUX_MIN_BLOCKS) k_flux(Grid G, Box 
 
   // reconstruction (avg2point, finite.c:89-289) of this lane's side
   double ps[NVMAX];
-  if (G.int_order == 4) {
+  if (SPLIT) {
+    const long nb = b.n(), fi = t >> 1;
+    const double *src = side ? sr : sl;
+#pragma unroll
+    for (int iv = 0; iv < nv; iv++) ps[iv] = src[(long)iv * nb + fi];
+  } else if (G.int_order == 4) {
     // left: MP5 centred on i-1 over cells i-3..i+1; right: centred on i,
     // stencil mirrored, cells i+2..i-2
     const long c0 = side ? cR + 2 * stride : cR - 3 * stride;
@@ -639,7 +686,8 @@ __global__ void k_emf(Grid G, Box b) {
 // unsplit update with metric source terms (finite.c:1062-1160,
 // f_metric_source_term_arb physics.c:324-465)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, KGPU_UPDATE_MIN_BLOCKS) k_update(Grid G, Box b, const double *dtp, double fac,
+template <int MB = KGPU_UPDATE_MIN_BLOCKS>
+__global__ void __launch_bounds__(128, MB) k_update(Grid G, Box b, const double *dtp, double fac,
                                                                         double *save) {
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
@@ -926,7 +974,8 @@ __device__ inline int u2p_run(const Grid &G, int Etype, U2PCell &x, int stop, do
   return u2p_final(G.gamma, st, W, iter, x.uc, x.pp, x.g);
 }
 
-__global__ void __launch_bounds__(128, KGPU_U2P_MIN_BLOCKS) k_u2p(Grid G, Box b, U2PQueues Q, int stop) {
+template <int MB = KGPU_U2P_MIN_BLOCKS>
+__global__ void __launch_bounds__(128, MB) k_u2p(Grid G, Box b, U2PQueues Q, int stop) {
   int ix, iy, iz;
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (!box_coord(b, t, ix, iy, iz)) return;
@@ -1214,17 +1263,64 @@ __global__ void k_begin_step(Grid G) {
   G.scal[S_TSTEPDENMAX] = -1.;
 }
 
+// copyi_u, addi_u, addi_u_3 (finite.c:2492-2620): domain cells, all NV
+// variables, the reference's products and sums in its order
 __global__ void k_copy_domain(Grid G, Box b, double f, const double *src, double *dst) {
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
   long c = cell_index(G, ix, iy, iz);
-  for (int iv = 0; iv < NVMAX; iv++) dst[iv * G.ncell + c] = f * src[iv * G.ncell + c];
+  for (int iv = 0; iv < G.nv; iv++) dst[iv * G.ncell + c] = f * src[iv * G.ncell + c];
 }
 __global__ void k_add_domain(Grid G, Box b, double f1, const double *a, double f2, const double *bb, double *c3) {
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
   long c = cell_index(G, ix, iy, iz);
-  for (int iv = 0; iv < NVMAX; iv++) c3[iv * G.ncell + c] = f1 * a[iv * G.ncell + c] + f2 * bb[iv * G.ncell + c];
+  for (int iv = 0; iv < G.nv; iv++) c3[iv * G.ncell + c] = f1 * a[iv * G.ncell + c] + f2 * bb[iv * G.ncell + c];
+}
+__global__ void k_add3_domain(Grid G, Box b, double f1, const double *a, double f2, const double *bb, double f3,
+                              const double *cc, double *d4) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  long c = cell_index(G, ix, iy, iz);
+  for (int iv = 0; iv < G.nv; iv++) {
+    const long i = iv * G.ncell + c;
+    d4[i] = f1 * a[i] + f2 * bb[i] + f3 * cc[i];
+  }
+}
+
+// The second half of flux_ct (magn.c:297-337): the magnetic components of
+// the face fluxes rewritten from the corner EMFs, over the corner box
+// (loop_4: 0..NX x 0..NY x 0..NZ).  op_explicit applies the same values
+// inside k_update without storing them; this kernel stores them in the
+// face-flux arrays, as the reference leaves its flbx/flby/flbz.
+__global__ void k_flux_ct_rewrite(Grid G, Box b) {
+  int ix, iy, iz;
+  if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  const int NX = G.nx, NY = G.ny, NZ = G.nz;
+  const long ne = (long)(NX + 1) * (NY + 1) * (NZ + 1);
+#define EMFV(comp, a, b2, c2) G.emf[((comp)-1) * ne + emf_index(G, a, b2, c2)]
+  if (NX > 1 && iy < NY && iz < NZ) {
+    double *f = G.flb[0];
+    const long n = G.nface[0], i = face_index(G, ix, iy, iz, 0);
+    f[B1 * n + i] = 0.;
+    f[B2 * n + i] = 0.5 * (EMFV(3, ix, iy, iz) + EMFV(3, ix, iy + 1, iz));
+    f[B3 * n + i] = -0.5 * (EMFV(2, ix, iy, iz) + EMFV(2, ix, iy, iz + 1));
+  }
+  if (NY > 1 && ix < NX && iz < NZ) {
+    double *f = G.flb[1];
+    const long n = G.nface[1], i = face_index(G, ix, iy, iz, 1);
+    f[B1 * n + i] = -0.5 * (EMFV(3, ix, iy, iz) + EMFV(3, ix + 1, iy, iz));
+    f[B2 * n + i] = 0.;
+    f[B3 * n + i] = 0.5 * (EMFV(1, ix, iy, iz) + EMFV(1, ix, iy, iz + 1));
+  }
+  if (NZ > 1 && ix < NX && iy < NY) {
+    double *f = G.flb[2];
+    const long n = G.nface[2], i = face_index(G, ix, iy, iz, 2);
+    f[B1 * n + i] = 0.5 * (EMFV(2, ix, iy, iz) + EMFV(2, ix + 1, iy, iz));
+    f[B2 * n + i] = -0.5 * (EMFV(1, ix, iy, iz) + EMFV(1, ix, iy + 1, iz));
+    f[B3 * n + i] = 0.;
+  }
+#undef EMFV
 }
 
 // KORAL layout [cell][var] <-> device [var][cell]
@@ -1266,13 +1362,14 @@ __global__ void k_fill(double *a, long n, double v) {
 // ---------------------------------------------------------------------------
 enum KernelId { K_BC = 0, K_WAVESPEEDS, K_FLUX0, K_FLUX1, K_FLUX2, K_EMF, K_UPDATE, K_U2P, K_U2P_RESUME,
                 K_U2P_ENT, K_U2P_RESUME_ENT, K_FIXUP, K_COMMIT, K_BEGIN, K_FLUXRAD0, K_FLUXRAD1, K_FLUXRAD2,
-                K_UPDATE_RAD, K_U2P_RAD, K_IMP_GATHER, K_IMP_WARM, K_IMP_SOLVE, K_IMP_SCATTER, K_IMEX, K_NKERNELS };
+                K_UPDATE_RAD, K_U2P_RAD, K_IMP_GATHER, K_IMP_WARM, K_IMP_SOLVE, K_IMP_SCATTER, K_IMEX, K_RECON0,
+                K_RECON1, K_RECON2, K_NKERNELS };
 static const char *kKernelNames[K_NKERNELS] = {"k_bc", "k_wavespeeds", "k_flux_x", "k_flux_y", "k_flux_z", "k_emf",
                                                "k_update", "k_u2p", "k_u2p_resume", "k_u2p_entropy",
                                                "k_u2p_resume_entropy", "k_fixup", "k_commit", "k_begin_step",
                                                "k_flux_rad_x", "k_flux_rad_y", "k_flux_rad_z", "k_update_rad",
                                                "k_u2p_rad", "k_imp_gather", "k_imp_warm_start", "k_imp_solve",
-                                               "k_imp_scatter", "k_imex"};
+                                               "k_imp_scatter", "k_imex", "k_recon_x", "k_recon_y", "k_recon_z"};
 
 int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
                            const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
@@ -1281,6 +1378,52 @@ int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, c
                            const kgpu_rad_solver_opts *opts);
 kgpu::RadParams kgpu_rad_device_params(const kgpu_rad_params &p);
 bool kgpu_rad_opts_valid(const kgpu_rad_solver_opts &o);
+
+// Variants of the face-flux, update and first inversion kernels compiled
+// for different numbers of resident blocks per SM (registers traded
+// against occupancy); the context picks one of each (kgpu_set_tuning,
+// kgpu_autotune).  Every variant performs the same arithmetic.
+template <int D>
+static void launch_flux(int mb, unsigned nb, cudaStream_t st, const Grid &G, Box b) {
+  switch (mb) {
+    case 5: k_flux<D, 5><<<nb, 128, 0, st>>>(G, b, nullptr, nullptr); break;
+    case 6: k_flux<D, 6><<<nb, 128, 0, st>>>(G, b, nullptr, nullptr); break;
+    case 8: k_flux<D, 8><<<nb, 128, 0, st>>>(G, b, nullptr, nullptr); break;
+    default: k_flux<D, 7><<<nb, 128, 0, st>>>(G, b, nullptr, nullptr); break;
+  }
+}
+template <int D>
+static void launch_flux_split(int mb, unsigned nb, cudaStream_t st, const Grid &G, Box b, const double *sl,
+                              const double *sr) {
+  switch (mb) {
+    case 5: k_flux<D, 5, true><<<nb, 128, 0, st>>>(G, b, sl, sr); break;
+    case 6: k_flux<D, 6, true><<<nb, 128, 0, st>>>(G, b, sl, sr); break;
+    case 8: k_flux<D, 8, true><<<nb, 128, 0, st>>>(G, b, sl, sr); break;
+    default: k_flux<D, 7, true><<<nb, 128, 0, st>>>(G, b, sl, sr); break;
+  }
+}
+static void launch_update(int mb, unsigned nb, cudaStream_t st, const Grid &G, Box b, const double *dtp, double fac,
+                          double *save) {
+  switch (mb) {
+    case 3: k_update<3><<<nb, 128, 0, st>>>(G, b, dtp, fac, save); break;
+    case 5: k_update<5><<<nb, 128, 0, st>>>(G, b, dtp, fac, save); break;
+    default: k_update<4><<<nb, 128, 0, st>>>(G, b, dtp, fac, save); break;
+  }
+}
+static void launch_u2p_first(int mb, unsigned nb, cudaStream_t st, const Grid &G, Box b, U2PQueues Q, int stop) {
+  switch (mb) {
+    case 4: k_u2p<4><<<nb, 128, 0, st>>>(G, b, Q, stop); break;
+    case 6: k_u2p<6><<<nb, 128, 0, st>>>(G, b, Q, stop); break;
+    default: k_u2p<5><<<nb, 128, 0, st>>>(G, b, Q, stop); break;
+  }
+}
+static bool tuning_valid(const kgpu_tuning &t) {
+  return t.flux_blocks >= 5 && t.flux_blocks <= 8 && (t.flux_split == 0 || t.flux_split == 1) && t.update_blocks >= 3 && t.update_blocks <= 5 &&
+         t.u2p_blocks >= 4 && t.u2p_blocks <= 6 && t.u2p_pass_iters >= 1 &&
+         (t.implicit_mode == KGPU_RAD_PLAIN || t.implicit_mode == KGPU_RAD_BATCHED ||
+          t.implicit_mode == KGPU_RAD_PERSISTENT) &&
+         kgpu_rad_opts_valid(t.implicit);
+}
 
 struct ProfRec {
   int id;
@@ -1300,9 +1443,14 @@ struct kgpu_ctx {
   cudaStream_t stream;
   std::vector<void *> allocs;
   double *stage;        // AoS staging for uploads / downloads
+  double *ut2 = nullptr; // RK2's k2 array of the per-operator loop (KGPU_ARR_UT2)
+  bool flux_ct_done = false;  // the face fluxes already hold flux_ct's rewrite
   int *fixmark;
   U2PQueues u2pq;                // work queues of the inversion passes
   int u2p_pass_iters = 8;        // Newton steps before a solve is queued for resumption
+  int flux_blocks = KGPU_FLUX_MIN_BLOCKS, update_blocks = KGPU_UPDATE_MIN_BLOCKS, u2p_blocks = KGPU_U2P_MIN_BLOCKS;
+  int flux_split = 0;            // face states by k_recon, then the flux kernel reads them
+  double *fsl = nullptr, *fsr = nullptr;   // face states of one direction [NVMAX][faces of its box]
   int sm_count;
   double *rhofl_c = nullptr, *rhofl_f = nullptr;
   double min_dx, min_dy, min_dz;
@@ -1466,9 +1614,15 @@ extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
     }                                            \
     ptr = (decltype(ptr))p;                      \
   } while (0)
-  AL(G.u, ncv * d8); AL(G.p, ncv * d8); AL(G.ut0, ncv * d8); AL(G.ut1, ncv * d8);
+  AL(G.u, ncv * d8); AL(G.p, ncv * d8); AL(G.ut0, ncv * d8); AL(G.ut1, ncv * d8); AL(c->ut2, ncv * d8);
   AL(G.pfix, ncv * d8); AL(G.ufix, ncv * d8); AL(c->stage, ncv * d8);
   int n[3] = {G.nx, G.ny, G.nz};
+  {
+    long fmax = G.nface[0] > G.nface[1] ? G.nface[0] : G.nface[1];
+    if (G.nface[2] > fmax) fmax = G.nface[2];
+    AL(c->fsl, fmax * NVMAX * d8);
+    AL(c->fsr, fmax * NVMAX * d8);
+  }
   for (int d = 0; d < 3; d++) {
     double *xb;
     AL(xb, (n[d] + 1 + 2 * G.ng) * d8);
@@ -1691,6 +1845,7 @@ static double *arr_ptr(kgpu_ctx *c, int which) {
     case KGPU_ARR_P: return c->G.p;
     case KGPU_ARR_UT0: return c->G.ut0;
     case KGPU_ARR_UT1: return c->G.ut1;
+    case KGPU_ARR_UT2: return c->ut2;
     default: return nullptr;
   }
 }
@@ -1868,6 +2023,7 @@ static int launch_bc(kgpu_ctx *c) {
 
 static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *save) {
   Grid &G = c->G;
+  c->flux_ct_done = false;
   const int lim = G.int_order == 4 ? 2 : 1;
   int lx = G.nx > 1 ? lim : 0, ly = G.ny > 1 ? lim : 0, lz = G.nz > 1 ? lim : 0;
   Box wb{-lx, -ly, -lz, G.nx + 2 * lx, G.ny + 2 * ly, G.nz + 2 * lz};
@@ -1878,7 +2034,16 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
   int ex0 = -1, enx = G.nx + 2;
   if (G.nx > 1) {
     Box b{0, ey0, ez0, G.nx + 1, eny, enz};
-    { LaunchScope ls(c, K_FLUX0); k_flux<0><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b); }
+    if (c->flux_split) {
+      { LaunchScope ls(c, K_RECON0);
+        k_recon<0><<<nblocks(b.n() * NVMAX, 256), 256, 0, c->stream>>>(G, b, c->fsl, c->fsr); }
+      CKL("k_recon<0>");
+      LaunchScope ls(c, K_FLUX0);
+      launch_flux_split<0>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b, c->fsl, c->fsr);
+    } else {
+      LaunchScope ls(c, K_FLUX0);
+      launch_flux<0>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b);
+    }
     CKL("k_flux<0>");
     if (G.rad) {
       LaunchScope ls(c, K_FLUXRAD0);
@@ -1888,7 +2053,16 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
   }
   if (G.ny > 1) {
     Box b{ex0, 0, ez0, enx, G.ny + 1, enz};
-    { LaunchScope ls(c, K_FLUX1); k_flux<1><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b); }
+    if (c->flux_split) {
+      { LaunchScope ls(c, K_RECON1);
+        k_recon<1><<<nblocks(b.n() * NVMAX, 256), 256, 0, c->stream>>>(G, b, c->fsl, c->fsr); }
+      CKL("k_recon<1>");
+      LaunchScope ls(c, K_FLUX1);
+      launch_flux_split<1>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b, c->fsl, c->fsr);
+    } else {
+      LaunchScope ls(c, K_FLUX1);
+      launch_flux<1>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b);
+    }
     CKL("k_flux<1>");
     if (G.rad) {
       LaunchScope ls(c, K_FLUXRAD1);
@@ -1898,7 +2072,16 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
   }
   if (G.nz > 1) {
     Box b{ex0, ey0, 0, enx, eny, G.nz + 1};
-    { LaunchScope ls(c, K_FLUX2); k_flux<2><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b); }
+    if (c->flux_split) {
+      { LaunchScope ls(c, K_RECON2);
+        k_recon<2><<<nblocks(b.n() * NVMAX, 256), 256, 0, c->stream>>>(G, b, c->fsl, c->fsr); }
+      CKL("k_recon<2>");
+      LaunchScope ls(c, K_FLUX2);
+      launch_flux_split<2>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b, c->fsl, c->fsr);
+    } else {
+      LaunchScope ls(c, K_FLUX2);
+      launch_flux<2>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b);
+    }
     CKL("k_flux<2>");
     if (G.rad) {
       LaunchScope ls(c, K_FLUXRAD2);
@@ -1910,7 +2093,7 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
   { LaunchScope ls(c, K_EMF); k_emf<<<nblocks(eb.n(), 128), 128, 0, c->stream>>>(G, eb); }
   CKL("k_emf");
   Box db = domain_box(G);
-  { LaunchScope ls(c, K_UPDATE); k_update<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, dtp, fac, save); }
+  { LaunchScope ls(c, K_UPDATE); launch_update(c->update_blocks, nblocks(db.n(), 128), c->stream, G, db, dtp, fac, save); }
   CKL("k_update");
   if (G.rad) {
     { LaunchScope ls(c, K_UPDATE_RAD); k_update_rad<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, dtp, fac); }
@@ -1923,7 +2106,7 @@ static int launch_u2p(kgpu_ctx *c, int combine) {
   Grid &G = c->G;
   Box db = domain_box(G);
   const int sweep = c->sm_count * 4;   // grid of the queue passes (grid-stride loops)
-  { LaunchScope ls(c, K_U2P); k_u2p<<<nblocks(db.n(), 128), 128, 0, c->stream>>>(G, db, c->u2pq, c->u2p_pass_iters); }
+  { LaunchScope ls(c, K_U2P); launch_u2p_first(c->u2p_blocks, nblocks(db.n(), 128), c->stream, G, db, c->u2pq, c->u2p_pass_iters); }
   CKL("k_u2p");
   { LaunchScope ls(c, K_U2P_RESUME); k_u2p_resume<<<sweep, 128, 0, c->stream>>>(G, db, c->u2pq, 0); }
   CKL("k_u2p_resume");
@@ -2002,6 +2185,37 @@ extern "C" int kgpu_addi_u(kgpu_ctx *c, double f1, int a, double f2, int b, int 
   Box db = domain_box(c->G);
   k_add_domain<<<nblocks(db.n(), 256), 256, 0, c->stream>>>(c->G, db, f1, pa, f2, pb, pc);
   CKL("k_add_domain");
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_addi_u_3(kgpu_ctx *c, double f1, int a, double f2, int b, double f3, int cc, int d) {
+  if (!c) return KGPU_EINVAL;
+  double *pa = arr_ptr(c, a), *pb = arr_ptr(c, b), *pc = arr_ptr(c, cc), *pd = arr_ptr(c, d);
+  if (!pa || !pb || !pc || !pd) return KGPU_EINVAL;
+  Box db = domain_box(c->G);
+  k_add3_domain<<<nblocks(db.n(), 256), 256, 0, c->stream>>>(c->G, db, f1, pa, f2, pb, f3, pc, pd);
+  CKL("k_add3_domain");
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+// do_correct (finite.c:605-640): the polar-axis corrections it runs exist
+// only with CORRECT_POLARAXIS / CORRECT_POLARAXIS_3D / SMOOTH_POLARAXIS,
+// which the configurations this library runs do not define; the problem's
+// my_finger hook is host code and stays on the host.
+extern "C" int kgpu_do_correct(kgpu_ctx *c) { return c ? 0 : KGPU_EINVAL; }
+
+extern "C" int kgpu_flux_ct(kgpu_ctx *c) {
+  if (!c) return KGPU_EINVAL;
+  if (c->flux_ct_done) return KGPU_ESTATE;   // the EMFs come from the fluxes before the rewrite
+  Grid &G = c->G;
+  Box eb{0, 0, 0, G.nx + 1, G.ny + 1, G.nz + 1};
+  k_emf<<<nblocks(eb.n(), 128), 128, 0, c->stream>>>(G, eb);
+  CKL("k_emf");
+  k_flux_ct_rewrite<<<nblocks(eb.n(), 128), 128, 0, c->stream>>>(G, eb);
+  CKL("k_flux_ct_rewrite");
+  c->flux_ct_done = true;
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
@@ -2312,6 +2526,209 @@ extern "C" int kgpu_rk2imex_steps_graph(kgpu_ctx *c, int nsteps) {
   return run_graph(c, nsteps, 1, enqueue_rk2imex);
 }
 
+// ---------------------------------------------------------------------------
+// tuning and the autotuner
+// ---------------------------------------------------------------------------
+extern "C" int kgpu_get_tuning(kgpu_ctx *c, kgpu_tuning *t) {
+  if (!c || !t) return KGPU_EINVAL;
+  t->flux_blocks = c->flux_blocks;
+  t->flux_split = c->flux_split;
+  t->update_blocks = c->update_blocks;
+  t->u2p_blocks = c->u2p_blocks;
+  t->u2p_pass_iters = c->u2p_pass_iters;
+  t->implicit_mode = c->imp_mode;
+  t->implicit = c->imp_opts;
+  return 0;
+}
+
+extern "C" int kgpu_set_tuning(kgpu_ctx *c, const kgpu_tuning *t) {
+  if (!c || !t || !tuning_valid(*t)) return KGPU_EINVAL;
+  if (c->warm && t->implicit_mode == KGPU_RAD_PLAIN) return KGPU_EINVAL;
+  c->flux_blocks = t->flux_blocks;
+  c->flux_split = t->flux_split;
+  c->update_blocks = t->update_blocks;
+  c->u2p_blocks = t->u2p_blocks;
+  c->u2p_pass_iters = t->u2p_pass_iters;
+  c->imp_mode = t->implicit_mode;
+  c->imp_opts = t->implicit;
+  drop_graph(c);
+  return 0;
+}
+
+extern "C" int kgpu_tune_select(int n, const double *ms, int incumbent, double min_gain) {
+  if (n < 1 || !ms || incumbent < 0 || incumbent >= n || !(min_gain >= 0.)) return KGPU_EINVAL;
+  int best = -1;
+  for (int i = 0; i < n; i++)
+    if (std::isfinite(ms[i]) && ms[i] >= 0. && (best < 0 || ms[i] < ms[best])) best = i;
+  if (best < 0 || best == incumbent) return incumbent;
+  const double inc = ms[incumbent];
+  if (!(std::isfinite(inc) && inc >= 0.)) return best;   // the incumbent's trial failed
+  return ms[best] < inc * (1. - min_gain) ? best : incumbent;
+}
+
+namespace {
+struct DevMemRaii {
+  void *p = nullptr;
+  ~DevMemRaii() {
+    if (p) cudaFree(p);
+  }
+};
+struct TuneKey {
+  int dev, nx, ny, nz, nv, int_order, fluxmethod, rad;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(dev, nx, ny, nz, nv, int_order, fluxmethod, rad) <
+           std::tie(o.dev, o.nx, o.ny, o.nz, o.nv, o.int_order, o.fluxmethod, o.rad);
+  }
+};
+std::map<TuneKey, kgpu_tuning> g_tuned;   // choices of this process
+std::mutex g_tuned_mutex;
+
+// One knob of kgpu_tuning: candidate values and access to the field.
+struct Knob {
+  int *(*field)(kgpu_tuning &);
+  std::vector<int> values;
+};
+}  // namespace
+
+// time per step (ms) of `steps` steps from the saved state under tuning t;
+// a negative value when a step fails
+static double tune_trial(kgpu_ctx *c, const kgpu_tuning &t, int steps, const double *u0, const double *p0,
+                         double tsd, cudaEvent_t ea, cudaEvent_t eb) {
+  if (kgpu_set_tuning(c, &t)) return -1.;
+  Grid &G = c->G;
+  const size_t bytes = (size_t)G.ncell * G.nv * sizeof(double);
+  if (cudaMemcpyAsync(G.u, u0, bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess) return -1.;
+  if (cudaMemcpyAsync(G.p, p0, bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess) return -1.;
+  if (cudaMemcpyAsync(G.scal + S_TSTEPDENMAX, &tsd, sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    return -1.;
+  if (cudaEventRecord(ea, c->stream) != cudaSuccess) return -1.;
+  for (int i = 0; i < steps; i++)
+    if ((G.rad ? enqueue_rk2imex(c) : enqueue_rk2(c)) != 0) return -1.;
+  if (cudaEventRecord(eb, c->stream) != cudaSuccess) return -1.;
+  if (cudaEventSynchronize(eb) != cudaSuccess) return -1.;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ea, eb) != cudaSuccess) return -1.;
+  return (double)ms / steps;
+}
+
+extern "C" int kgpu_autotune(kgpu_ctx *c, int steps, double min_gain, int reuse, kgpu_tuning *chosen, double *ms_out) {
+  if (!c || steps < 1 || !(min_gain >= 0.)) return KGPU_EINVAL;
+  int r = c->G.rad ? ready_rad(c) : ready(c);
+  if (r) return r;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  const kgpu_config &k = c->cfg;
+  const TuneKey key{dev, k.nx, k.ny, k.nz, k.nv, k.int_order, k.fluxmethod, c->G.rad};
+  kgpu_tuning cur;
+  kgpu_get_tuning(c, &cur);
+  if (reuse) {
+    std::lock_guard<std::mutex> lock(g_tuned_mutex);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      kgpu_tuning t = it->second;
+      t.implicit.warm_attempts = cur.implicit.warm_attempts;   // a choice of the caller, not of the tuner
+      if (c->warm && t.implicit_mode == KGPU_RAD_PLAIN) t.implicit_mode = cur.implicit_mode;
+      if ((r = kgpu_set_tuning(c, &t))) return r;
+      if (chosen) *chosen = t;
+      if (ms_out) ms_out[0] = ms_out[1] = -1.;
+      return 0;
+    }
+  }
+  // the state the trials start from, and what the trials change besides it
+  Grid &G = c->G;
+  const size_t bytes = (size_t)G.ncell * G.nv * sizeof(double);
+  DevMemRaii save_u, save_p;
+  CK(cudaMalloc(&save_u.p, bytes));
+  CK(cudaMalloc(&save_p.p, bytes));
+  CK(cudaMemcpyAsync(save_u.p, G.u, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(save_p.p, G.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  double tsd = 0.;
+  unsigned long long cnt[C_NCNT];
+  CK(cudaMemcpyAsync(&tsd, G.scal + S_TSTEPDENMAX, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(cnt, G.cnt, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const bool prof = c->profiling;
+  c->profiling = false;
+  const long long launches = c->launches;
+  cudaEvent_t ea, eb;
+  CK(cudaEventCreate(&ea));
+  CK(cudaEventCreate(&eb));
+  std::vector<Knob> knobs = {
+      {[](kgpu_tuning &t) { return &t.flux_split; }, {0, 1}},
+      {[](kgpu_tuning &t) { return &t.flux_blocks; }, {5, 6, 7, 8}},
+      {[](kgpu_tuning &t) { return &t.update_blocks; }, {3, 4, 5}},
+      {[](kgpu_tuning &t) { return &t.u2p_blocks; }, {4, 5, 6}},
+      {[](kgpu_tuning &t) { return &t.u2p_pass_iters; }, {4, 8, 16}},
+  };
+  if (G.rad) {
+    knobs.push_back({[](kgpu_tuning &t) { return &t.implicit_mode; }, {KGPU_RAD_BATCHED, KGPU_RAD_PERSISTENT}});
+    knobs.push_back({[](kgpu_tuning &t) { return &t.implicit.inner_cap; }, {32, 64, 128}});
+  }
+  kgpu_tuning best = cur;
+  if (best.implicit_mode == KGPU_RAD_PLAIN && G.rad && !c->warm) best.implicit_mode = KGPU_RAD_BATCHED;
+  const double ms_start = tune_trial(c, cur, steps, (const double *)save_u.p, (const double *)save_p.p, tsd, ea, eb);
+  double ms_best = ms_start;
+  int status = 0;
+  for (size_t ki = 0; ki < knobs.size() && !status; ki++) {
+    std::vector<Knob> round = {knobs[ki]};
+    // the settings that belong to the solver form just chosen
+    if (G.rad && knobs[ki].field(best) == &best.implicit.inner_cap) {
+      if (best.implicit_mode == KGPU_RAD_BATCHED) {
+        round.push_back({[](kgpu_tuning &t) { return &t.implicit.pass_iters; }, {4, 8, 16}});
+        round.push_back({[](kgpu_tuning &t) { return &t.implicit.tail; }, {0, 1}});
+      } else {
+        round.push_back({[](kgpu_tuning &t) { return &t.implicit.thin; }, {4, 8, 16}});
+      }
+    }
+    for (const Knob &kn : round) {
+      std::vector<double> ms;
+      int inc = -1;
+      for (size_t i = 0; i < kn.values.size(); i++) {
+        kgpu_tuning t = best;
+        *kn.field(t) = kn.values[i];
+        if (*kn.field(t) == *kn.field(best)) inc = (int)i;
+        ms.push_back(tune_trial(c, t, steps, (const double *)save_u.p, (const double *)save_p.p, tsd, ea, eb));
+      }
+      if (inc < 0) {   // the incumbent value is not a candidate: time it as one more
+        ms.push_back(tune_trial(c, best, steps, (const double *)save_u.p, (const double *)save_p.p, tsd, ea, eb));
+        inc = (int)ms.size() - 1;
+      }
+      const int pick = kgpu_tune_select((int)ms.size(), ms.data(), inc, min_gain);
+      if (pick < 0) { status = KGPU_EINVAL; break; }
+      if (pick != inc) {
+        *kn.field(best) = kn.values[pick];
+        ms_best = ms[pick];
+      } else {
+        ms_best = ms[inc];
+      }
+    }
+  }
+  cudaEventDestroy(ea);
+  cudaEventDestroy(eb);
+  // back to the saved state with the choice applied
+  int r2 = kgpu_set_tuning(c, &best);
+  CK(cudaMemcpyAsync(G.u, save_u.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(G.p, save_p.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(G.scal + S_TSTEPDENMAX, &tsd, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(G.cnt, cnt, sizeof(cnt), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->profiling = prof;
+  c->launches = launches;
+  if (status) return status;
+  if (r2) return r2;
+  if (ms_start < 0. || ms_best < 0.) return set_err("kgpu_autotune: a trial step failed", cudaErrorUnknown);
+  {
+    std::lock_guard<std::mutex> lock(g_tuned_mutex);
+    g_tuned[key] = best;
+  }
+  if (chosen) *chosen = best;
+  if (ms_out) {
+    ms_out[0] = ms_start;
+    ms_out[1] = ms_best;
+  }
+  return 0;
+}
+
 extern "C" int kgpu_get_counters(kgpu_ctx *c, unsigned long long out[4]) {
   if (!c || !out) return KGPU_EINVAL;
   unsigned long long h[C_NCNT];
@@ -2466,6 +2883,65 @@ extern "C" int kgpu_u2p_cells(int n, const kgpu_config *cfg, const double *uu, d
   CK(cudaMemcpy(fixup, df.p, n * 4, cudaMemcpyDeviceToHost));
   for (int i = 0; i < n; i++)
     for (int k = 0; k < G.nv; k++) pp[(size_t)i * G.nv + k] = sp[(size_t)k * n + i];
+  return 0;
+}
+
+// u2p (u2p.c:176-485) with all its outputs on cells in KORAL's cell-major
+// layout: the MHD inversion, then (with radiation) u2p_rad, and the
+// corrected/fixups flags as the reference sets them
+__global__ void k_u2p_cells_full(Grid G, RadParams R, int hasrad, int n, const double *uu, double *pp,
+                                 const double *g20, const double *G20, int *status, int *corrected, int *fixups) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  RadGeom rg;
+  rad_geom(g20 + 20L * i, G20 + 20L * i, rg);
+  const int nv = G.nv;
+  double u[NVR], p[NVR];
+  for (int iv = 0; iv < nv; iv++) {
+    u[iv] = uu[(long)i * nv + iv];
+    p[iv] = pp[(long)i * nv + iv];
+  }
+  int fix = 0;
+  const int ret = u2p(G, u, p, rg.g, fix);
+  int radcor = 0;
+  if (hasrad) u2p_rad(R, u, p, rg, radcor);
+  for (int iv = 0; iv < nv; iv++) pp[(long)i * nv + iv] = p[iv];
+  status[i] = ret;
+  corrected[3L * i + 0] = ret < 0 ? 1 : 0;
+  corrected[3L * i + 1] = radcor > 0 ? 1 : 0;
+  corrected[3L * i + 2] = 0;
+  fixups[2L * i + 0] = fix;
+  fixups[2L * i + 1] = radcor > 0 ? 1 : 0;
+}
+
+extern "C" int kgpu_u2p_cells_full(int n, const kgpu_config *cfg, const kgpu_rad_params *rp, const double *uu,
+                                   double *pp, const double *g, const double *Gi, int *status, int *corrected,
+                                   int *fixups) {
+  if (n < 0 || !cfg || (n > 0 && (!uu || !pp || !g || !Gi || !status || !corrected || !fixups))) return KGPU_EINVAL;
+  if (!((cfg->nv == 9 && !rp) || (cfg->nv == NVR && rp))) return KGPU_EINVAL;
+  if (rp && !(rp->gamma == cfg->gamma)) return KGPU_EINVAL;
+  if (n == 0) return 0;
+  Grid G;
+  fill_grid_params(G, *cfg);
+  RadParams R;
+  memset(&R, 0, sizeof(R));
+  if (rp) R = kgpu_rad_device_params(*rp);
+  const size_t bs = (size_t)n * cfg->nv * 8, bm = (size_t)n * 20 * 8;
+  DevBuf du, dp, dg, dG, ds, dc, df;
+  CK(cudaMalloc(&du.p, bs)); CK(cudaMalloc(&dp.p, bs)); CK(cudaMalloc(&dg.p, bm)); CK(cudaMalloc(&dG.p, bm));
+  CK(cudaMalloc(&ds.p, (size_t)n * 4)); CK(cudaMalloc(&dc.p, (size_t)n * 12)); CK(cudaMalloc(&df.p, (size_t)n * 8));
+  CK(cudaMemcpy(du.p, uu, bs, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dp.p, pp, bs, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dg.p, g, bm, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dG.p, Gi, bm, cudaMemcpyHostToDevice));
+  k_u2p_cells_full<<<nblocks(n, 128), 128>>>(G, R, rp ? 1 : 0, n, (const double *)du.p, (double *)dp.p,
+                                             (const double *)dg.p, (const double *)dG.p, (int *)ds.p, (int *)dc.p,
+                                             (int *)df.p);
+  CKL("k_u2p_cells_full");
+  CK(cudaMemcpy(pp, dp.p, bs, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(status, ds.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(corrected, dc.p, (size_t)n * 12, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(fixups, df.p, (size_t)n * 8, cudaMemcpyDeviceToHost));
   return 0;
 }
 

@@ -11,19 +11,24 @@
 //   11 lapse                       12  g_tt + 1
 //   13 log10 sqrt(g_33) / 2        14  1 when the cascade starts on gas primitives, else 0
 //   15 log10(E_rad / u_gas) / 6
-// Outputs, the change from the state before the solve to the converged one:
+// Outputs 0-4, the change from the state before the solve to the converged
+// one:
 //   0  ln(u_gas' / u_gas)          1  ln(E_rad' / E_rad)
 //   2-4  change of the velocity the first attempt iterates (the gas's when
 //        it works on gas primitives, the radiation frame's otherwise),
 //        x sqrt(g_ii)
-// Each output is standardised with a mean and a scale kept with the weights.
+// and two scores of how the cascade goes (trained on 0/1 targets):
+//   5  the first attempt fails     6  the first two attempts fail
+// Each output is standardised with a mean and a scale kept with the weights
+// (the scores with mean 0 and scale 1).
 #pragma once
 
 #include "kgpu_rad.cuh"
 
 namespace kgpu {
 
-constexpr int MLP_IN = 16, MLP_H = 128, MLP_OUT = 5, MLP_OUTP = 8;
+constexpr int MLP_IN = 16, MLP_H = 128, MLP_OUT = 7, MLP_OUTP = 8;
+constexpr int MLP_NREG = 5;   // outputs that build the initial iterate
 
 KG_HD double mlp_safe_log10(double x) { return log10(x > 1e-300 ? x : 1e-300); }
 
@@ -48,16 +53,30 @@ KG_HD void mlp_features(const RadParams &R, const double *pp, const RadGeom &rg,
 }
 
 // raw (unstandardised) targets from the state before and after the solve
-KG_HD void mlp_targets(const double *pp0, const double *pp1, const RadGeom &rg, int startwith, double t[MLP_OUT]) {
+// and the attempt that succeeded (-1: none)
+KG_HD void mlp_targets(const double *pp0, const double *pp1, const RadGeom &rg, int startwith, int attempt,
+                       double t[MLP_OUT]) {
   const auto &gg = rg.g.gg;
   t[0] = log(pp1[UU] / pp0[UU]);
   t[1] = log(pp1[EE0] / pp0[EE0]);
   const int v = startwith == IMP_MHD ? VX : FX0;
   for (int i = 0; i < 3; i++) t[2 + i] = (pp1[v + i] - pp0[v + i]) * sqrt(gg[i + 1][i + 1]);
+  t[5] = attempt != 0 ? 1. : 0.;
+  t[6] = (attempt < 0 || attempt >= 2) ? 1. : 0.;
+}
+
+// The attempt a warm-started cascade begins with: the energy-equation
+// attempts the network expects to fail are skipped (all four solve the
+// same equation to the same tolerance; the entropy attempts are never
+// skipped to)
+KG_HD int mlp_first_attempt(const double t[MLP_OUT]) {
+  if (t[6] > 0.5) return 2;
+  if (t[5] > 0.5) return 1;
+  return 0;
 }
 
 // initial iterate from the (unstandardised) prediction
-KG_HD void mlp_guess(const double *pp0, const RadGeom &rg, int startwith, const double t[MLP_OUT], double *guess) {
+KG_HD void mlp_guess(const double *pp0, const RadGeom &rg, int startwith, const double t[MLP_NREG], double *guess) {
   const auto &gg = rg.g.gg;
   for (int i = 0; i < NVR; i++) guess[i] = pp0[i];
   guess[UU] = pp0[UU] * exp(t[0]);

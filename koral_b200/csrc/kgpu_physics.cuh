@@ -11,6 +11,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "kgpu_math.cuh"
+
 namespace kgpu {
 
 #define KG_HD __host__ __device__ inline

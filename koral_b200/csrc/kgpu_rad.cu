@@ -71,6 +71,7 @@ struct Opts {
   int warm_attempts = IMP_NATTEMPTS;
   int thin = 8;             // persistent: hand-off threshold of live lanes once the list is empty
   int blocks_per_sm = 0;    // persistent: resident blocks per SM (0: occupancy limit)
+  int skip = 1;             // warm start: begin with the attempt the network expects to succeed
 };
 Opts g_opts;   // the context-free entry points' values
 
@@ -82,6 +83,7 @@ Opts from_api(const kgpu_rad_solver_opts &o) {
   r.warm_attempts = o.warm_attempts;
   r.thin = o.thin;
   r.blocks_per_sm = o.blocks_per_sm;
+  r.skip = o.skip;
   return r;
 }
 kgpu_rad_solver_opts to_api(const Opts &o) {
@@ -92,12 +94,13 @@ kgpu_rad_solver_opts to_api(const Opts &o) {
   r.warm_attempts = o.warm_attempts;
   r.thin = o.thin;
   r.blocks_per_sm = o.blocks_per_sm;
+  r.skip = o.skip;
   return r;
 }
 bool opts_valid(const kgpu_rad_solver_opts &o) {
   return o.pass_iters >= 1 && o.inner_cap >= 0 && (o.tail == 0 || o.tail == 1) && o.warm_attempts >= 1 &&
          o.warm_attempts <= IMP_NATTEMPTS && o.thin >= 0 && o.thin <= 32 && o.blocks_per_sm >= 0 &&
-         o.blocks_per_sm <= 16;
+         o.blocks_per_sm <= 16 && o.skip >= 0 && o.skip <= 2;
 }
 
 // upper bound of the passes a cell can need: six attempts of at most
@@ -247,21 +250,31 @@ __global__ void __launch_bounds__(128, KGPU_RAD_MIN_BLOCKS) k_rad_plain(RadParam
 // gate >= 0: only cells whose previous solve (the attempt and iteration
 // outputs, read before this solve overwrites them) needed a later attempt
 // or more than gate Newton iterations start from the prediction
-__global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypred, int gate) {
+// skip 1: a warm-started cell begins with the attempt the network expects
+// to be the first that succeeds (mlp_first_attempt) instead of the first
+// one; skip 2: besides, only the cells the network expects to fail their
+// first attempt start from the prediction, the others from their own guess
+__global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypred, int gate, int skip) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   RadGeom rg;
   rad_geom(C.g + 20L * k, C.G + 20L * k, rg);
   const double *p0 = C.pp + (long)k * NVR;
   const int sw = imp_startwith(R, p0, rg.g);
+  int first = 0;
   W.wsw[k] = sw;
-  W.watt[k] = 0;
   W.wit[k] = 0;
-  if (ypred && (gate < 0 || C.attempt[k] != 0 || C.iters[k] > gate)) {
-    // learned warm start: the first attempt begins at the predicted state
-    double t[MLP_OUT], guess[NVR];
+  double t[MLP_OUT];
+  bool warm = ypred && (gate < 0 || C.attempt[k] != 0 || C.iters[k] > gate);
+  if (warm) {
     for (int o = 0; o < MLP_OUT; o++) t[o] = ypred[(long)k * MLP_OUTP + o];
+    if (skip == 2 && mlp_first_attempt(t) == 0) warm = false;
+  }
+  if (warm) {
+    // learned warm start: the first attempt begins at the predicted state
+    double guess[NVR];
     mlp_guess(p0, rg, sw, t, guess);
+    if (skip) first = mlp_first_attempt(t);
     for (int i = 0; i < NVR; i++) {
       W.wpp[(long)k * NVR + i] = guess[i];
       W.wguess[(long)k * NVR + i] = guess[i];
@@ -271,9 +284,10 @@ __global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypr
     for (int i = 0; i < NVR; i++) W.wpp[(long)k * NVR + i] = p0[i];
     W.wwarm[k] = 0;
   }
+  W.watt[k] = first;
   // the queue is chosen by the predicate, never by the pointer: every lane
   // of a warp-aggregated push must name the same queue
-  const int type = imp_attempt(0, sw).prim;
+  const int type = imp_attempt(first, sw).prim;
   warp_push(W.q[0][0], W.count + 0, type == 0, k);
   warp_push(W.q[0][1], W.count + 1, type == 1, k);
 }
@@ -902,7 +916,7 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
   RCK(cudaMemsetAsync(W.ctl, 0, 4 * sizeof(unsigned), st));
   if (acc) W.stats = acc;
   else RCK(cudaMemsetAsync(W.stats, 0, 8 * sizeof(unsigned long long), st));
-  k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n, ypred, gate);
+  k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n, ypred, gate, o.skip);
   RCK(cudaGetLastError());
   if (mode == KGPU_RAD_PERSISTENT) {
     const int grid = sm_count() * persist_blocks_per_sm(o);
@@ -997,14 +1011,14 @@ __global__ void k_rad_features(RadParams R, int n, const double *pp, const doubl
 // training targets (float [n][5]) from the states before and after a solve;
 // cells whose solve failed get NaN
 __global__ void k_rad_targets(RadParams R, int n, const double *pp, const double *pp1, const double *g,
-                              const double *G, const int *status, float *T) {
+                              const double *G, const int *status, const int *attempt, float *T) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   RadGeom rg;
   rad_geom(g + 20L * k, G + 20L * k, rg);
   const double *p0 = pp + (long)k * NVR;
   double t[MLP_OUT];
-  mlp_targets(p0, pp1 + (long)k * NVR, rg, imp_startwith(R, p0, rg.g), t);
+  mlp_targets(p0, pp1 + (long)k * NVR, rg, imp_startwith(R, p0, rg.g), status[k] == 0 ? attempt[k] : -1, t);
   for (int o = 0; o < MLP_OUT; o++) T[(long)k * MLP_OUT + o] = status[k] == 0 ? (float)t[o] : __int_as_float(0x7fc00000);
 }
 
@@ -1018,11 +1032,12 @@ extern "C" int kgpu_rad_features_device(int n, const kgpu_rad_params *rp, const 
 }
 
 extern "C" int kgpu_rad_targets_device(int n, const kgpu_rad_params *rp, const double *pp, const double *pp1,
-                                       const double *g, const double *G, const int *status, float *T,
-                                       void *stream) {
-  if (n < 0 || !rp || (n > 0 && (!pp || !pp1 || !g || !G || !status || !T))) return KGPU_EINVAL;
+                                       const double *g, const double *G, const int *status, const int *attempt,
+                                       float *T, void *stream) {
+  if (n < 0 || !rp || (n > 0 && (!pp || !pp1 || !g || !G || !status || !attempt || !T))) return KGPU_EINVAL;
   if (n == 0) return 0;
-  k_rad_targets<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(to_dev(*rp), n, pp, pp1, g, G, status, T);
+  k_rad_targets<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(to_dev(*rp), n, pp, pp1, g, G, status, attempt,
+                                                                    T);
   RCK(cudaGetLastError());
   return 0;
 }
@@ -1129,5 +1144,37 @@ extern "C" int kgpu_fp64_peak(double *ops_per_s) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   *ops_per_s = 2.0 * 8.0 * iters * (double)blocks * threads / (best * 1e-3);
+  return 0;
+}
+
+// The device's powers and logarithm on host arrays, for checking them
+// against the host C library: kind 0 x^2, 1 x^4, 2 x^-3.5, 3 x^y with 4y an
+// integer (else pow), 4 log(x), 5 the library pow(x, y).
+__global__ void k_eval_powers(int n, int kind, double y, const double *x, double *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double v = x[i];
+  double r;
+  switch (kind) {
+    case 0: r = pw2(v); break;
+    case 1: r = pw4(v); break;
+    case 2: r = pw_m3p5(v); break;
+    case 3: r = pw_any(v, y); break;
+    case 4: r = log(v); break;
+    default: r = pow(v, y); break;
+  }
+  out[i] = r;
+}
+
+extern "C" int kgpu_eval_powers(int n, int kind, double y, const double *x, double *out) {
+  if (n < 0 || kind < 0 || kind > 5 || (n > 0 && (!x || !out))) return KGPU_EINVAL;
+  if (n == 0) return 0;
+  DevMem m;
+  RCK(cudaMalloc(&m.p, (size_t)n * 16));
+  double *dx = (double *)m.p, *dout = dx + n;
+  RCK(cudaMemcpy(dx, x, (size_t)n * 8, cudaMemcpyHostToDevice));
+  k_eval_powers<<<(n + 255) / 256, 256>>>(n, kind, y, dx, dout);
+  RCK(cudaGetLastError());
+  RCK(cudaMemcpy(out, dout, (size_t)n * 8, cudaMemcpyDeviceToHost));
   return 0;
 }

@@ -179,7 +179,7 @@ KG_RAD_CALL KG_HD void calc_Gi(const RadParams &R, const double *pp, const Geom 
   double u = pp[1];
   double p = (R.gamma - 1.) * u;
   double Tgas = p * R.mu * R.mp / R.kb / rho;
-  double B = R.sigma * pow(Tgas, 4.) / RAD_PI;
+  double B = R.sigma * pw4(Tgas) / RAD_PI;
   double kappa = rad_kappa_abs(R, pp);
   double kappaes = rad_kappa_es(R, pp);
   double Ruu = 0.;
@@ -202,7 +202,10 @@ KG_RAD_CALL KG_HD void calc_Gi(const RadParams &R, const double *pp, const Geom 
 // The closed forms are the reference's (generated by computer algebra);
 // they are kept term for term so that the rounding is the same.
 // ---------------------------------------------------------------------------
-KG_HD double m1_pow2(double x) { return pow(x, 2.); }
+// pow(x, 2.) of the closed forms: the product, which is the correctly
+// rounded square (a general pow is not always; the host library's almost
+// always is)
+KG_HD double m1_pow2(double x) { return pw2(x); }
 
 // lab-frame gamma^2 of the radiation frame from R_t_mu (u2prad.c:116-250)
 KG_RAD_CALL KG_HD double m1_gammarel2(const RadParams &R, const RadGeom &rg, const double Avcov[4]) {

@@ -258,6 +258,16 @@ class RefRadCells:
         self.L.kref_rad_u2p(n, _p(uu), _p(pp), _p(g), _p(G), _i(st), _i(co))
         return pp, st, co
 
+    def u2p_full(self, uu, pp, g, G):
+        """The reference's u2p (u2p.c:176, MHD then M1) per cell; returns
+        (pp, status, corrected [n][3], fixups [n][2])."""
+        n = uu.shape[0]
+        pp = pp.copy()
+        st = np.zeros(n, np.int32)
+        co, fx = np.zeros((n, 3), np.int32), np.zeros((n, 2), np.int32)
+        self.L.kref_u2p_full(n, _p(uu), _p(pp), _p(g), _p(G), _i(st), _i(co), _i(fx))
+        return pp, st, co, fx
+
     # counter slot of the successful attempt -> (primitives, equation, frame)
     SLOTS = {0: ("RAD", "energy", "lab"), 13: ("RAD", "energy", "ff"), 2: ("MHD", "energy", "lab"),
              14: ("MHD", "energy", "ff"), 4: ("RAD", "entropy", "lab"), 6: ("MHD", "entropy", "lab")}

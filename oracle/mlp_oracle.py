@@ -9,7 +9,7 @@ pass and gradients.
 """
 import numpy as np
 
-NIN, NH, NOUT, NOUTP = 16, 128, 5, 8
+NIN, NH, NOUT, NOUTP = 16, 128, 7, 8
 OW1 = 0
 OB1 = OW1 + NIN * NH
 OW2 = OB1 + NH

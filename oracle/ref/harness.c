@@ -418,6 +418,21 @@ int kref_rad_u2p(int n, const double *uu, double *pp, const double *g20, const d
   return 0;
 }
 
+/* The reference's own u2p (u2p.c:176, type 0) on n cells with their own
+ * metric points, with all its outputs: status, corrected[3], fixups[2] per
+ * cell. */
+int kref_u2p_full(int n, const double *uu, double *pp, const double *g20, const double *G20, int *status,
+                  int *corrected, int *fixups)
+{
+  int k;
+  for (k = 0; k < n; k++) {
+    struct geometry geom;
+    kref_geom_from(g20 + 20 * k, G20 + 20 * k, &geom);
+    status[k] = u2p((double *)uu + (long)k * NV, pp + (long)k * NV, &geom, corrected + 3 * k, fixups + 2 * k, 0);
+  }
+  return 0;
+}
+
 /* The same solves for CPU timing: all cells loaded first, then solved in an
  * OpenMP loop when the build has OpenMP (the reference's counters are then
  * updated without synchronisation, as in its own parallel loops). */

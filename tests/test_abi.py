@@ -36,3 +36,21 @@ def test_invalid_config_rejected_without_gpu(kgpu):
     assert kgpu.lib().kgpu_create(ctypes.byref(cfg), ctypes.byref(h)) == -1
     cfg = kgpu.default_config(16, 16, 1, int_order=3)
     assert kgpu.lib().kgpu_create(ctypes.byref(cfg), ctypes.byref(h)) == -1
+
+
+def build_rk2_loop(kgpu, out_dir):
+    """Compiles tests/abi/rk2_loop.c (KORAL's RK2 loop written against the
+    header) with gcc and links it to the library."""
+    import subprocess
+    exe = os.path.join(str(out_dir), "rk2_loop")
+    libdir = os.path.dirname(kgpu.LIB_PATH)
+    subprocess.check_call(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "abi", "rk2_loop.c"), "-L", libdir, "-lkoral_b200",
+                           "-Wl,-rpath," + libdir, "-o", exe])
+    return exe
+
+
+def test_rk2_loop_program_compiles_and_links(kgpu, tmp_path):
+    """The host-side loop compiles as C99 against include/koral_b200.h and
+    links against every symbol it names."""
+    assert os.path.exists(build_rk2_loop(kgpu, tmp_path))

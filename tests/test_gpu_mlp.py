@@ -26,11 +26,11 @@ def _random_setup(kgpu, n, seed):
     rng = np.random.default_rng(seed)
     m = kgpu.Mlp(seed=seed)
     blob = m.get()
-    blob[-16:-11] = rng.normal(0, 0.1, 5)
-    blob[-8:-3] = rng.uniform(0.5, 2.0, 5)
+    blob[-16:-9] = rng.normal(0, 0.1, 7)
+    blob[-8:-1] = rng.uniform(0.5, 2.0, 7)
     m.set(blob)
     X = rng.normal(0, 1, (n, 16)).astype(np.float32)
-    T = rng.normal(0, 1, (n, 5)).astype(np.float32)
+    T = rng.normal(0, 1, (n, 7)).astype(np.float32)
     return m, m.get(), X, T
 
 
@@ -39,7 +39,7 @@ def test_mlp_forward_matches_oracle(kgpu, torch):
     m, blob, X, _ = _random_setup(kgpu, 1000, 3)
     Y = m.forward(torch.from_numpy(X).cuda()).cpu().numpy()
     ref = mo.predict(blob, X)
-    d = np.abs(Y[:, :5] - ref[:, :5])
+    d = np.abs(Y[:, :7] - ref[:, :7])
     print("forward: max abs diff", d.max(), "mean", d.mean())
     assert d.max() <= 2e-2 and d.mean() <= 1e-3
 
@@ -64,9 +64,9 @@ def _solved_pairs(kgpu, torch, n, seed):
     rp = kgpu.rad_params()
     uu, pp, g, G, dt = kgpu.rad_cells(n, seed, rp, sigma=(1e-3, 1e3))
     d = [torch.from_numpy(a).cuda() for a in (uu, pp, g, G, dt)]
-    po, _, st, _, _, _ = kgpu.rad_solve_device(rp, *d)
+    po, _, st, at, _, _ = kgpu.rad_solve_device(rp, *d)
     X = kgpu.rad_features_device(rp, d[1], d[2], d[3], d[4])
-    T = kgpu.rad_targets_device(rp, d[1], po, d[2], d[3], st)
+    T = kgpu.rad_targets_device(rp, d[1], po, d[2], d[3], st, at)
     ok = torch.isfinite(T).all(dim=1) & torch.isfinite(X).all(dim=1)
     return rp, d, X, T, ok
 
@@ -76,8 +76,8 @@ def test_mlp_training_lowers_the_loss(kgpu, torch):
     X, T = X[ok].contiguous(), T[ok].contiguous()
     m = kgpu.Mlp(seed=5)
     blob = m.get()
-    blob[-16:-11] = T.mean(0).cpu().numpy()
-    blob[-8:-3] = T.std(0).cpu().numpy()
+    blob[-16:-9] = T.mean(0).cpu().numpy()
+    blob[-8:-1] = T.std(0).cpu().numpy().clip(1e-3)
     m.set(blob)
     losses = [m.train_epoch(X, T, batch=1024, lr=2e-3, seed=e) for e in range(4)]
     print("losses", losses)
@@ -105,9 +105,12 @@ WEIGHTS = os.path.join(os.path.dirname(__file__), "..", "koral_b200", "data", "w
 
 @pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="no trained warm-start weights")
 def test_trained_warm_start_cuts_newton_iterations(kgpu, torch):
-    """The trained network (held-out cells, seed not used in training): mean
-    Newton iterations of the succeeding attempt at least 1.8x lower than the
-    plain solve, same success on 99% of the cells."""
+    """The trained network on held-out cells (seed not used in training):
+    Newton iterations per implicit solve counted over every attempt the
+    solve makes (failed attempts, skipped ones not run, and the fallback to
+    the reference cascade included) at least 2x fewer than the plain
+    batched solve at the same residual, and the same success on 99% of the
+    cells."""
     from koral_b200 import train_warmstart
     m = train_warmstart.load(kgpu, WEIGHTS)
     rp = kgpu.rad_params()
@@ -120,7 +123,9 @@ def test_trained_warm_start_cuts_newton_iterations(kgpu, torch):
     ip, iw = plain[4].cpu().numpy(), warm[4].cpu().numpy()
     sp, sw = plain[2].cpu().numpy(), warm[2].cpu().numpy()
     ok = (sp == 0) & (sw == 0)
-    print(f"iterations plain {ip[ok].mean():.3f} learned {iw[ok].mean():.3f}; fallbacks {warm[5][2]}; "
-          f"status agree {np.mean(sp == sw):.4f}")
+    all_plain, all_warm = plain[5][0] / len(sp), warm[5][0] / len(sp)
+    print(f"iterations per solve over all attempts: plain {all_plain:.3f} learned {all_warm:.3f} "
+          f"(ratio {all_plain / all_warm:.3f}); succeeding attempt: plain {ip[ok].mean():.3f} "
+          f"learned {iw[ok].mean():.3f}; fallbacks {warm[5][2]}; status agree {np.mean(sp == sw):.4f}")
     assert np.mean(sp == sw) >= 0.99
-    assert iw[ok].mean() * 1.8 <= ip[ok].mean()
+    assert all_warm * 2.0 <= all_plain

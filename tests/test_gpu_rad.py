@@ -148,3 +148,22 @@ def test_rad_persistent_launches(kgpu, cells):
     d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (uu, pp, g, G, dt)]
     out = kgpu.rad_solve_device(rp, *d, mode=kgpu.RAD_PERSISTENT, nstats=7)
     assert out[5][1] in (1, 2)   # launches that had work: the resident kernel, and the finish if cells were handed on
+
+
+def test_u2p_full_matches_reference(kgpu, ref, cells):
+    """The per-cell u2p with all its outputs (kgpu_u2p_cells_full): the MHD
+    inversion and then u2p_rad on the 13 variables of each cell, against the
+    reference's own u2p (u2p.c:176).  Status, corrected[3] and fixups[2]
+    equal; MHD primitives bit-identical except the entropy (CUDA's log and
+    pow: 1e-12), radiation primitives within 1e-12 (pow in the closure)."""
+    rp, uu, pp, g, G, dt = cells
+    rng = np.random.default_rng(7)
+    guess = pp * (1 + rng.uniform(-0.02, 0.02, pp.shape))
+    pr, sr, cr, fr = ref.u2p_full(uu, guess, g, G)
+    cfg = kgpu.default_config(8, 8, 1, nv=13, gamma=rp.gamma)
+    pg, sg, cg, fg = kgpu.u2p_cells_full(cfg, uu, guess, g, G, rp)
+    assert np.array_equal(sg, sr) and np.array_equal(cg, cr) and np.array_equal(fg, fr)
+    print("statuses", np.unique(sr, return_counts=True), "rad corrected", cr[:, 1].sum())
+    assert np.array_equal(pg[:, NONENT[:8]], pr[:, NONENT[:8]])
+    rel = np.abs(pg - pr) / (np.abs(pr) + 1e-300)
+    assert rel[:, 5].max() <= 1e-12 and rel[:, 9:].max() <= 1e-12, (rel[:, 5].max(), rel[:, 9:].max())

@@ -180,3 +180,35 @@ def test_u2p_pause_and_resume_is_exact(kgpu, oracle):
             assert cnt["paused"] > 0
     for u, p in states[1:]:
         assert np.array_equal(u, states[0][0]) and np.array_equal(p, states[0][1])
+
+
+def test_flux_ct_fluxes_match_reference(kgpu, oracle):
+    """flux_ct through the C-ABI: after op_explicit from the reference's
+    state, kgpu_flux_ct stores the face fluxes with their magnetic
+    components rewritten from the corner EMFs; they equal the reference's
+    flbx/flby/flbz after its op_explicit (which calls flux_ct), every
+    variable bit for bit except the entropy flux (1e-12).  A second call
+    for the same op_explicit is refused."""
+    R, s = make_pair(kgpu, oracle)
+    R.step(3)
+    s.upload_state(R.array("u").copy(), R.array("p").copy())
+    s.tstepdenmax = R.scalar("tstepdenmax")
+    import ctypes
+    R.L.op_explicit.argtypes = [ctypes.c_double, ctypes.c_double]
+    dt = R.scalar("dt")
+    R.L.op_explicit(0., dt)
+    s.op_explicit(0., dt)
+    s.flux_ct()
+    with pytest.raises(kgpu.KgpuError):
+        s.flux_ct()
+    g, nx, ny, nz, nv = R.ng, R.nx, R.ny, R.nz, R.nv
+    sx, sy, sz = R.sx, R.sy, R.sz
+    shapes = {0: ("flbx", (sz, sy, sx + 1, nv), (nz, ny, nx + 1)), 1: ("flby", (sz, sy + 1, sx, nv), (nz, ny + 1, nx)),
+              2: ("flbz", (sz + 1, sy, sx, nv), (nz + 1, ny, nx))}
+    for d, (name, shp, (kz, ky, kx)) in shapes.items():
+        got = s.download_flux(d).reshape(shp)[g:g + kz, g:g + ky, g:g + kx]
+        ref = R.array(name, shp)[g:g + kz, g:g + ky, g:g + kx]
+        nonent = [0, 1, 2, 3, 4, 6, 7, 8]
+        assert np.array_equal(got[..., nonent], ref[..., nonent]), name
+        assert np.all(np.abs(got[..., 5] - ref[..., 5]) <= 1e-12 * (np.abs(ref[..., 5]) + 1e-6 * np.abs(ref[..., 5]).max())), name
+        assert np.any(ref[..., 6:9] != 0.), name   # the rewritten components are not trivially zero
