@@ -157,17 +157,20 @@ def parse():
     ap.add_argument("--workload", default="radtorus", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-solve", choices=["plain", "batched", "persistent"], default=None,
-                    help="radtorus only, a profiling aid: after the warm-up steps solve the cells of the last "
-                         "implicit step again with this solver and print its counters as JSON (no bench line)")
+                    help="a profiling aid: radtorus: after the warm-up steps solve the cells of the last implicit "
+                         "step again with this solver; radcells: solve the first cells of the batched-solve "
+                         "distribution; print the solver's counters as JSON (no bench line)")
     ap.add_argument("--profile-cells", type=int, default=0,
                     help="with --profile-solve: solve only the first this many cells (0: all)")
     return ap.parse_args()
 
 
 def profile_solve(args):
-    """A profiling aid for the radiative torus: after the warm-up steps, the
-    cells of the last implicit step (their inputs, as the step gathered
-    them; the first --profile-cells of them, or all) are solved once more
+    """A profiling aid for the implicit solve.  Radiative torus: after the
+    warm-up steps, the cells of the last implicit step (their inputs, as the
+    step gathered them; the first --profile-cells of them, or all); batched-
+    solve workload: the first --profile-cells cells of its distribution
+    (seed 2026).  They are solved once
     with the given solver through kgpu_rad_implicit_cells_device_ex, for an
     ncu capture of its kernels; prints the solver's counters (solves, Newton
     iterations, residual evaluations, nested inversion work) and its event
@@ -178,22 +181,29 @@ def profile_solve(args):
     from koral_b200 import build
     build.build()
     torch.cuda.set_device(0)
-    s = make_subdomain(k, "radtorus")
-    mlp, _ = warmstart_network(k)
-    s.set_implicit_options(warm_attempts=WARM_ATTEMPTS_RADTORUS, skip=SKIP_RADTORUS)
-    s.set_implicit_solver(k.RAD_BATCHED, mlp)
-    s.rk2imex_steps(max(1, args.warmup), graph=True)
-    n, b = s.implicit_buffers()
-    m = min(n, args.profile_cells) if args.profile_cells > 0 else n
+    if args.workload == "radcells":
+        rp = k.rad_params()
+        m = args.profile_cells if args.profile_cells > 0 else WORKLOADS["radcells"]["ncells"]
+        d = [torch.from_numpy(a).cuda() for a in k.rad_cells(m, 2026, rp)]
+    else:
+        s = make_subdomain(k, "radtorus")
+        mlp, _ = warmstart_network(k)
+        s.set_implicit_options(warm_attempts=WARM_ATTEMPTS_RADTORUS, skip=SKIP_RADTORUS)
+        s.set_implicit_solver(k.RAD_BATCHED, mlp)
+        s.rk2imex_steps(max(1, args.warmup), graph=True)
+        n, b = s.implicit_buffers()
+        m = min(n, args.profile_cells) if args.profile_cells > 0 else n
 
-    class Dev:
-        def __init__(self, ptr, shape):
-            self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f8", "data": (ptr, False), "version": 3}
+        class Dev:
+            def __init__(self, ptr, shape):
+                self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f8", "data": (ptr, False),
+                                                 "version": 3}
 
-    d = [torch.as_tensor(Dev(b[key], shape), device="cuda")[:m].clone()
-         for key, shape in (("uu_in", (n, 13)), ("pp_in", (n, 13)), ("g20", (n, 20)), ("G20", (n, 20)), ("dt", (n,)))]
-    rp = s._rp
-    s.close()
+        d = [torch.as_tensor(Dev(b[key], shape), device="cuda")[:m].clone()
+             for key, shape in (("uu_in", (n, 13)), ("pp_in", (n, 13)), ("g20", (n, 20)), ("G20", (n, 20)),
+                                ("dt", (n,)))]
+        rp = s._rp
+        s.close()
     mode = {"plain": k.RAD_PLAIN, "batched": k.RAD_BATCHED, "persistent": k.RAD_PERSISTENT}[args.profile_solve]
     torch.cuda.synchronize()
     a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -566,8 +576,12 @@ MAIN_SOLVER = "batched"
 # FP64 work of one residual evaluation of the implicit solve on the torus's
 # own cells, nested MHD inversion included: DADD + DMUL + 2 DFMA thread
 # instructions of the one-thread-per-cell solver over its counted
-# evaluations (ncu capture, profiles/k_rad_radtorus_256x128x64.md)
-IMP_FP64_PER_EVAL = 2972.0
+# evaluations (ncu capture of the first 262144 cells of the implicit step
+# after 3 time steps, profiles/k_rad_plain_fp64_per_evaluation.md)
+IMP_FP64_PER_EVAL = 2884.5
+# the same figure on the batched-solve cells (the first 65536 of the 2^22,
+# seed 2026; profiles/k_rad_plain_fp64_per_evaluation.md)
+IMP_FP64_PER_EVAL_CELLS = 2838.5
 
 CPU_REF_CHILD = r"""
 import json, sys, time
@@ -878,6 +892,57 @@ def learned_leg(k, rp, d_in, work, stream, n, st_plain, it_plain, all_plain, arg
                     "frac": flop / (ms_mlp / 1e3) / 1e12 / bf16_peak, "bound": "tensor"}}
 
 
+def u2p_leg(k, rp, n, stream, dev):
+    """The MHD inversion with and without its learned warm start on n
+    held-out cells of the warm start's distribution (the batched-solve cells
+    with a magnetic field, B^2/rho log-uniform in [1e-3, 1e3], seed 2026):
+    the gas state after the plain implicit solve, inverted from the
+    primitives before it (calc_u2p's situation after a step that moved the
+    gas energy); device time and Newton iterations over all solves of each
+    inversion."""
+    import numpy as np
+    import torch
+    from koral_b200 import train_warmstart
+    path = train_warmstart.DEFAULT_OUT_U2P
+    if not os.path.exists(path):
+        return {"unavailable": "no trained weights (python -m koral_b200.train_warmstart --source u2p)"}
+    mlp = train_warmstart.load(k, path)
+    U, P0, gg, GG = train_warmstart.u2p_cells(k, rp, n, 2026)
+    m = U.shape[0]
+    cfg = k.u2p_config(rp.gamma)
+
+    def plain():
+        return k.u2p_cells_device(cfg, U, P0, gg, GG)
+
+    def learned():
+        Y = mlp.forward(k.u2p_features_device(cfg, U, P0, gg, GG))
+        return k.u2p_cells_device(cfg, U, P0, gg, GG, ypred=Y)
+
+    res = {}
+    for tag, fn in (("plain", plain), ("learned", learned)):
+        fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        res[tag] = (a.elapsed_time(b), out)
+    (ms_p, op), (ms_l, ol) = res["plain"], res["learned"]
+    sp, sl = op[1].cpu().numpy(), ol[1].cpu().numpy()
+    return {"inversions": m, "cells": "2^22 batched-solve cells with a magnetic field (sigma 1e-3..1e3, seed 2026) "
+                                      "whose plain implicit solve succeeded",
+            "plain": {"value": m / (ms_p / 1e3), "unit": "inversions/s",
+                                       "mean_iterations": op[4][0] / m, "w_evaluations": op[4][2] / m,
+                                       "entropy_rate": float(np.mean(sp == -1))},
+            "learned": {"value": m / (ms_l / 1e3), "unit": "inversions/s", "mean_iterations": ol[4][0] / m,
+                        "w_evaluations": ol[4][2] / m, "fallback_rate": ol[4][1] / m,
+                        "status_agreement": float(np.mean(sp == sl)), "wgate": k.U2P_WGATE, "sgate": k.U2P_SGATE},
+            "iteration_ratio": op[4][0] / max(1, ol[4][0]),
+            "note": "Newton iterations per inversion over all its solves (energy, entropy, fallback), plain over "
+                    "learned; the learned time includes features and network"}
+
+
 def our_arm_radcells(args, wl, rank, world, local_rank):
     import numpy as np
     import torch
@@ -933,15 +998,24 @@ def our_arm_radcells(args, wl, rank, world, local_rank):
     steps_plain = max(1, min(3, args.steps))
     ms_plain = timed(k.RAD_PLAIN, steps_plain)
     plain_value = n * steps_plain * world / (ms_plain / 1e3)
-    # iteration statistics of one batched solve
-    stats = (ctypes.c_ulonglong * 2)()
-    solve(k.RAD_BATCHED, stats)
+    # iteration statistics of one batched solve, with its residual evaluations
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    sout = k.rad_solve_device(rp, *d_in, mode=k.RAD_BATCHED, work=work, nstats=4)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_one = ev0.elapsed_time(ev1)
+    stats = sout[5]
+    d_po.copy_(sout[0]), d_uo.copy_(sout[1]), d_st.copy_(sout[2]), d_at.copy_(sout[3]), d_it.copy_(sout[4])
     st = d_st.cpu().numpy()
     it = d_it.cpu().numpy()
     at = d_at.cpu().numpy()
     peak = ctypes.c_double()
     k._check(L.kgpu_fp64_peak(ctypes.byref(peak)), "kgpu_fp64_peak")
     learned = learned_leg(k, rp, d_in, work, stream, n, st, it, stats[0], args, dev)
+    u2p = u2p_leg(k, rp, n, stream, dev)
+    fp64_peak = peak.value / 1e12
+    tf = IMP_FP64_PER_EVAL_CELLS * stats[3] / (ms_one / 1e3) / 1e12 if IMP_FP64_PER_EVAL_CELLS else None
 
     # e2e: the host-pointer entry point with pinned buffers, copies included
     hin = []
@@ -977,13 +1051,17 @@ def our_arm_radcells(args, wl, rank, world, local_rank):
                    "parallelism": "replicas" if world > 1 else "one batch", "solver": "batched work queue"},
         "plain": {"value": plain_value, "unit": RAD_UNIT, "ms_per_step": ms_plain / steps_plain},
         "learned": learned,
+        "u2p_warm_start": u2p,
         "newton": {"mean_iterations_successful_attempt": float(it[ok].mean()),
                    "mean_iterations_all_attempts": stats[0] / n, "passes_with_work": int(stats[1]),
                    "success_rate": float(ok.mean()),
                    "attempt_histogram": {int(a): int((at == a).sum()) for a in np.unique(at)}},
-        "roofline": {"kernel": "k_rad_pass", "bound": "fp64", "peak": peak.value / 1e12, "unit": "TFLOP/s",
-                     "peak_source": "measured live (DMUL+DADD chains, no FMA)", "achieved": None, "frac": None,
-                     "traffic": None},
+        "roofline": {"kernel": "k_rad_pass + k_rad_slow + k_rad_tail (batched implicit solve)", "bound": "fp64",
+                     "peak": fp64_peak, "unit": "TFLOP/s",
+                     "peak_source": "measured live (DMUL+DADD chains, no FMA)", "achieved": tf,
+                     "frac": tf / fp64_peak if tf else None, "traffic": None, "evaluations": int(stats[3]),
+                     "solve_ms": ms_one,
+                     "flop_per_evaluation": IMP_FP64_PER_EVAL_CELLS},
         "e2e": {"value": e2e_value, "unit": RAD_UNIT, "h2d_bytes_per_step": n * (13 + 13 + 20 + 20 + 1) * 8,
                 "d2h_bytes_per_step": n * (26 * 8 + 12)},
         "gpu_launches": passes * args.steps,

@@ -434,6 +434,34 @@ int kgpu_rad_targets_device(int n, const kgpu_rad_params *rp, const double *pp, 
                             const double *g, const double *G, const int *status, const int *attempt, float *T,
                             void *stream);
 
+/* Learned warm start of the MHD inversion.  Replaces, on independent cells,
+ * the per-cell u2p(uu,pp,geom,corrected,fixups,0) of u2p.c:176, whose
+ * Newton iteration starts from W = (rho + GAMMA u) gamma^2 of the guess pp
+ * (u2p.c:2093-2112).  Cells are rows of nv >= 9 doubles (the nine MHD
+ * variables first; 13 with radiation), metric points 20 doubles; device
+ * pointers, the call waits for its stream when stats are asked for.
+ * kgpu_u2p_cells_device: with ypred null, the reference's u2p (same results
+ * as kgpu_u2p_cells); with ypred (float [n][8], kgpu_mlp_forward's output)
+ * the solve starts from W_guess exp(ypred[0]) where |ypred[0]| >= wgate
+ * (from W_guess elsewhere), with the entropy equation alone where
+ * ypred[1] > sgate, and falls back to the reference's u2p from the guess
+ * where it does not converge.  iters (optional) gets each cell's
+ * Newton iterations over all its solves; stats: [0] Newton iterations,
+ * [1] fallbacks, [2] W-function evaluations (bracketing and damped trials
+ * included).  kgpu_u2p_features_device: network inputs (float [n][16]) of
+ * the conserved state uu and the guess pp; kgpu_u2p_targets_device:
+ * training targets (float [n][7]: ln(W/W_guess), 1/0 for an entropy
+ * inversion, zeros) from the guess and the inverted primitives pp1, NaN
+ * where status is neither 0 nor -1.  cfg supplies GAMMA, U2PCONV and
+ * the density floor; its grid fields are not read. */
+int kgpu_u2p_cells_device(int n, const kgpu_config *cfg, int nv, const double *uu, double *pp, const double *g,
+                          const double *G, const float *ypred, float wgate, float sgate, int *status, int *fixup,
+                          int *iters, void *stream, unsigned long long *stats, int nstats);
+int kgpu_u2p_features_device(int n, const kgpu_config *cfg, int nv, const double *uu, const double *pp,
+                             const double *g, const double *G, float *X, void *stream);
+int kgpu_u2p_targets_device(int n, const kgpu_config *cfg, int nv, const double *pp, const double *pp1,
+                            const double *g, const double *G, const int *status, float *T, void *stream);
+
 /* The warm-start network: 16 -> 128 -> 128 -> 7, SiLU, BF16 weights and
  * activations with FP32 accumulation on the tensor cores; trained and run on
  * the device.  The parameter blob (kgpu_mlp_blob_size() floats) holds

@@ -189,6 +189,11 @@ def lib():
         sop = ctypes.POINTER(SolverOpts)
         L.kgpu_rad_implicit_cells_device_ex.argtypes = [ctypes.c_int, rpp] + [vp] * 11 + [
             ctypes.c_int, sop, vp, vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]
+        cfp = ctypes.POINTER(Config)
+        L.kgpu_u2p_cells_device.argtypes = [ctypes.c_int, cfp, ctypes.c_int] + [vp] * 5 + [ctypes.c_float] * 2 + [
+            vp] * 4 + [ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]
+        L.kgpu_u2p_features_device.argtypes = [ctypes.c_int, cfp, ctypes.c_int] + [vp] * 6
+        L.kgpu_u2p_targets_device.argtypes = [ctypes.c_int, cfp, ctypes.c_int] + [vp] * 7
         L.kgpu_rad_default_solver_opts.argtypes = [sop]
         L.kgpu_rad_set_solver_opts.argtypes = [sop]
         L.kgpu_rad_get_solver_opts.argtypes = [sop]
@@ -985,6 +990,59 @@ def rad_targets_device(rp, pp, pp1, g, G, status, attempt):
     _check(lib().kgpu_rad_targets_device(pp.shape[0], ctypes.byref(rp), _vp(pp), _vp(pp1), _vp(g), _vp(G),
                                          _vp(status), _vp(attempt), _vp(T), _stream()), "kgpu_rad_targets_device")
     return T
+
+
+U2P_WGATE, U2P_SGATE = 0.005, 0.5   # default gates of the u2p warm start (measured best on held-out cells)
+
+
+def u2p_cells_device(cfg, uu, pp, g, G, ypred=None, wgate=U2P_WGATE, sgate=U2P_SGATE):
+    """The MHD inversion of n cells on device tensors (kgpu_u2p_cells_device):
+    uu, pp [n][nv] (nine MHD variables first), g, G [n][20]; pp is the guess.
+    With ypred (the network's output on u2p_features_device), the learned
+    warm start: the predicted W where |ln(W/W_guess)| >= wgate, the entropy
+    equation alone where the score passes sgate.  Returns (pp, status,
+    fixup, iters, stats) with stats = [Newton iterations, fallbacks,
+    W-function evaluations]."""
+    import torch
+    n, nv = uu.shape
+    dev = uu.device
+    po = pp.clone()
+    st, fx, it = (torch.empty(n, dtype=torch.int32, device=dev) for _ in range(3))
+    stats = (ctypes.c_ulonglong * 3)()
+    _check(lib().kgpu_u2p_cells_device(n, ctypes.byref(cfg), nv, _vp(uu), _vp(po), _vp(g), _vp(G),
+                                       _vp(ypred) if ypred is not None else None, float(wgate), float(sgate),
+                                       _vp(st), _vp(fx), _vp(it),
+                                       _stream(), stats, 3), "kgpu_u2p_cells_device")
+    return po, st, fx, it, list(stats)
+
+
+def u2p_features_device(cfg, uu, pp, g, G):
+    """Network inputs [n][16] of the u2p warm start (kgpu_u2p_features_device)."""
+    import torch
+    n, nv = uu.shape
+    X = torch.empty((n, 16), dtype=torch.float32, device=uu.device)
+    _check(lib().kgpu_u2p_features_device(n, ctypes.byref(cfg), nv, _vp(uu), _vp(pp), _vp(g), _vp(G), _vp(X),
+                                          _stream()), "kgpu_u2p_features_device")
+    return X
+
+
+def u2p_targets_device(cfg, pp, pp1, g, G, status):
+    """Training targets [n][7] of the u2p warm start (kgpu_u2p_targets_device)."""
+    import torch
+    n, nv = pp.shape
+    T = torch.empty((n, MLP_OUT), dtype=torch.float32, device=pp.device)
+    _check(lib().kgpu_u2p_targets_device(n, ctypes.byref(cfg), nv, _vp(pp), _vp(pp1), _vp(g), _vp(G), _vp(status),
+                                         _vp(T), _stream()), "kgpu_u2p_targets_device")
+    return T
+
+
+def u2p_config(gamma, u2pconv=1e-10, rhofloor=1e-50):
+    """A Config carrying the inversion's parameters (GAMMA, U2PCONV, the
+    density floor) for the per-cell u2p entry points."""
+    cfg = default_config(1, 1, 1, ng=3, gamma=gamma)
+    cfg.u2pconv = u2pconv
+    cfg.rhofloor = rhofloor
+    return cfg
 
 
 def rad_solve_device(rp, uu, pp, g, G, dt, mode=RAD_BATCHED, ypred=None, work=None, opts=None, nstats=3):

@@ -88,4 +88,67 @@ KG_HD void mlp_guess(const double *pp0, const RadGeom &rg, int startwith, const 
     for (int i = 0; i < 3; i++) guess[FX0 + i] = pp0[FX0 + i] + t[2 + i] / sqrt(gg[i + 1][i + 1]);
 }
 
+// ---------------------------------------------------------------------------
+// The same network as the warm start of the MHD inversion (u2p).  Inputs:
+// the invariants of the conserved state that u2p_setup forms (D, the
+// normal-frame energy E = -Q.n, |Q_perp|^2, B^2, (Q.B)^2, the entropy
+// density), the reference's starting W (u2p.c:2093-2112) with the energy
+// residual and Newton step there, and the metric at the cell:
+//   0  log10 D / 4 + 1              1  log10(E / D - 1) / 4
+//   2  |Q_perp| / E                 3  log10(1 - Q_perp^2 / E^2) / 4
+//   4  log10(B^2 / D) / 4           5  (Q.B)^2 / (B^2 Q_perp^2)
+//   6  log10(W_guess / D) / 4       7  asinh(f(W_guess) / E)
+//   8  asinh(-f / (f' W_guess))     9  log10(u / rho) / 4 of the guess
+//   10 log10(gamma^2) / 2 of the guess   11 lapse
+//   12 g_tt + 1                     13 log10 sqrt(g_33) / 2
+//   14 asinh(S_c / D) / 4           15 log10(E / W_guess)
+// Outputs: 0  ln(W / W_guess), W the root the plain inversion reached;
+//          1  1 when the plain inversion needed the entropy equation.
+// ---------------------------------------------------------------------------
+KG_HD double mlp_clip_log10(double x, double lo) { return log10(x > lo ? x : lo); }
+
+KG_HD void u2p_features(double GAMMA, const double *uu, const double *pp0, const Geom &g, float x[MLP_IN]) {
+  U2PState s;
+  u2p_setup(uu, g, s);
+  const double D = s.c.D > 1e-300 ? s.c.D : 1e-300;
+  const double E = -s.c.Qn;
+  const double Ep = fabs(E) > 1e-300 ? fabs(E) : 1e-300;
+  const double W0 = u2p_initial_w(GAMMA, pp0, g);
+  double f0 = 0., df0 = 0., err0 = 0.;
+  f_u2p(GAMMA, 0, W0 - s.c.D, s.c, f0, df0, err0);
+  const double q2 = s.c.Qt2 / (Ep * Ep);
+  x[0] = (float)(mlp_clip_log10(D, 1e-300) / 4. + 1.);
+  x[1] = (float)(mlp_clip_log10(E / D - 1., 1e-30) / 4.);
+  x[2] = (float)sqrt(q2 < 1. ? q2 : 1.);
+  x[3] = (float)(mlp_clip_log10(1. - q2, 1e-12) / 4.);
+  x[4] = (float)(mlp_clip_log10(s.c.Bsq / D, 1e-12) / 4.);
+  x[5] = (float)(s.c.Bsq * s.c.Qt2 > 0. ? s.c.QdotBsq / (s.c.Bsq * s.c.Qt2) : 0.);
+  x[6] = (float)(mlp_clip_log10(W0 / D, 1e-30) / 4.);
+  x[7] = (float)asinh(f0 / Ep);
+  x[8] = (float)(df0 != 0. && isfinite(f0 / df0) ? asinh(-f0 / (df0 * W0)) : 0.);
+  x[9] = (float)(mlp_clip_log10(pp0[UU] / pp0[RHO], 1e-30) / 4.);
+  x[10] = (float)(mlp_clip_log10(W0 / (pp0[RHO] + GAMMA * pp0[UU]), 1.) / 2.);
+  x[11] = (float)sqrt(-1. / g.GG[0][0]);
+  x[12] = (float)g.gttpert;
+  x[13] = (float)(mlp_clip_log10(sqrt(g.gg[3][3]), 1e-300) / 2.);
+  x[14] = (float)(asinh(s.c.Sc / D) / 4.);
+  x[15] = (float)mlp_clip_log10(Ep / W0, 1e-30);
+  for (int f = 0; f < MLP_IN; f++)
+    if (!isfinite(x[f])) x[f] = 0.f;
+}
+
+KG_HD void u2p_targets(double GAMMA, const double *pp0, const double *pp1, const Geom &g, int status,
+                       double t[MLP_OUT]) {
+  for (int o = 0; o < MLP_OUT; o++) t[o] = 0.;
+  t[0] = log(u2p_initial_w(GAMMA, pp1, g) / u2p_initial_w(GAMMA, pp0, g));
+  t[1] = status != 0 ? 1. : 0.;
+}
+
+// the starting W of a warm-started inversion (0 when the prediction gives
+// no usable value)
+KG_HD double u2p_warm_w(double GAMMA, const double *pp0, const Geom &g, float y0) {
+  const double W = u2p_initial_w(GAMMA, pp0, g) * exp((double)y0);
+  return (isfinite(W) && W > 0.) ? W : 0.;
+}
+
 }  // namespace kgpu
