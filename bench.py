@@ -429,8 +429,18 @@ def our_arm(args, wl, rank, world, local_rank):
         if dist is not None:
             dist.barrier()
 
-    # warm-up (graph capture happens here)
+    # warm-up (graph capture happens here), then the autotuner's choice of
+    # launch shapes on the state reached (the same arithmetic whatever it
+    # picks)
     s.rk2_steps(max(1, args.warmup), graph=True)
+    tuning = None
+    if args.workload == "torus":
+        t_tune = time.perf_counter()
+        tuned, tune_ms = s.autotune(steps=2)
+        tuning = {"chosen": tuned.as_dict(), "seconds": time.perf_counter() - t_tune,
+                  "ms_per_step_before": tune_ms[0], "ms_per_step_after": tune_ms[1],
+                  "by": "kgpu_autotune on the warmed-up state"}
+        s.rk2_steps(1, graph=True)   # capture the step with the chosen shapes
 
     def timed_steps(k, profile=False):
         """k steps, L2 flushed before each; returns summed device ms."""
@@ -523,7 +533,8 @@ def our_arm(args, wl, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": wl["desc"], "cells_per_gpu": cells, "l2": "flushed (256 MB write) before every step",
-                   "parallelism": "replicas" if world > 1 else "single subdomain", "graph": "one CUDA graph per RK2 step"},
+                   "parallelism": "replicas" if world > 1 else "single subdomain", "graph": "one CUDA graph per RK2 step",
+                   "tuning": tuning},
         "roofline": roof,
         "kernels": {k: {"ms_per_launch": v[0] / max(1, v[1]), "share": v[0] / total if total else 0.}
                     for k, v in prof.items() if v[1]},
@@ -568,8 +579,16 @@ def warmstart_network(k):
 # step with all six)
 WARM_ATTEMPTS_RADTORUS = 2
 # on the torus only the cells the network expects to fail their first
-# attempt start from its prediction (kgpu_rad_solver_opts.skip = 2): the
-# others are already close to their solution at the previous state
+# attempt start from its prediction (kgpu_rad_solver_opts.skip = 2).  With
+# skip = 1 (every cell from the prediction, beginning with the attempt the
+# network expects to succeed) 10 settled steps (21-30) from one state took
+# 146.7 ms per step against 179.0 with skip = 2 and 177.0 without the
+# network, but the run from the initial torus reached states where both
+# solvers fail 50 times more solves (62074 against 1161 without the network
+# over steps 6-105) and every step costs more (11.32 M zone-cycles/s
+# against 11.69 M): the prediction sends some cells of the transient to
+# another solution of the same equations; skip = 2 keeps the reference's
+# start for the cells it expects to succeed
 SKIP_RADTORUS = 2
 # the implicit solver of the timed radiative-torus steps
 MAIN_SOLVER = "batched"
@@ -698,6 +717,11 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
     # times the same K steps from the state reached
     s.set_implicit_solver(main_mode, mlp)
     s.rk2imex_steps(max(1, args.warmup), graph=True)
+    # launch shapes and solver settings chosen by the autotuner on the state
+    # reached (same arithmetic whatever it picks; every leg uses the choice)
+    t_tune = time.perf_counter()
+    tuned, tune_ms = s.autotune(steps=2)
+    tune_s = time.perf_counter() - t_tune
     u_start, p_start = s.download_state()
     tsd_start = s.tstepdenmax
     launches0 = s.launches
@@ -778,6 +802,8 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
                    "graph": "one CUDA graph per RK2IMEX step", "solver": MAIN_SOLVER,
                    "warm_start_weights": mlp_name, "warm_attempts": WARM_ATTEMPTS_RADTORUS,
                    "warm_start_skip": SKIP_RADTORUS,
+                   "tuning": {"chosen": tuned.as_dict(), "seconds": tune_s, "ms_per_step_before": tune_ms[0],
+                              "ms_per_step_after": tune_ms[1], "by": "kgpu_autotune on the warmed-up state"},
                    "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps} from the initial torus"},
         "newton": {"learned": newton(c_main), "no_network": newton(c_n),
                    "iteration_ratio_no_network_over_learned": it_n / it_main if it_main > 0 else None},
