@@ -663,6 +663,35 @@ typedef struct kgpu_scalars_params {
 int kgpu_calc_scalars(kgpu_ctx *ctx, const kgpu_scalars_params *sp, double t, double *scalars);
 int kgpu_calc_scalars_device(kgpu_ctx *ctx, const kgpu_scalars_params *sp, double t, double *scalars_dev);
 
+/* Time averages.  Replaces save_avg(dt) (fileop.c:10-70): every domain cell
+ * adds the quantities of p2avg (p2u.c:313-541) times dt to the running sums
+ * pavg, and dt is added to avgtime; the reference's loop calls it once per
+ * time step with AVGOUTPUT=1 (ko.c:504-507, 606-610), after the second
+ * stage's inversion and implicit step.  Per cell the sums hold NV + NAVGVARS
+ * values (NAVGVARS = 112 + 3 NV, or 153 + 3 NV with radiation, choices.h:
+ * 260-265) in the slots of mnemonics.h:170-199; kgpu_avg_count returns the
+ * count.  The face fluxes of the last op_explicit are given flux_ct's
+ * rewrite first, as the reference's flbx/flby/flbz hold it.  Two slots the
+ * reference leaves as an uninitialised local value are zero here:
+ * AVGEHAT without radiation and AVGGHATCOMPT (Comptonisation only).
+ *  kgpu_set_avg      allocates and zeroes the sums on first use; with on = 1
+ *                    the fused steps (kgpu_rk2_steps, kgpu_rk2imex_steps and
+ *                    their graph forms) call save_avg once per step as the
+ *                    reference's loop does.  mass (solar masses) sets the
+ *                    unit constants of the averaged gas temperature
+ *                    (K_BOLTZ, M_PROTON, ko.h:4-48); with radiation the
+ *                    context's radiation constants are used.
+ *  kgpu_save_avg     one save_avg(dt) now (after kgpu_set_avg).
+ *  kgpu_download_avg the sums in KORAL's layout [SZ][SY][SX][NV+NAVGVARS]
+ *                    (ghost cells zero) and avgtime; the reference divides by
+ *                    avgtime when it writes an avg file (ko.c:785).
+ *  kgpu_reset_avg    zeroes the sums and avgtime (ko.c:798-799). */
+int kgpu_avg_count(kgpu_ctx *ctx);
+int kgpu_set_avg(kgpu_ctx *ctx, int on, double mass);
+int kgpu_save_avg(kgpu_ctx *ctx, double dt);
+int kgpu_download_avg(kgpu_ctx *ctx, double *pavg, double *avgtime);
+int kgpu_reset_avg(kgpu_ctx *ctx);
+
 /* Last CUDA error string of this thread's most recent failing call. */
 const char *kgpu_last_error(void);
 int kgpu_abi_version(void);

@@ -154,6 +154,11 @@ def lib():
             "kgpu_read_restart": [vp, ctypes.c_char_p, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_int)],
             "kgpu_download_emf": [vp, _dp],
+            "kgpu_avg_count": [vp],
+            "kgpu_set_avg": [vp, ctypes.c_int, ctypes.c_double],
+            "kgpu_save_avg": [vp, ctypes.c_double],
+            "kgpu_download_avg": [vp, _dp, _dp],
+            "kgpu_reset_avg": [vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -333,6 +338,29 @@ class Subdomain:
         out = np.zeros(NSCALARS)
         _check(self.L.kgpu_calc_scalars(self.h, ctypes.byref(sp), float(t), _ptr(out)), "kgpu_calc_scalars")
         return out
+
+    # time averages (save_avg, fileop.c:10-70)
+    def set_avg(self, on=True, mass=10.0):
+        """Allocate the averages; with on, the fused steps call save_avg once
+        per step (AVGOUTPUT=1).  mass (solar masses) sets the units of the
+        averaged temperature when there is no radiation."""
+        _check(self.L.kgpu_set_avg(self.h, int(bool(on)), float(mass)), "kgpu_set_avg")
+
+    def save_avg(self, dt):
+        _check(self.L.kgpu_save_avg(self.h, float(dt)), "kgpu_save_avg")
+
+    def reset_avg(self):
+        _check(self.L.kgpu_reset_avg(self.h), "kgpu_reset_avg")
+
+    def download_avg(self):
+        """(pavg [SZ][SY][SX][NV+NAVGVARS], avgtime)"""
+        nav = self.L.kgpu_avg_count(self.h)
+        if nav < 0:
+            _check(nav, "kgpu_avg_count")
+        out = np.zeros(self.shape[:3] + (nav,))
+        t = ctypes.c_double()
+        _check(self.L.kgpu_download_avg(self.h, _ptr(out), ctypes.byref(t)), "kgpu_download_avg")
+        return out, t.value
 
     def download_metric(self):
         """The metric tables in KORAL's layout, in the argument order of

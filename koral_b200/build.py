@@ -14,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libkoral_b200.so")
-SOURCES = ["kgpu.cu", "kgpu_setup.cu", "kgpu_diag.cu", "kgpu_noalloc.cu", "kgpu_rad.cu", "kgpu_mlp.cu", "kgpu_u2p_warm.cu"]
+SOURCES = ["kgpu.cu", "kgpu_setup.cu", "kgpu_diag.cu", "kgpu_avg.cu", "kgpu_noalloc.cu", "kgpu_rad.cu", "kgpu_mlp.cu",
+           "kgpu_u2p_warm.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

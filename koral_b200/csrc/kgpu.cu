@@ -33,6 +33,7 @@
 #include "kgpu_rad.cuh"
 #include "kgpu_setup.cuh"
 #include "kgpu_diag.cuh"
+#include "kgpu_avg.cuh"
 
 using namespace kgpu;
 
@@ -1352,6 +1353,14 @@ __global__ void k_minkowski(double *met, long npts) {
   met[32 * npts + t] = 1.;
   met[38 * npts + t] = 1.;
 }
+// cells c0 .. c0+m-1 of a [nv][n] array into [m][nv]
+__global__ void k_soa_slab_to_aos(const double *soa, long n, long c0, long m, int nv, double *aos) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= m * nv) return;
+  const long cc = t / nv;
+  const int v = (int)(t - cc * nv);
+  aos[t] = soa[(long)v * n + c0 + cc];
+}
 __global__ void k_fill(double *a, long n, double v) {
   long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (t < n) a[t] = v;
@@ -1363,13 +1372,14 @@ __global__ void k_fill(double *a, long n, double v) {
 enum KernelId { K_BC = 0, K_WAVESPEEDS, K_FLUX0, K_FLUX1, K_FLUX2, K_EMF, K_UPDATE, K_U2P, K_U2P_RESUME,
                 K_U2P_ENT, K_U2P_RESUME_ENT, K_FIXUP, K_COMMIT, K_BEGIN, K_FLUXRAD0, K_FLUXRAD1, K_FLUXRAD2,
                 K_UPDATE_RAD, K_U2P_RAD, K_IMP_GATHER, K_IMP_WARM, K_IMP_SOLVE, K_IMP_SCATTER, K_IMEX, K_RECON0,
-                K_RECON1, K_RECON2, K_NKERNELS };
+                K_RECON1, K_RECON2, K_AVG, K_NKERNELS };
 static const char *kKernelNames[K_NKERNELS] = {"k_bc", "k_wavespeeds", "k_flux_x", "k_flux_y", "k_flux_z", "k_emf",
                                                "k_update", "k_u2p", "k_u2p_resume", "k_u2p_entropy",
                                                "k_u2p_resume_entropy", "k_fixup", "k_commit", "k_begin_step",
                                                "k_flux_rad_x", "k_flux_rad_y", "k_flux_rad_z", "k_update_rad",
                                                "k_u2p_rad", "k_imp_gather", "k_imp_warm_start", "k_imp_solve",
-                                               "k_imp_scatter", "k_imex", "k_recon_x", "k_recon_y", "k_recon_z"};
+                                               "k_imp_scatter", "k_imex", "k_recon_x", "k_recon_y", "k_recon_z",
+                                               "k_save_avg"};
 
 int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, const double *pp, const double *g,
                            const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
@@ -1475,6 +1485,12 @@ struct kgpu_ctx {
   int warm_gate = -1;            // warm-start only cells whose previous solve took more than this (-1: all)
   long long metric_gen = 0, packed_gen = -1;
   double *diag_work = nullptr, *diag_out = nullptr;   // calc_scalars on the device
+  // time averages (save_avg): running sums [NV + NAVGVARS][ncell], the
+  // summed time, the unit constants of the averaged temperatures, and
+  // whether the fused steps add to them once per step
+  double *pavg = nullptr, *avgtime = nullptr;
+  RadParams avg_units;
+  bool avg_on = false, avg_ready = false;
 };
 
 static cudaEvent_t pool_event(kgpu_ctx *c) {
@@ -2256,6 +2272,24 @@ extern "C" int kgpu_begin_step(kgpu_ctx *c, double *dt_out) {
 }
 
 // one RK2 step (ko.c:571-626) with dt in device memory
+// save_avg (fileop.c:10-70) on the stream: the face fluxes get flux_ct's
+// rewrite from the corner EMFs of the last op_explicit (the reference's
+// flbx/flby/flbz hold it when its loop calls save_avg), then every domain
+// cell adds its p2avg quantities times dt (device memory) to the sums.
+static int enqueue_avg(kgpu_ctx *c, const double *dtp) {
+  Grid &G = c->G;
+  if (!c->flux_ct_done) {
+    Box eb{0, 0, 0, G.nx + 1, G.ny + 1, G.nz + 1};
+    { LaunchScope ls(c, K_AVG); k_flux_ct_rewrite<<<nblocks(eb.n(), 128), 128, 0, c->stream>>>(G, eb); }
+    CKL("k_flux_ct_rewrite");
+    c->flux_ct_done = true;
+  }
+  int r;
+  { LaunchScope ls(c, K_AVG); r = avg_enqueue(G, c->avg_units, dtp, c->pavg, c->avgtime, c->stream); }
+  if (r < 0) return set_err("k_save_avg", cudaGetLastError());
+  return 0;
+}
+
 static int enqueue_rk2(kgpu_ctx *c) {
   Grid &G = c->G;
   int r;
@@ -2265,6 +2299,9 @@ static int enqueue_rk2(kgpu_ctx *c) {
   if ((r = launch_u2p(c, 0))) return r;
   if ((r = launch_explicit(c, G.scal + S_DT, 1.0, G.ut1))) return r;   // ut1 = U^{n+1/2}
   if ((r = launch_u2p(c, 1))) return r;                                // u = ut0 + (u - ut1)
+  // save_avg(dt) after the second stage's inversion (ko.c:606-610); the
+  // combination above changed u only, and p2avg reads p
+  if (c->avg_on && (r = enqueue_avg(c, G.scal + S_DT))) return r;
   return 0;
 }
 
@@ -2464,6 +2501,7 @@ static int enqueue_rk2imex(kgpu_ctx *c) {
   CKL("k_imex_stage1");                                                     // F(U(1)); u; uforget = u
   if ((r = launch_u2p(c, 0))) return r;
   if ((r = enqueue_implicit(c, dtp, gam))) return r;                       // U(2)
+  if (c->avg_on && (r = enqueue_avg(c, dtp))) return r;                    // save_avg(dt), ko.c:504-507
   { LaunchScope ls(c, K_IMEX); k_imex_rate<<<nb, 128, 0, c->stream>>>(G, db, dtp, gam, G.ut1, c->drt2, G.ut1); }
   CKL("k_imex_rate");                                                       // R(U(2)); ut2 = U(2)
   if ((r = launch_u2p(c, 0))) return r;
@@ -3206,6 +3244,92 @@ extern "C" int kgpu_calc_scalars_device(kgpu_ctx *c, const kgpu_scalars_params *
   r = diag_scalars_enqueue(c->G, I, K, c->diag_work, scalars_dev, c->stream);
   if (r < 0) return r;
   c->launches += r;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// time averages (save_avg, fileop.c:10-70; p2avg, p2u.c:313-541)
+// ---------------------------------------------------------------------------
+static int avg_count(const kgpu_ctx *c) { return c->G.nv + navg_vars(c->G.nv, c->G.rad != 0); }
+
+static int avg_prepare(kgpu_ctx *c, double mass) {
+  int r = ready(c);
+  if (r) return r;
+  if (!c->avg_ready) {
+    if (!(mass > 0.)) return KGPU_EINVAL;
+    if (c->G.rad) {
+      c->avg_units = kgpu_rad_device_params(c->rp);
+    } else {
+      kgpu_rad_params u;
+      if ((r = kgpu_rad_default_params(&u, mass, c->G.gamma, 0., 0.))) return r;
+      c->avg_units = kgpu_rad_device_params(u);
+    }
+    void *p;
+    if ((r = dalloc(c, &p, (size_t)avg_count(c) * c->G.ncell * sizeof(double)))) return r;
+    c->pavg = (double *)p;
+    if ((r = dalloc(c, &p, 2 * sizeof(double)))) return r;
+    c->avgtime = (double *)p;
+    CK(cudaMemsetAsync(c->pavg, 0, (size_t)avg_count(c) * c->G.ncell * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->avgtime, 0, 2 * sizeof(double), c->stream));
+    c->avg_ready = true;
+  }
+  return 0;
+}
+
+extern "C" int kgpu_avg_count(kgpu_ctx *c) {
+  if (!c) return KGPU_EINVAL;
+  return avg_count(c);
+}
+
+extern "C" int kgpu_set_avg(kgpu_ctx *c, int on, double mass) {
+  if (!c || (on != 0 && on != 1)) return KGPU_EINVAL;
+  int r = avg_prepare(c, mass);
+  if (r) return r;
+  if (c->avg_on != (on != 0)) drop_graph(c);
+  c->avg_on = on != 0;
+  return 0;
+}
+
+extern "C" int kgpu_save_avg(kgpu_ctx *c, double dt) {
+  if (!c) return KGPU_EINVAL;
+  if (!c->avg_ready) return KGPU_ESTATE;
+  // the time step of this call in the spare device slot (avgtime[1])
+  k_fill<<<1, 1, 0, c->stream>>>(c->avgtime + 1, 1, dt);
+  CKL("k_fill");
+  int r = enqueue_avg(c, c->avgtime + 1);
+  if (r) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_reset_avg(kgpu_ctx *c) {
+  if (!c) return KGPU_EINVAL;
+  if (!c->avg_ready) return KGPU_ESTATE;
+  CK(cudaMemsetAsync(c->pavg, 0, (size_t)avg_count(c) * c->G.ncell * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->avgtime, 0, sizeof(double), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_download_avg(kgpu_ctx *c, double *pavg, double *avgtime) {
+  if (!c || !pavg) return KGPU_EINVAL;
+  if (!c->avg_ready) return KGPU_ESTATE;
+  const int nav = avg_count(c);
+  const long n = c->G.ncell;
+  // KORAL's layout [cell][quantity], transposed on the device in slabs of
+  // cells so that the staging stays small
+  const long slab = n < (1L << 18) ? n : (1L << 18);
+  DevBuf tmp;
+  CK(cudaMalloc(&tmp.p, (size_t)nav * slab * sizeof(double)));
+  for (long c0 = 0; c0 < n; c0 += slab) {
+    const long m = n - c0 < slab ? n - c0 : slab;
+    k_soa_slab_to_aos<<<nblocks(m * nav, 256), 256, 0, c->stream>>>(c->pavg, n, c0, m, nav, (double *)tmp.p);
+    CKL("k_soa_slab_to_aos");
+    CK(cudaMemcpyAsync(pavg + (size_t)c0 * nav, tmp.p, (size_t)nav * m * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+  }
+  if (avgtime) CK(cudaMemcpyAsync(avgtime, c->avgtime, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
 
