@@ -154,11 +154,37 @@ int kgpu_save_timesteps(kgpu_ctx *ctx);
 int kgpu_copyi_u(kgpu_ctx *ctx, double factor, int src, int dst);
 int kgpu_addi_u(kgpu_ctx *ctx, double f1, int a, double f2, int b, int c);
 int kgpu_addi_u_3(kgpu_ctx *ctx, double f1, int a, double f2, int b, double f3, int c, int d);
-/* do_correct(), finite.c:605: the polar-axis corrections it can run are
- * compiled only with CORRECT_POLARAXIS(_3D) or SMOOTH_POLARAXIS, which no
- * configuration of this library defines, so it returns 0; the problem's
- * my_finger hook stays host code. */
+/* do_correct(), finite.c:605-640: the polar-axis corrections switched on by
+ * kgpu_set_polar_correction (none by default, when it returns at once); the
+ * problem's my_finger hook stays host code.  The fused steps call it where
+ * the reference's loop does (ko.c:444-626). */
 int kgpu_do_correct(kgpu_ctx *ctx);
+/* The polar-axis corrections of a problem build (spherical-like
+ * coordinates, theta along y), NCCORRECTPOLAR = nc rows at each axis:
+ *  KGPU_POLAR_CORRECT     CORRECT_POLARAXIS, correct_polaraxis
+ *                         (finite.c:4923-5166): the nc most polar cells of a
+ *                         column take density, energy, entropy, radial and
+ *                         azimuthal velocities (and radiation) from the cell
+ *                         nc rows from the axis, the theta velocities scaled
+ *                         by the distance from the axis; flux-CT's EMFs 1 and
+ *                         3 vanish on the polar edges (magn.c:343-376)
+ *  KGPU_POLAR_CORRECT_3D  CORRECT_POLARAXIS_3D without POLARAXISAVGIN3D,
+ *                         correct_polaraxis_3d (finite.c:5170-5474): those
+ *                         cells take the whole state of that cell
+ *  KGPU_POLAR_SMOOTH      SMOOTH_POLARAXIS, smooth_polaraxis
+ *                         (finite.c:4832-4921): the nc most polar rows take
+ *                         their phi average
+ * Every corrected state is converted with p2u and the magnetic field is
+ * left as it is.  With CORRECT or CORRECT_3D the corrected cells are not
+ * evolved as the reference treats them (is_cell_corrected_polaraxis,
+ * finite.c:5604-5625): their inversion recovers the field only
+ * (u2p_solver_Bonly, u2p.c:49-101) and the implicit source step skips
+ * them (finite.c:1270).  Needs NY >= 2 nc + 2.  Drops the captured step
+ * graph. */
+#define KGPU_POLAR_CORRECT 1
+#define KGPU_POLAR_CORRECT_3D 2
+#define KGPU_POLAR_SMOOTH 4
+int kgpu_set_polar_correction(kgpu_ctx *ctx, int flags, int nc);
 /* flux_ct(), magn.c:199-339: corner EMFs from the face fluxes of the last
  * op_explicit and the magnetic components of those fluxes rewritten from
  * them, as the reference leaves flbx/flby/flbz (kgpu_download_flux reads

@@ -21,6 +21,7 @@ PPM, MP5 = 2, 4
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECT, BC_PERIODIC_COPY = 0, 1, 2, 3
 LAXF, HLL = 0, 1
 ARR_U, ARR_P, ARR_UT0, ARR_UT1, ARR_UT2 = 0, 1, 2, 3, 4
+POLAR_CORRECT, POLAR_CORRECT_3D, POLAR_SMOOTH = 1, 2, 4   # KGPU_POLAR_* (kgpu_set_polar_correction)
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -154,6 +155,7 @@ def lib():
             "kgpu_read_restart": [vp, ctypes.c_char_p, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_int)],
             "kgpu_download_emf": [vp, _dp],
+            "kgpu_set_polar_correction": [vp, ctypes.c_int, ctypes.c_int],
             "kgpu_avg_count": [vp],
             "kgpu_set_avg": [vp, ctypes.c_int, ctypes.c_double],
             "kgpu_save_avg": [vp, ctypes.c_double],
@@ -338,6 +340,11 @@ class Subdomain:
         out = np.zeros(NSCALARS)
         _check(self.L.kgpu_calc_scalars(self.h, ctypes.byref(sp), float(t), _ptr(out)), "kgpu_calc_scalars")
         return out
+
+    def set_polar_correction(self, flags, nc=2):
+        """The polar-axis corrections of do_correct (POLAR_CORRECT,
+        POLAR_CORRECT_3D, POLAR_SMOOTH bits; nc = NCCORRECTPOLAR)."""
+        _check(self.L.kgpu_set_polar_correction(self.h, int(flags), int(nc)), "kgpu_set_polar_correction")
 
     # time averages (save_avg, fileop.c:10-70)
     def set_avg(self, on=True, mass=10.0):

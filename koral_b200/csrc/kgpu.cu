@@ -980,6 +980,16 @@ __global__ void __launch_bounds__(128, MB) k_u2p(Grid G, Box b, U2PQueues Q, int
   int ix, iy, iz;
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (!box_coord(b, t, ix, iy, iz)) return;
+  if (polar_cell(G, iy)) {
+    // a corrected polar cell: only its field is inverted (u2p_solver_Bonly,
+    // u2p.c:2356-2377), no floors, no fixup, conserved state as it is
+    // (calc_primitives, u2p.c:49-101)
+    const long c = cell_index(G, ix, iy, iz);
+    const double gdet = G.met_c[(long)(3 * 5 + 4) * G.nmet + met_index(G, ix, iy, iz)];
+    for (int iv = B1; iv <= B3; iv++) G.p[iv * G.ncell + c] = G.u[iv * G.ncell + c] / gdet;
+    G.flag[c] = 0;
+    return;
+  }
   U2PCell x;
   u2p_load(G, ix, iy, iz, G.p, x);
   if (x.negrho) {
@@ -1067,6 +1077,7 @@ __global__ void __launch_bounds__(128) k_u2p_entropy(Grid G, Box b, U2PQueues Q,
 __global__ void __launch_bounds__(128) k_u2p_rad(Grid G, Box b) {
   int ix, iy, iz;
   if (!box_coord(b, blockIdx.x * (long)blockDim.x + threadIdx.x, ix, iy, iz)) return;
+  if (polar_cell(G, iy)) return;   // corrected polar cells: field only (u2p.c:49-101)
   const long c = cell_index(G, ix, iy, iz);
   double uu[NVR], pp[NVR];
   load_rad(G.u, G.ncell, c, uu);
@@ -1130,6 +1141,10 @@ __global__ void k_imp_scatter(Grid G, Box b, const double *pp, const double *uu,
   int ix, iy, iz;
   if (!box_coord(b, k, ix, iy, iz)) return;
   const long c = cell_index(G, ix, iy, iz);
+  if (polar_cell(G, iy)) {   // op_implicit skips corrected polar cells (finite.c:1270-1272)
+    G.flag[c] = 0;
+    return;
+  }
   const bool ok = status[k] == 0;
   count_lanes(&G.cnt[C_RADIMP_FAIL], !ok);
   count_lanes(&G.cnt[C_IMP_SOLVES], true);
@@ -1324,6 +1339,110 @@ __global__ void k_flux_ct_rewrite(Grid G, Box b) {
 #undef EMFV
 }
 
+// ---------------------------------------------------------------------------
+// polar-axis corrections (do_correct, finite.c:605-640)
+// ---------------------------------------------------------------------------
+// cell-centre code coordinate along d (set_x of set_grid, finite.c:1646-1664)
+__device__ inline double centre_x(const Grid &G, int ic, int d) {
+  return .5 * (G.xb[d][ic + 1 + G.ng] + G.xb[d][ic + G.ng]);
+}
+// writes pp and its conserved state into cell c except the magnetic field
+__device__ inline void polar_store(const Grid &G, long c, const double *pp, const Geom &g) {
+  double uu[NVR];
+  if (G.rad) p2u_rad_full(G, pp, uu, g);
+  else p2u_full(G, pp, uu, g);
+  for (int iv = 0; iv < G.nv; iv++) {
+    if (iv >= B1 && iv <= B3) continue;   // the field is not overwritten
+    G.p[iv * G.ncell + c] = pp[iv];
+    G.u[iv * G.ncell + c] = uu[iv];
+  }
+}
+// correct_polaraxis (finite.c:4923-5166, spherical-like coordinates;
+// mode 1) and correct_polaraxis_3d without POLARAXISAVGIN3D
+// (finite.c:5170-5474; mode 2): each of the nc most polar cells of a
+// column takes its state from the cell nc rows from the axis; mode 1 scales
+// the theta velocities by the distance from the axis.  One thread per
+// (ix, iz, ic, side); the source cells are not written.
+__global__ void k_correct_polar(Grid G, int nc, int mode) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long n = (long)G.nx * G.nz * nc * 2;
+  if (t >= n) return;
+  const int ix = (int)(t % G.nx);
+  long r = t / G.nx;
+  const int iz = (int)(r % G.nz);
+  r /= G.nz;
+  const int ic = (int)(r % nc);
+  const int lower = (int)(r / nc);
+  const int iy = lower ? G.ny - 1 - ic : ic;
+  const int iysrc = lower ? G.ny - 1 - nc : nc;
+  const long c = cell_index(G, ix, iy, iz), cs = cell_index(G, ix, iysrc, iz);
+  Geom g;
+  geom_centre(G, ix, iy, iz, g);
+  double pp[NVR];
+  if (mode == 2) {
+    for (int iv = 0; iv < G.nv; iv++) pp[iv] = G.p[iv * G.ncell + cs];
+  } else {
+    const double thaxis = G.xb[1][(lower ? G.ny : 0) + G.ng];
+    const double th = centre_x(G, iy, 1), thsrc = centre_x(G, iysrc, 1);
+    for (int iv = 0; iv < G.nv; iv++) pp[iv] = G.p[iv * G.ncell + c];
+    const double f = fabs((th - thaxis) / (thsrc - thaxis));
+    pp[RHO] = G.p[RHO * G.ncell + cs];
+    pp[UU] = G.p[UU * G.ncell + cs];
+    pp[ENTR] = G.p[ENTR * G.ncell + cs];
+    pp[VX] = G.p[VX * G.ncell + cs];
+    pp[VZ] = G.p[VZ * G.ncell + cs];
+    pp[VY] = f * G.p[VY * G.ncell + cs];
+    if (G.rad) {
+      pp[EE0] = G.p[EE0 * G.ncell + cs];
+      pp[FX0] = G.p[FX0 * G.ncell + cs];
+      pp[FZ0] = G.p[FZ0 * G.ncell + cs];
+      pp[FY0] = f * G.p[FY0 * G.ncell + cs];
+    }
+  }
+  polar_store(G, c, pp, g);
+}
+// smooth_polaraxis (finite.c:4832-4921): each of the nc most polar rows
+// takes, in every cell, the phi average of the row (summed in phi order),
+// with the cell's own magnetic field.  One thread per (ix, ic, side), so
+// the row is read in full before it is written.
+__global__ void k_smooth_polar(Grid G, int nc) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= (long)G.nx * nc * 2) return;
+  const int ix = (int)(t % G.nx);
+  const int ic = (int)((t / G.nx) % nc);
+  const int lower = (int)(t / ((long)G.nx * nc));
+  const int iy = lower ? G.ny - 1 - ic : ic;
+  double pp[NVR];
+  for (int iv = 0; iv < G.nv; iv++) pp[iv] = 0.;
+  for (int iz = 0; iz < G.nz; iz++) {
+    const long c = cell_index(G, ix, iy, iz);
+    for (int iv = 0; iv < G.nv; iv++) pp[iv] += G.p[iv * G.ncell + c];
+  }
+  for (int iv = 0; iv < G.nv; iv++) pp[iv] /= G.nz;
+  for (int iz = 0; iz < G.nz; iz++) {
+    const long c = cell_index(G, ix, iy, iz);
+    Geom g;
+    geom_centre(G, ix, iy, iz, g);
+    pp[B1] = G.p[B1 * G.ncell + c];
+    pp[B2] = G.p[B2 * G.ncell + c];
+    pp[B3] = G.p[B3 * G.ncell + c];
+    polar_store(G, c, pp, g);
+  }
+}
+// adjust_fluxcttoth_emfs (magn.c:343-376, CORRECT_POLARAXIS): EMF
+// components 1 and 3 vanish on the corners of both polar edges
+__global__ void k_emf_polar(Grid G) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long ne = (long)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
+  if (t >= (long)(G.nx + 1) * (G.nz + 1) * 2) return;
+  const int ix = (int)(t % (G.nx + 1));
+  const int iz = (int)((t / (G.nx + 1)) % (G.nz + 1));
+  const int iy = t / ((long)(G.nx + 1) * (G.nz + 1)) ? G.ny : 0;
+  const long e = emf_index(G, ix, iy, iz);
+  G.emf[0 * ne + e] = 0.;
+  G.emf[2 * ne + e] = 0.;
+}
+
 // KORAL layout [cell][var] <-> device [var][cell]
 __global__ void k_aos_to_soa(const double *aos, double *soa, long n, int nv) {
   long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -1491,6 +1610,8 @@ struct kgpu_ctx {
   double *pavg = nullptr, *avgtime = nullptr;
   RadParams avg_units;
   bool avg_on = false, avg_ready = false;
+  // polar-axis corrections of do_correct: KGPU_POLAR_* bits and the rows
+  int polar_flags = 0, polar_nc = 2;
 };
 
 static cudaEvent_t pool_event(kgpu_ctx *c) {
@@ -2108,6 +2229,10 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
   Box eb{0, 0, 0, G.nx + 1, G.ny + 1, G.nz + 1};
   { LaunchScope ls(c, K_EMF); k_emf<<<nblocks(eb.n(), 128), 128, 0, c->stream>>>(G, eb); }
   CKL("k_emf");
+  if (G.polar_emf) {
+    { LaunchScope ls(c, K_EMF); k_emf_polar<<<nblocks(2L * (G.nx + 1) * (G.nz + 1), 128), 128, 0, c->stream>>>(G); }
+    CKL("k_emf_polar");
+  }
   Box db = domain_box(G);
   { LaunchScope ls(c, K_UPDATE); launch_update(c->update_blocks, nblocks(db.n(), 128), c->stream, G, db, dtp, fac, save); }
   CKL("k_update");
@@ -2220,7 +2345,28 @@ extern "C" int kgpu_addi_u_3(kgpu_ctx *c, double f1, int a, double f2, int b, do
 // only with CORRECT_POLARAXIS / CORRECT_POLARAXIS_3D / SMOOTH_POLARAXIS,
 // which the configurations this library runs do not define; the problem's
 // my_finger hook is host code and stays on the host.
-extern "C" int kgpu_do_correct(kgpu_ctx *c) { return c ? 0 : KGPU_EINVAL; }
+static int launch_correct(kgpu_ctx *c);
+
+extern "C" int kgpu_do_correct(kgpu_ctx *c) {
+  int r = ready(c);
+  if (r) return r;
+  if (!c->polar_flags) return 0;
+  if ((r = launch_correct(c))) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+extern "C" int kgpu_set_polar_correction(kgpu_ctx *c, int flags, int nc) {
+  if (!c) return KGPU_EINVAL;
+  if (flags & ~(KGPU_POLAR_CORRECT | KGPU_POLAR_CORRECT_3D | KGPU_POLAR_SMOOTH)) return KGPU_EINVAL;
+  if (flags && (nc < 1 || c->G.ny < 2 * nc + 2)) return KGPU_EINVAL;
+  c->polar_flags = flags;
+  c->polar_nc = flags ? nc : 2;
+  c->G.polar_nc = (flags & (KGPU_POLAR_CORRECT | KGPU_POLAR_CORRECT_3D)) ? nc : 0;
+  c->G.polar_emf = (flags & KGPU_POLAR_CORRECT) ? 1 : 0;
+  drop_graph(c);
+  return 0;
+}
 
 extern "C" int kgpu_flux_ct(kgpu_ctx *c) {
   if (!c) return KGPU_EINVAL;
@@ -2229,6 +2375,10 @@ extern "C" int kgpu_flux_ct(kgpu_ctx *c) {
   Box eb{0, 0, 0, G.nx + 1, G.ny + 1, G.nz + 1};
   k_emf<<<nblocks(eb.n(), 128), 128, 0, c->stream>>>(G, eb);
   CKL("k_emf");
+  if (G.polar_emf) {
+    k_emf_polar<<<nblocks(2L * (G.nx + 1) * (G.nz + 1), 128), 128, 0, c->stream>>>(G);
+    CKL("k_emf_polar");
+  }
   k_flux_ct_rewrite<<<nblocks(eb.n(), 128), 128, 0, c->stream>>>(G, eb);
   CKL("k_flux_ct_rewrite");
   c->flux_ct_done = true;
@@ -2272,6 +2422,26 @@ extern "C" int kgpu_begin_step(kgpu_ctx *c, double *dt_out) {
 }
 
 // one RK2 step (ko.c:571-626) with dt in device memory
+// do_correct (finite.c:605-640) on the stream: the polar-axis corrections
+// the context has switched on, in the reference's order
+static int launch_correct(kgpu_ctx *c) {
+  Grid &G = c->G;
+  const int nc = c->polar_nc;
+  if (c->polar_flags & KGPU_POLAR_CORRECT) {
+    k_correct_polar<<<nblocks(2L * G.nx * G.nz * nc, 128), 128, 0, c->stream>>>(G, nc, 1);
+    CKL("k_correct_polar");
+  }
+  if (c->polar_flags & KGPU_POLAR_CORRECT_3D) {
+    k_correct_polar<<<nblocks(2L * G.nx * G.nz * nc, 128), 128, 0, c->stream>>>(G, nc, 2);
+    CKL("k_correct_polar");
+  }
+  if (c->polar_flags & KGPU_POLAR_SMOOTH) {
+    k_smooth_polar<<<nblocks(2L * G.nx * nc, 128), 128, 0, c->stream>>>(G, nc);
+    CKL("k_smooth_polar");
+  }
+  return 0;
+}
+
 // save_avg (fileop.c:10-70) on the stream: the face fluxes get flux_ct's
 // rewrite from the corner EMFs of the last op_explicit (the reference's
 // flbx/flby/flbz hold it when its loop calls save_avg), then every domain
@@ -2295,7 +2465,18 @@ static int enqueue_rk2(kgpu_ctx *c) {
   int r;
   { LaunchScope ls(c, K_BEGIN); k_begin_step<<<1, 1, 0, c->stream>>>(G); }
   CKL("k_begin_step");
-  if ((r = launch_explicit(c, G.scal + S_DT, 0.5, G.ut0))) return r;   // ut0 = U^n
+  if (c->polar_flags) {
+    // copyi_u(1.,u,ut0) before do_correct (ko.c:577-579): ut0 keeps the
+    // uncorrected state
+    CK(cudaMemcpyAsync(G.ut0, G.u, G.ncell * G.nv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    if ((r = launch_correct(c))) return r;
+    // op_explicit begins with set_bc (finite.c:672), here after the
+    // corrected cells changed the ghosts' sources
+    if ((r = launch_bc(c))) return r;
+    if ((r = launch_explicit(c, G.scal + S_DT, 0.5, nullptr))) return r;
+  } else if ((r = launch_explicit(c, G.scal + S_DT, 0.5, G.ut0))) {   // ut0 = U^n
+    return r;
+  }
   if ((r = launch_u2p(c, 0))) return r;
   if ((r = launch_explicit(c, G.scal + S_DT, 1.0, G.ut1))) return r;   // ut1 = U^{n+1/2}
   if ((r = launch_u2p(c, 1))) return r;                                // u = ut0 + (u - ut1)
@@ -2495,21 +2676,26 @@ static int enqueue_rk2imex(kgpu_ctx *c) {
   { LaunchScope ls(c, K_IMEX); k_imex_rate<<<nb, 128, 0, c->stream>>>(G, db, dtp, gam, G.ut0, c->drt1, G.ut1); }
   CKL("k_imex_rate");                                                       // R(U(1)); ut1 = U(1)
   if ((r = launch_u2p(c, 0))) return r;
+  if (c->polar_flags && ((r = launch_correct(c)) || (r = launch_bc(c)))) return r;
   if ((r = launch_explicit(c, dtp, 1.0, nullptr))) return r;
   { LaunchScope ls(c, K_IMEX);
     k_imex_stage1<<<nb, 128, 0, c->stream>>>(G, db, dtp, gam, G.ut0, G.ut1, c->dut1, c->drt1, G.ut1); }
   CKL("k_imex_stage1");                                                     // F(U(1)); u; uforget = u
   if ((r = launch_u2p(c, 0))) return r;
+  if (c->polar_flags && (r = launch_correct(c))) return r;
   if ((r = enqueue_implicit(c, dtp, gam))) return r;                       // U(2)
   if (c->avg_on && (r = enqueue_avg(c, dtp))) return r;                    // save_avg(dt), ko.c:504-507
   { LaunchScope ls(c, K_IMEX); k_imex_rate<<<nb, 128, 0, c->stream>>>(G, db, dtp, gam, G.ut1, c->drt2, G.ut1); }
   CKL("k_imex_rate");                                                       // R(U(2)); ut2 = U(2)
   if ((r = launch_u2p(c, 0))) return r;
+  if (c->polar_flags && ((r = launch_correct(c)) || (r = launch_bc(c)))) return r;
   if ((r = launch_explicit(c, dtp, 1.0, nullptr))) return r;
   { LaunchScope ls(c, K_IMEX);
     k_imex_final<<<nb, 128, 0, c->stream>>>(G, db, dtp, G.ut0, G.ut1, c->dut1, c->drt1, c->drt2); }
   CKL("k_imex_final");
-  return launch_u2p(c, 0);
+  if ((r = launch_u2p(c, 0))) return r;
+  if (c->polar_flags && (r = launch_correct(c))) return r;
+  return 0;
 }
 
 static int ready_rad(kgpu_ctx *c) {

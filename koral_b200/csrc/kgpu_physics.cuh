@@ -57,7 +57,16 @@ struct Grid {
   int rad_limiter;                   // optical-depth limiter of the radiative wave speeds
   const RadParams *radp;             // device copy of the radiation constants
   double *arl[3], *arr[3];           // radiative wave speeds per cell and direction
+  // polar-axis correction (CORRECT_POLARAXIS / _3D): the cells within
+  // polar_nc rows of either theta boundary are corrected, not evolved
+  // (0: none); polar_emf: flux-CT's EMFs zeroed on the polar edges
+  int polar_nc, polar_emf;
 };
+
+// is_cell_corrected_polaraxis (finite.c:5604-5625)
+KG_HD bool polar_cell(const Grid &G, int iy) {
+  return G.polar_nc > 0 && (iy < G.polar_nc || iy > G.ny - G.polar_nc - 1);
+}
 
 enum ScalarSlot { S_TSTEPDENMAX = 0, S_TSTEPDENMIN = 1, S_DT = 2, S_T = 3, S_NSCAL = 8 };
 enum CounterSlot {
