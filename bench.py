@@ -162,6 +162,9 @@ def parse():
                          "distribution; print the solver's counters as JSON (no bench line)")
     ap.add_argument("--profile-cells", type=int, default=0,
                     help="with --profile-solve: solve only the first this many cells (0: all)")
+    ap.add_argument("--profile-file", default=None,
+                    help="with --profile-solve on the radiative torus: the cells are read from this .npz when it "
+                         "exists (no warm-up steps), else written to it after the warm-up")
     return ap.parse_args()
 
 
@@ -185,6 +188,12 @@ def profile_solve(args):
         rp = k.rad_params()
         m = args.profile_cells if args.profile_cells > 0 else WORKLOADS["radcells"]["ncells"]
         d = [torch.from_numpy(a).cuda() for a in k.rad_cells(m, 2026, rp)]
+    elif args.profile_file and os.path.exists(args.profile_file):
+        import numpy as np
+        f = np.load(args.profile_file)
+        m = args.profile_cells if args.profile_cells > 0 else f["uu"].shape[0]
+        d = [torch.from_numpy(f[key][:m]).cuda() for key in ("uu", "pp", "g", "G", "dt")]
+        rp = k.rad_params(mass=k.RADTORUS_MASS, gamma=13.0 / 9.0)
     else:
         s = make_subdomain(k, "radtorus")
         mlp, _ = warmstart_network(k)
@@ -204,6 +213,9 @@ def profile_solve(args):
                                 ("dt", (n,)))]
         rp = s._rp
         s.close()
+        if args.profile_file:
+            import numpy as np
+            np.savez(args.profile_file, **{key: t.cpu().numpy() for key, t in zip(("uu", "pp", "g", "G", "dt"), d)})
     mode = {"plain": k.RAD_PLAIN, "batched": k.RAD_BATCHED, "persistent": k.RAD_PERSISTENT}[args.profile_solve]
     torch.cuda.synchronize()
     a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -372,8 +372,10 @@ int kgpu_rad_default_params(kgpu_rad_params *rp, double mass, double gamma, doub
  *                 residual evaluation may take in a single lane before that
  *                 evaluation is repeated by a whole warp with the damped
  *                 trials tried 32 at a time (64; 0: never)
- *  tail           batched: once the cells left after a pass fit in one wave
- *                 of warps, each is run to its end by a whole warp (1; 0: off)
+ *  tail           batched: the size of the warp-per-cell tail, in blocks of
+ *                 four warps per SM (0..32, default 8; 0: none): once the
+ *                 cells left after a pass are no more than its warps, each is
+ *                 run to its end by a whole warp
  *  warm_attempts  learned warm start: attempts of the cascade a warm-started
  *                 cell runs from the predicted iterate before the reference
  *                 cascade runs from the reference guess (1..6, default 6)
@@ -612,7 +614,7 @@ int kgpu_set_tuning(kgpu_ctx *ctx, const kgpu_tuning *t);
  * are restored afterwards, and the choice is applied.  Candidates: the
  * fused or split face flux, flux 5..8, update 3..5, u2p 4..6 blocks; u2p_pass_iters 4, 8, 16; with
  * radiation the batched and the persistent solver, pass_iters 4, 8, 16,
- * inner_cap 32, 64, 128, tail on/off or thin 4, 8, 16.  A candidate
+ * inner_cap 32, 64, 128, tail 0, 4, 8, 16 or thin 4, 8, 16.  A candidate
  * replaces the incumbent only when it is faster by min_gain (a fraction,
  * e.g. 0.02) in the same round of trials.  The choice is cached per device
  * and grid configuration for the process: with reuse = 1 a cached choice

@@ -2899,7 +2899,7 @@ extern "C" int kgpu_autotune(kgpu_ctx *c, int steps, double min_gain, int reuse,
     if (G.rad && knobs[ki].field(best) == &best.implicit.inner_cap) {
       if (best.implicit_mode == KGPU_RAD_BATCHED) {
         round.push_back({[](kgpu_tuning &t) { return &t.implicit.pass_iters; }, {4, 8, 16}});
-        round.push_back({[](kgpu_tuning &t) { return &t.implicit.tail; }, {0, 1}});
+        round.push_back({[](kgpu_tuning &t) { return &t.implicit.tail; }, {0, 4, 8, 16}});
       } else {
         round.push_back({[](kgpu_tuning &t) { return &t.implicit.thin; }, {4, 8, 16}});
       }

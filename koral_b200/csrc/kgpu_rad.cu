@@ -32,8 +32,19 @@
 using namespace kgpu;
 
 // resident blocks of 128 threads per SM the solver kernels are compiled for
+// (128 registers at 4: on the settled 256x128x64 radiative torus 16 warps
+// per SM hide more of the solver's instruction-fetch and FP64 latency than
+// the added spills cost: 197 against 224 ms per step at 1 block, 201 at 5,
+// 203 at 6, with a tail of as many blocks; batched-solve cells within 5%)
 #ifndef KGPU_RAD_MIN_BLOCKS
-#define KGPU_RAD_MIN_BLOCKS 1
+#define KGPU_RAD_MIN_BLOCKS 4
+#endif
+// default size of the warp-per-cell tail, in blocks of four warps per SM
+// (kgpu_rad_solver_opts.tail): 8 = two waves at 4 resident blocks; measured
+// on the same steps with 4 Newton iterations per pass: 193.5 ms per step at
+// 4 blocks, 189.1 at 6, 187.3 at 8
+#ifndef KGPU_RAD_TAIL_BLOCKS
+#define KGPU_RAD_TAIL_BLOCKS 8
 #endif
 
 int kgpu_report_cuda(const char *what, cudaError_t e);   // kgpu.cu: records the error for kgpu_last_error
@@ -67,7 +78,7 @@ RadParams to_dev(const kgpu_rad_params &p) {
 struct Opts {
   int pass_iters = 8;       // Newton iterations per cell and pass of the batched form
   int inner_cap = 64;       // W-function evaluations of a nested inversion in one lane (0: no cap)
-  int tail = 1;             // batched: warp-per-cell tail
+  int tail = KGPU_RAD_TAIL_BLOCKS;   // batched: blocks per SM of the warp-per-cell tail (0: none)
   int warm_attempts = IMP_NATTEMPTS;
   int thin = 8;             // persistent: hand-off threshold of live lanes once the list is empty
   int blocks_per_sm = 0;    // persistent: resident blocks per SM (0: occupancy limit)
@@ -98,7 +109,7 @@ kgpu_rad_solver_opts to_api(const Opts &o) {
   return r;
 }
 bool opts_valid(const kgpu_rad_solver_opts &o) {
-  return o.pass_iters >= 1 && o.inner_cap >= 0 && (o.tail == 0 || o.tail == 1) && o.warm_attempts >= 1 &&
+  return o.pass_iters >= 1 && o.inner_cap >= 0 && o.tail >= 0 && o.tail <= 32 && o.warm_attempts >= 1 &&
          o.warm_attempts <= IMP_NATTEMPTS && o.thin >= 0 && o.thin <= 32 && o.blocks_per_sm >= 0 &&
          o.blocks_per_sm <= 16 && o.skip >= 0 && o.skip <= 2;
 }
@@ -832,7 +843,7 @@ extern "C" int kgpu_rad_set_inner_cap(int cap) {
 }
 
 extern "C" int kgpu_rad_set_tail(int on) {
-  g_opts.tail = on ? 1 : 0;
+  g_opts.tail = on ? KGPU_RAD_TAIL_BLOCKS : 0;
   return 0;
 }
 
@@ -936,8 +947,9 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
         RCK(cudaGetLastError());
       }
       if (o.tail && p < passes - 1) {
-        // one wave: two blocks of four warps per SM at this kernel's registers
-        k_rad_tail<<<sm_count() * 2, 128, 0, st>>>(R, C, W, n, p, sm_count() * 8, o.warm_attempts);
+        // o.tail blocks of four warps per SM, one cell per warp at a time;
+        // it takes over once the unfinished cells are no more than its warps
+        k_rad_tail<<<sm_count() * o.tail, 128, 0, st>>>(R, C, W, n, p, sm_count() * o.tail * 4, o.warm_attempts);
         RCK(cudaGetLastError());
       }
     }

@@ -124,7 +124,7 @@ def test_rad_batched_equals_plain(kgpu, cells):
     host = kgpu.rad_implicit_cells(rp, uu, pp, g, G, dt, mode=kgpu.RAD_PLAIN)
     for x, y in zip(a, host):
         assert np.array_equal(x, y)
-    variants = [(kgpu.RAD_BATCHED, dict(tail=tail, pass_iters=k)) for tail in (1, 0) for k in (1, 3, 8)]
+    variants = [(kgpu.RAD_BATCHED, dict(tail=tail, pass_iters=k)) for tail in (16, 1, 0) for k in (1, 3, 8)]
     variants += [(kgpu.RAD_PERSISTENT, dict(thin=thin, inner_cap=cap, blocks_per_sm=b))
                  for thin, cap, b in ((8, 64, 0), (0, 64, 0), (32, 64, 1), (8, 0, 0), (16, 4, 1))]
     stats = {}
