@@ -753,6 +753,37 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
         a, b = a[g:-g, g:-g, g:-g], b[g:-g, g:-g, g:-g]
         return [float(np.abs(a[..., v] - b[..., v]).sum() / (np.abs(b[..., v]).sum() + 1e-300)) for v in range(13)]
 
+    # the flow's own sensitivity: the steps without the network again, from
+    # the same state with the gas energy of the densest cell moved by one
+    # unit in the last place; the L1 between the two runs is what any
+    # last-place change grows to over these steps
+    s.set_implicit_solver(main_mode, None)
+    u_nudge0 = u_start.copy()
+    dom_u = u_nudge0[g:-g, g:-g, g:-g]
+    iz, iy, ix = np.unravel_index(np.argmax(p_start[g:-g, g:-g, g:-g, 0]), dom_u.shape[:3])
+    dom_u[iz, iy, ix, 1] = np.nextafter(dom_u[iz, iy, ix, 1], np.inf)
+    s.upload_state(u_nudge0, p_start.copy())
+    s.tstepdenmax = tsd_start
+    s.reset_counters()
+    barrier()
+    timed_steps(args.steps)
+    u_nudge, _ = s.download_state()
+
+    def density_l1_by_region(a, b):
+        """Shares of the density L1 difference by radius and near the axes
+        (MKS2 with R0 = 0: r = exp(x1), x1 uniform in [ln 1.8, ln 1000])."""
+        d = np.abs(a[g:-g, g:-g, g:-g, 0] - b[g:-g, g:-g, g:-g, 0])
+        tot = d.sum() or 1.
+        r = np.exp(np.log(1.8) + (np.arange(nx) + 0.5) * (np.log(1000.) - np.log(1.8)) / nx)
+        rh = 1. + np.sqrt(1. - 0.9 * 0.9)
+        out = {}
+        for lo, hi, tag in ((0., 2. * rh, "r < 2 r_h"), (2. * rh, 10., "2 r_h <= r < 10"), (10., 50., "10 <= r < 50"),
+                            (50., 1e9, "r >= 50")):
+            m = (r >= lo) & (r < hi)
+            out[tag] = float(d[:, :, m].sum() / tot)
+        out["within 8 rows of an axis"] = float((d[:, :8].sum() + d[:, -8:].sum()) / tot)
+        return out
+
     # per-kernel device times (events around each launch, stream replay) and
     # the solver's counters over the same steps
     s.set_implicit_solver(main_mode, mlp)
@@ -820,7 +851,12 @@ def our_arm_radtorus(args, wl, rank, world, local_rank):
         "newton": {"learned": newton(c_main), "no_network": newton(c_n),
                    "iteration_ratio_no_network_over_learned": it_n / it_main if it_main > 0 else None},
         "no_network": {"value": cells * args.steps * world / (ms_n / 1e3), "unit": UNIT,
-                       "ms_per_step": ms_n / args.steps, "end_state_l1_vs_learned": l1(u_main, u_n)},
+                       "ms_per_step": ms_n / args.steps, "end_state_l1_vs_learned": l1(u_main, u_n),
+                       "end_state_l1_one_ulp_nudge": l1(u_nudge, u_n),
+                       "one_ulp_nudge": "gas energy of the densest cell moved by one unit in the last place at "
+                                        "the start of the timed steps, the same steps without the network",
+                       "density_l1_vs_learned_by_region": density_l1_by_region(u_main, u_n),
+                       "density_l1_one_ulp_nudge_by_region": density_l1_by_region(u_nudge, u_n)},
         other_name: {"value": cells * args.steps * world / (ms_o / 1e3), "unit": UNIT,
                      "ms_per_step": ms_o / args.steps, "with_network": mlp_name is not None,
                      "same_state_as_main": bool(np.array_equal(u_o, u_main)), "newton": newton(c_o)},
