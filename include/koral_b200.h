@@ -391,7 +391,14 @@ int kgpu_rad_default_params(kgpu_rad_params *rp, double mass, double gamma, doub
  *                 network expects to fail their first attempt start from the
  *                 prediction, the others from their own guess; 0: every
  *                 warm-started cell begins with attempt 0.  Every cell still
- *                 converges to RADIMPCONV or runs the reference cascade */
+ *                 converges to RADIMPCONV or runs the reference cascade
+ *  hard           batched, in a context's implicit step: a cell whose
+ *                 previous solve in that context took a later attempt,
+ *                 failed, or took more than `hard` Newton iterations skips
+ *                 the first pass and starts in the warp-per-cell tail, where
+ *                 long cascades run fastest (default 16; -1: every cell
+ *                 starts in the first pass; the context-free entry points
+ *                 have no previous solve and ignore it) */
 typedef struct {
   int pass_iters;
   int inner_cap;
@@ -400,6 +407,7 @@ typedef struct {
   int thin;
   int blocks_per_sm;
   int skip;
+  int hard;
 } kgpu_rad_solver_opts;
 int kgpu_rad_default_solver_opts(kgpu_rad_solver_opts *opts);
 
@@ -614,7 +622,8 @@ int kgpu_set_tuning(kgpu_ctx *ctx, const kgpu_tuning *t);
  * are restored afterwards, and the choice is applied.  Candidates: the
  * fused or split face flux, flux 5..8, update 3..5, u2p 4..6 blocks; u2p_pass_iters 4, 8, 16; with
  * radiation the batched and the persistent solver, pass_iters 4, 8, 16,
- * inner_cap 32, 64, 128, tail 0, 4, 8, 16 or thin 4, 8, 16.  A candidate
+ * inner_cap 32, 64, 128, tail 0, 4, 8, 16, hard -1, 8, 16, 32 or thin 4, 8,
+ * 16.  A candidate
  * replaces the incumbent only when it is faster by min_gain (a fraction,
  * e.g. 0.02) in the same round of trials.  The choice is cached per device
  * and grid configuration for the process: with reuse = 1 a cached choice

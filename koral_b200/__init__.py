@@ -39,7 +39,7 @@ class SolverOpts(ctypes.Structure):
     """kgpu_rad_solver_opts (include/koral_b200.h): tuning of the batched and
     persistent implicit solvers."""
     _fields_ = [(n, ctypes.c_int) for n in ("pass_iters", "inner_cap", "tail", "warm_attempts", "thin",
-                                            "blocks_per_sm", "skip")]
+                                            "blocks_per_sm", "skip", "hard")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

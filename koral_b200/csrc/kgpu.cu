@@ -2900,6 +2900,7 @@ extern "C" int kgpu_autotune(kgpu_ctx *c, int steps, double min_gain, int reuse,
       if (best.implicit_mode == KGPU_RAD_BATCHED) {
         round.push_back({[](kgpu_tuning &t) { return &t.implicit.pass_iters; }, {4, 8, 16}});
         round.push_back({[](kgpu_tuning &t) { return &t.implicit.tail; }, {0, 4, 8, 16}});
+        round.push_back({[](kgpu_tuning &t) { return &t.implicit.hard; }, {-1, 8, 16, 32}});
       } else {
         round.push_back({[](kgpu_tuning &t) { return &t.implicit.thin; }, {4, 8, 16}});
       }

@@ -83,6 +83,7 @@ struct Opts {
   int thin = 8;             // persistent: hand-off threshold of live lanes once the list is empty
   int blocks_per_sm = 0;    // persistent: resident blocks per SM (0: occupancy limit)
   int skip = 1;             // warm start: begin with the attempt the network expects to succeed
+  int hard = 16;            // batched, context: cells hard in their previous solve start in the tail (-1: off)
 };
 Opts g_opts;   // the context-free entry points' values
 
@@ -95,6 +96,7 @@ Opts from_api(const kgpu_rad_solver_opts &o) {
   r.thin = o.thin;
   r.blocks_per_sm = o.blocks_per_sm;
   r.skip = o.skip;
+  r.hard = o.hard;
   return r;
 }
 kgpu_rad_solver_opts to_api(const Opts &o) {
@@ -106,12 +108,13 @@ kgpu_rad_solver_opts to_api(const Opts &o) {
   r.thin = o.thin;
   r.blocks_per_sm = o.blocks_per_sm;
   r.skip = o.skip;
+  r.hard = o.hard;
   return r;
 }
 bool opts_valid(const kgpu_rad_solver_opts &o) {
   return o.pass_iters >= 1 && o.inner_cap >= 0 && o.tail >= 0 && o.tail <= 32 && o.warm_attempts >= 1 &&
          o.warm_attempts <= IMP_NATTEMPTS && o.thin >= 0 && o.thin <= 32 && o.blocks_per_sm >= 0 &&
-         o.blocks_per_sm <= 16 && o.skip >= 0 && o.skip <= 2;
+         o.blocks_per_sm <= 16 && o.skip >= 0 && o.skip <= 2 && o.hard >= -1;
 }
 
 // upper bound of the passes a cell can need: six attempts of at most
@@ -265,7 +268,13 @@ __global__ void __launch_bounds__(128, KGPU_RAD_MIN_BLOCKS) k_rad_plain(RadParam
 // to be the first that succeeds (mlp_first_attempt) instead of the first
 // one; skip 2: besides, only the cells the network expects to fail their
 // first attempt start from the prediction, the others from their own guess
-__global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypred, int gate, int skip) {
+// hard >= 0 (batched form, where attempt and iteration outputs of a
+// previous solve are valid): a cell whose previous solve took a later
+// attempt, failed, or took more than `hard` iterations goes to the queue of
+// the second pass instead of the first, so that the warp-per-cell tail,
+// which follows the first pass, starts it; the cell's arithmetic is the same
+// in either kernel
+__global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypred, int gate, int skip, int hard) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   RadGeom rg;
@@ -299,8 +308,11 @@ __global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypr
   // the queue is chosen by the predicate, never by the pointer: every lane
   // of a warp-aggregated push must name the same queue
   const int type = imp_attempt(first, sw).prim;
-  warp_push(W.q[0][0], W.count + 0, type == 0, k);
-  warp_push(W.q[0][1], W.count + 1, type == 1, k);
+  const bool late = hard >= 0 && (C.attempt[k] != 0 || C.iters[k] > hard);
+  warp_push(W.q[0][0], W.count + 0, !late && type == 0, k);
+  warp_push(W.q[0][1], W.count + 1, !late && type == 1, k);
+  warp_push(W.q[1][0], W.count + 3, late && type == 0, k);
+  warp_push(W.q[1][1], W.count + 4, late && type == 1, k);
 }
 
 // warp-aggregated append that returns each pushing lane's slot (or -1)
@@ -387,13 +399,13 @@ __global__ void __launch_bounds__(128, KGPU_RAD_MIN_BLOCKS) k_rad_pass(RadParams
 }
 
 // The tail of the batched form.  Launched after pass p (and its cooperative
-// part): when the cells those left unfinished fit in one wave of warps
+// part): when the cells those left unfinished are no more than its warps
 // (at most `limit`), each is taken by a whole warp and run to its end.  At
 // the start of every Newton iteration lanes 0..8 evaluate the base and the
 // four Jacobian columns on both sides together (imp_eval_entry), and the
 // state machine, run by every lane alike, takes those entries instead of
 // evaluating them one after another (ImpCache); damped trials and the final
-// inversion it evaluates itself.  The sequence of operations per cell, and
+// inversion it evaluates itself, with warp-wide nested inversions.  The sequence of operations per cell, and
 // so its results and its statistics, are those of the passes; a cell's
 // latency falls from six evaluations per Newton iteration to about two.
 // The last block to finish empties the queue, so that the passes after
@@ -430,7 +442,12 @@ __global__ void __launch_bounds__(128, KGPU_RAD_MIN_BLOCKS) k_rad_tail(RadParams
     for (int i = 0; i < NVR; i++) s.pp[i] = W.wpp[(long)k * NVR + i];
     const int warm0 = s.warm;
     const double *wg = W.wguess + (long)k * NVR;
-    ImpInner how{nullptr, 0u, false, warm_attempts};
+    // what the state machine still evaluates itself (damped trials, the
+    // final inversion) runs its nested MHD inversion with the 32 lanes
+    // together: the tail's cells are the ones with the longest chains, so
+    // its latency is what counts (hard cells of a settled torus solve alone:
+    // 75.3 -> 65.4 ms)
+    ImpInner how{nullptr, 0u, true, warm_attempts};
     int budget = 1 << 30;
     int r;
     while (true) {
@@ -884,7 +901,7 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
                             const double *G, const double *dt, const float *ypred, double *pp_out, double *uu_out,
                             int *status, int *attempt, int *iters, int mode, void *work, void *stream,
                             unsigned long long *stats, int nstats, const Opts &o, unsigned long long *acc = nullptr,
-                            int gate = -1) {
+                            int gate = -1, bool have_prev = false) {
   if (n < 0 || !rp || (mode != KGPU_RAD_PLAIN && mode != KGPU_RAD_BATCHED && mode != KGPU_RAD_PERSISTENT))
     return KGPU_EINVAL;
   if (n > 0 && (!uu || !pp || !g || !G || !dt || !pp_out || !uu_out || !status || !attempt || !iters))
@@ -927,7 +944,8 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
   RCK(cudaMemsetAsync(W.ctl, 0, 4 * sizeof(unsigned), st));
   if (acc) W.stats = acc;
   else RCK(cudaMemsetAsync(W.stats, 0, 8 * sizeof(unsigned long long), st));
-  k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n, ypred, gate, o.skip);
+  const int hard = (have_prev && mode == KGPU_RAD_BATCHED && passes > 1) ? o.hard : -1;
+  k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n, ypred, gate, o.skip, hard);
   RCK(cudaGetLastError());
   if (mode == KGPU_RAD_PERSISTENT) {
     const int grid = sm_count() * persist_blocks_per_sm(o);
@@ -970,7 +988,7 @@ int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, c
   const Opts o = opts ? from_api(*opts) : g_opts;
   if (launches) *launches = solve_launches(to_dev(*rp), mode, o);
   return rad_solve_device(n, rp, uu, pp, g, G, dt, ypred, pp_out, uu_out, status, attempt, iters, mode, work, stream,
-                          nullptr, 0, o, acc, gate);
+                          nullptr, 0, o, acc, gate, true);
 }
 
 bool kgpu_rad_opts_valid(const kgpu_rad_solver_opts &o) { return opts_valid(o); }

@@ -180,10 +180,14 @@ def test_radtorus_solver_variants_and_graph_identical(kgpu, oracle):
     R.init()
     u, p, tsd = R.array("u").copy(), R.array("p").copy(), R.scalar("tstepdenmax")
     out = []
-    for mode, graph in ((kgpu.RAD_BATCHED, False), (kgpu.RAD_BATCHED, True), (kgpu.RAD_PLAIN, True),
-                        (kgpu.RAD_PERSISTENT, False), (kgpu.RAD_PERSISTENT, True)):
+    # hard: cells hard in their previous solve start in the tail (0: all that
+    # took more than no iteration, i.e. every cell after the first step; -1: none)
+    for mode, graph, hard in ((kgpu.RAD_BATCHED, False, 16), (kgpu.RAD_BATCHED, True, 16), (kgpu.RAD_PLAIN, True, 16),
+                              (kgpu.RAD_PERSISTENT, False, 16), (kgpu.RAD_PERSISTENT, True, 16),
+                              (kgpu.RAD_BATCHED, True, -1), (kgpu.RAD_BATCHED, True, 0)):
         s = make_gpu(kgpu, R)
         s.set_implicit_solver(mode, None)
+        s.set_implicit_options(hard=hard)
         s.upload_state(u.copy(), p.copy())
         s.tstepdenmax = tsd
         s.rk2imex_steps(3, graph=graph)
