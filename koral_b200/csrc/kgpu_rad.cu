@@ -274,7 +274,17 @@ __global__ void __launch_bounds__(128, KGPU_RAD_MIN_BLOCKS) k_rad_plain(RadParam
 // the second pass instead of the first, so that the warp-per-cell tail,
 // which follows the first pass, starts it; the cell's arithmetic is the same
 // in either kernel
-__global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypred, int gate, int skip, int hard) {
+// Cells whose previous solve was hard (the routing test of k_rad_start),
+// counted into *count.
+__global__ void k_rad_count_hard(Cell C, int n, int hard, unsigned *count) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool late = k < n && (C.attempt[k] != 0 || C.iters[k] > hard);
+  const unsigned m = __ballot_sync(0xffffffffu, late);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(count, (unsigned)__popc(m));
+}
+
+__global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypred, int gate, int skip, int hard,
+                            int limit) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   RadGeom rg;
@@ -308,7 +318,11 @@ __global__ void k_rad_start(RadParams R, Cell C, Work W, int n, const float *ypr
   // the queue is chosen by the predicate, never by the pointer: every lane
   // of a warp-aggregated push must name the same queue
   const int type = imp_attempt(first, sw).prim;
-  const bool late = hard >= 0 && (C.attempt[k] != 0 || C.iters[k] > hard);
+  // the routing applies only when all such cells fit in the tail (limit
+  // warps); with more of them (the transient of a run) every cell starts in
+  // the first pass.  The count is read from device memory, the same value
+  // in every block
+  const bool late = hard >= 0 && W.ctl[0] <= (unsigned)limit && (C.attempt[k] != 0 || C.iters[k] > hard);
   warp_push(W.q[0][0], W.count + 0, !late && type == 0, k);
   warp_push(W.q[0][1], W.count + 1, !late && type == 1, k);
   warp_push(W.q[1][0], W.count + 3, late && type == 0, k);
@@ -884,11 +898,12 @@ static int persist_blocks_per_sm(const Opts &o) {
 }
 
 // kernels one solve launches (for the launch counters)
-static long long solve_launches(const RadParams &R, int mode, const Opts &o) {
+static long long solve_launches(const RadParams &R, int mode, const Opts &o, bool have_prev) {
   if (mode == KGPU_RAD_PLAIN) return 1;
   if (mode == KGPU_RAD_PERSISTENT) return 3;
   const int np = max_passes(R, o.pass_iters);
-  return 1 + (o.inner_cap ? 2 : 1) * np + (o.tail ? np - 1 : 0);
+  const bool count = have_prev && np > 1 && o.tail > 0 && o.hard >= 0;   // k_rad_count_hard
+  return 1 + (count ? 1 : 0) + (o.inner_cap ? 2 : 1) * np + (o.tail ? np - 1 : 0);
 }
 
 // acc (device, optional): counters the solve adds to instead of reporting
@@ -944,8 +959,13 @@ static int rad_solve_device(int n, const kgpu_rad_params *rp, const double *uu, 
   RCK(cudaMemsetAsync(W.ctl, 0, 4 * sizeof(unsigned), st));
   if (acc) W.stats = acc;
   else RCK(cudaMemsetAsync(W.stats, 0, 8 * sizeof(unsigned long long), st));
-  const int hard = (have_prev && mode == KGPU_RAD_BATCHED && passes > 1) ? o.hard : -1;
-  k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n, ypred, gate, o.skip, hard);
+  const int hard = (have_prev && mode == KGPU_RAD_BATCHED && passes > 1 && o.tail > 0) ? o.hard : -1;
+  const int limit = sm_count() * o.tail * 4;
+  if (hard >= 0) {
+    k_rad_count_hard<<<(n + 127) / 128, 128, 0, st>>>(C, n, hard, W.ctl);
+    RCK(cudaGetLastError());
+  }
+  k_rad_start<<<(n + 127) / 128, 128, 0, st>>>(R, C, W, n, ypred, gate, o.skip, hard, limit);
   RCK(cudaGetLastError());
   if (mode == KGPU_RAD_PERSISTENT) {
     const int grid = sm_count() * persist_blocks_per_sm(o);
@@ -986,7 +1006,7 @@ int kgpu_rad_solve_enqueue(int n, const kgpu_rad_params *rp, const double *uu, c
                            int *status, int *attempt, int *iters, int mode, void *work, void *stream,
                            unsigned long long *acc, long long *launches, int gate, const kgpu_rad_solver_opts *opts) {
   const Opts o = opts ? from_api(*opts) : g_opts;
-  if (launches) *launches = solve_launches(to_dev(*rp), mode, o);
+  if (launches) *launches = solve_launches(to_dev(*rp), mode, o, true);
   return rad_solve_device(n, rp, uu, pp, g, G, dt, ypred, pp_out, uu_out, status, attempt, iters, mode, work, stream,
                           nullptr, 0, o, acc, gate, true);
 }
