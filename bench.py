@@ -4,10 +4,17 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload ot128]
 
-A step is one full RK2 time step (ko.c:571-626: two explicit operators and two
-inversions with fixups and boundary conditions) of the workload.  Workloads:
+A step is one full time step of the workload (RK2, ko.c:571-626: two explicit
+operators and two inversions with fixups and boundary conditions; RK2IMEX,
+ko.c:444-570, with radiation).  Workloads:
 
-  torus   (default) 3D magnetised Kerr torus, 192x96x64: spin 0.9, MKS2
+  radtorus  (default) the torus below on 256x128x64 with M1 radiation: a step
+          is one RK2IMEX step (implicit source solve in every substep,
+          batched solver with the learned warm start, one CUDA graph per
+          step); the line adds the same steps without the network, with the
+          persistent solver and with one thread per cell, and the flow's own
+          one-ulp sensitivity over those steps
+  torus   3D magnetised Kerr torus, 192x96x64: spin 0.9, MKS2
           coordinates, r in [1.8, 1000], Fishbone-Moncrief torus r_in = 6,
           r_max = 12, Gamma = 13/9, beta_min = 100, 2% seeded pressure noise,
           density floor 1e-4 r^-1.5, MP5 + HLL + flux-CT, RK2, CFL 0.5
@@ -15,11 +22,8 @@ inversions with fixups and boundary conditions) of the workload.  Workloads:
           Minkowski, Gamma = 5/3, CFL 0.5 (the reference's CPU-runnable case)
   radcells  2^22 independent radiating cells: a step is one batched implicit
           gas-radiation source solve (metric "implicit solves/s"); the line
-          adds the one-thread-per-cell form and the learned warm start
-  radtorus  the torus on 256x128x64 with M1 radiation: a step is one RK2IMEX
-          step (implicit source solve in every substep, batched solver with
-          the learned warm start, one CUDA graph per step); the line adds the
-          same steps without the network and with one thread per cell
+          adds the one-thread-per-cell form, the learned warm start and the
+          MHD inversion's learned warm start
 
 value  = cells x timed steps / device time (CUDA events on the library's own
          stream, L2 flushed between steps, inputs resident in HBM)
