@@ -716,8 +716,9 @@ int kgpu_calc_scalars_device(kgpu_ctx *ctx, const kgpu_scalars_params *sp, doubl
  *                    their graph forms) call save_avg once per step as the
  *                    reference's loop does.  mass (solar masses) sets the
  *                    unit constants of the averaged gas temperature
- *                    (K_BOLTZ, M_PROTON, ko.h:4-48); with radiation the
- *                    context's radiation constants are used.
+ *                    (K_BOLTZ, M_PROTON, ko.h:4-48) and is read on the
+ *                    first call only; with radiation the context's radiation
+ *                    constants are used.
  *  kgpu_save_avg     one save_avg(dt) now (after kgpu_set_avg).
  *  kgpu_download_avg the sums in KORAL's layout [SZ][SY][SX][NV+NAVGVARS]
  *                    (ghost cells zero) and avgtime; the reference divides by
