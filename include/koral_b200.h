@@ -367,7 +367,7 @@ int kgpu_rad_default_params(kgpu_rad_params *rp, double mass, double gamma, doub
  * (Newton iterations, evaluations) do not depend on any field except
  * warm_attempts, which chooses how long a warm-started cell trusts its
  * prediction.
- *  pass_iters     batched: Newton iterations a cell may take per pass (8)
+ *  pass_iters     batched: Newton iterations a cell may take per pass (4)
  *  inner_cap      W-function evaluations the MHD inversion nested in one
  *                 residual evaluation may take in a single lane before that
  *                 evaluation is repeated by a whole warp with the damped

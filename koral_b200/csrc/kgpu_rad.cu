@@ -76,7 +76,9 @@ RadParams to_dev(const kgpu_rad_params &p) {
 
 // Tuning of the batched and persistent forms (kgpu_rad_solver_opts)
 struct Opts {
-  int pass_iters = 8;       // Newton iterations per cell and pass of the batched form
+  int pass_iters = 4;       // Newton iterations per cell and pass of the batched form (4: 1674 against
+                            // 1743 ms at 8 on 2^21 batched-solve cells, 77.7 against 81.7 ms on a
+                            // settled torus solve)
   int inner_cap = 64;       // W-function evaluations of a nested inversion in one lane (0: no cap)
   int tail = KGPU_RAD_TAIL_BLOCKS;   // batched: blocks per SM of the warp-per-cell tail (0: none)
   int warm_attempts = IMP_NATTEMPTS;
