@@ -54,3 +54,30 @@ def test_rk2_loop_program_compiles_and_links(kgpu, tmp_path):
     """The host-side loop compiles as C99 against include/koral_b200.h and
     links against every symbol it names."""
     assert os.path.exists(build_rk2_loop(kgpu, tmp_path))
+
+
+def test_struct_layouts_match_python_mirrors(kgpu, tmp_path):
+    """The ctypes structures of koral_b200/__init__.py have the sizes and
+    field offsets a C compiler gives the header's structs (gcc on
+    tests/abi/layout.c)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        import pytest
+        pytest.skip("no C compiler")
+    exe = str(tmp_path / "layout")
+    subprocess.check_call([cc, "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "abi", "layout.c"),
+                           "-o", exe])
+    c = dict(line.rsplit(" ", 1) for line in subprocess.check_output([exe], text=True).splitlines())
+    c = {k: int(v) for k, v in c.items()}
+    py = {"kgpu_config": kgpu.Config, "kgpu_torus_params": kgpu.TorusParams, "kgpu_rad_params": kgpu.RadParams,
+          "kgpu_rad_solver_opts": kgpu.SolverOpts, "kgpu_tuning": kgpu.Tuning,
+          "kgpu_scalars_params": kgpu.ScalarsParams}
+    for name, cls in py.items():
+        assert ctypes.sizeof(cls) == c[name], name
+    for key, off in c.items():
+        if "." not in key:
+            continue
+        name, field = key.split(".")
+        assert getattr(py[name], field).offset == off, key
