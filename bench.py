@@ -80,31 +80,32 @@ WORKLOADS = {
 RAD_METRIC = "implicit solves/s (1 B200)"
 
 # From the ncu capture of the x-face flux kernel on the 192x96x64 torus
-# (profiles/k_flux_x_torus_192x96x64.md): DRAM bytes per launch and FP64
-# operations per face (DADD + DMUL + 2 DFMA thread instructions / faces).
-FLUX_X_TRAFFIC_BYTES_192 = 971.19e6
-FLUX_X_FACES_192 = 193 * 98 * 66
+# (profiles/k_flux_x_torus_192x96x64.md): FP64 operations per face (DADD +
+# DMUL + 2 DFMA thread instructions / faces).  That capture's DRAM bytes
+# (971 MB per launch, mostly register spill) belong to the build before the
+# magnetic floor moved to k_flux_fix, which cut the spills; the current
+# build's traffic has not been captured, so the line reports none.
 FLUX_FP64_PER_FACE = 1895.5
 
 
 def flux_roofline(prof, nx, ny, nz, hbm_peak, peak_src, fp64_peak):
-    """HBM roofline of the x-face flux kernel (algorithmic bytes 16 NV per
-    face over its event time) with the DRAM traffic ncu measured (scaled by
-    faces from the 192x96x64 capture), and its FP64 rate."""
+    """HBM roofline of the x-face flux (algorithmic bytes 16 NV per face
+    over the event time of k_flux_x and its magnetic-floor pass k_flux_fix,
+    timed as one), and its FP64 rate."""
     nfaces = (nx + 1) * (ny + 2) * (nz + 2)
     flux_ms = prof["k_flux_x"][0] / max(1, prof["k_flux_x"][1])
     flux_gbs = 16 * 9 * nfaces / (flux_ms / 1e3) / 1e9 if flux_ms > 0 else None
     tflops = FLUX_FP64_PER_FACE * nfaces / (flux_ms / 1e3) / 1e12 if flux_ms > 0 else None
     return {"kernel": "k_flux_x", "bound": "hbm", "achieved": flux_gbs, "peak": hbm_peak, "unit": "GB/s",
             "frac": (flux_gbs / hbm_peak) if flux_gbs else None,
-            "traffic": FLUX_X_TRAFFIC_BYTES_192 * nfaces / FLUX_X_FACES_192,
-            "traffic_source": "ncu dram bytes of one launch on 192x96x64, scaled by faces",
+            "traffic": None,
+            "traffic_source": "not captured for this build (the previous build's 971 MB per launch was "
+                              "register spill; deferring the magnetic floor cut the spill loads 4.5x)",
             "peak_source": peak_src, "algorithmic_bytes_per_launch": 16 * 9 * nfaces,
             "fp64": {"achieved_tflops": tflops, "peak_tflops": fp64_peak,
                      "frac": (tflops / fp64_peak) if (tflops and fp64_peak) else None,
                      "flop_per_face": FLUX_FP64_PER_FACE,
-                     "note": "the kernel is FP64-latency bound: 13.1 FLOP per algorithmic byte; the DRAM "
-                             "traffic above the algorithmic bytes is register spill of its 72-register build"}}
+                     "note": "the kernel is FP64-latency bound: 13.1 FLOP per algorithmic byte"}}
 
 
 def fp64_peak_tflops(k):

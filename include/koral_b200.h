@@ -222,7 +222,8 @@ int kgpu_get_counters(kgpu_ctx *ctx, unsigned long long out[4]);
  * steps of the MHD inversions nested in those evaluations, [15] their
  * W-function evaluations, [16] evaluations whose nested inversion went over
  * its per-lane cap and was handed to a whole warp, [17] implicit solves,
- * [18] cells where the radiation floors acted.  Returns how many were
+ * [18] cells where the radiation floors acted; [19] faces where a side's
+ * reconstructed state needed the magnetic floor.  Returns how many were
  * written. */
 int kgpu_get_counters_ex(kgpu_ctx *ctx, unsigned long long *out, int n);
 /* Tuning: Newton steps a cell may take in the first inversion pass before

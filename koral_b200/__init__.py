@@ -480,7 +480,7 @@ class Subdomain:
         return dict(fixups=a[0], entropy=a[1], failed=a[2], negrho=a[3], iters_energy=a[4], iters_entropy=a[5],
                     paused=a[6], to_entropy=a[7], rad_corrected=a[8], radimp_failed=a[9], imp_iters=a[10],
                     imp_passes=a[11], imp_fallbacks=a[12], imp_evals=a[13], imp_inner=a[14], imp_inner_f=a[15],
-                    imp_cooperative=a[16], imp_solves=a[17], rad_floors=a[18])
+                    imp_cooperative=a[16], imp_solves=a[17], rad_floors=a[18], face_floors=a[19])
 
     def set_radiation(self, rp, wavespeed_limiter=False):
         """Radiation in the step (nv = 13): M1 fluxes and speeds, u2p_rad and

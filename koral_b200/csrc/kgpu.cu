@@ -460,16 +460,20 @@ __global__ void __launch_bounds__(256) k_recon(Grid G, Box b, double *sl, double
   sr[(long)iv * nb + fi] = right;
 }
 
-// SPLIT: the face states come from k_recon (sl, sr) instead of being
-// reconstructed here; the rest is the same.
-template <int D, int MB = KGPU_FLUX_MIN_BLOCKS, bool SPLIT = false>
-__global__ void __launch_bounds__(128, MB) k_flux(Grid G, Box b, const double *sl, const double *sr) {
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const int side = (int)(t & 1);
+// The flux of face fi of box b, computed by the lane pair (side 0, side 1)
+// of pairmask.  SPLIT: the face states come from k_recon (sl, sr) instead
+// of being reconstructed here; the rest is the same.  DEFER: a face where
+// either side's state needs the magnetic floor (magnetic pressure above
+// B2RHORATIOMAX rho, u2p.c:617-671: a nested W inversion, rare and only in
+// the magnetised funnel) is appended to G.fq[D] and left; k_flux_fix
+// computes it, whole and with the same arithmetic, without DEFER.  The
+// floor's inversion then no longer sets the register budget of the common
+// path.
+template <int D, bool SPLIT, bool DEFER>
+__device__ __forceinline__ void face_flux(const Grid &G, const Box &b, const double *sl, const double *sr, long fi,
+                                          int side, unsigned pairmask) {
   int ix, iy, iz;
-  const bool valid = box_coord(b, t >> 1, ix, iy, iz);
-  const unsigned pairmask = __ballot_sync(0xffffffffu, valid);
-  if (!valid) return;
+  box_coord(b, fi, ix, iy, iz);
   constexpr int nv = NVMAX;
   const int i = D == 0 ? ix : (D == 1 ? iy : iz);
   const long stride = D == 0 ? 1 : (D == 1 ? (long)G.sx : (long)G.sx * G.sy);
@@ -479,7 +483,7 @@ __global__ void __launch_bounds__(128, MB) k_flux(Grid G, Box b, const double *s
   // reconstruction (avg2point, finite.c:89-289) of this lane's side
   double ps[NVMAX];
   if (SPLIT) {
-    const long nb = b.n(), fi = t >> 1;
+    const long nb = b.n();
     const double *src = side ? sr : sl;
 #pragma unroll
     for (int iv = 0; iv < nv; iv++) ps[iv] = src[(long)iv * nb + fi];
@@ -518,7 +522,26 @@ __global__ void __launch_bounds__(128, MB) k_flux(Grid G, Box b, const double *s
   {
     Kin k;
     bool kv;
-    check_floors_mhd(G, ps, g, rfl, &k, &kv);
+    if (DEFER) {
+      bool need = false;
+      check_floors_mhd(G, ps, g, rfl, &k, &kv, &need);
+      const bool pairneed = (__shfl_xor_sync(pairmask, (int)need, 1) | (int)need) != 0;
+      const unsigned defer = __ballot_sync(pairmask, pairneed);
+      if (pairneed) {
+        // one queue slot per deferred face, taken by its side-0 lane; one
+        // atomic per warp
+        const unsigned app = defer & 0x55555555u;
+        const int lane = (int)(threadIdx.x & 31), leader = __ffs(app) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(G.fqn + D, __popc(app));
+        base = __shfl_sync(defer, base, leader);
+        if (side == 0) G.fq[D][base + __popc(app & ((1u << lane) - 1u))] = (int)fi;
+        return;
+      }
+      pairmask &= ~defer;
+    } else {
+      check_floors_mhd(G, ps, g, rfl, &k, &kv);
+    }
     if (!kv) kinematics(ps, g, kMagn, k);
     flux_prime(G, ps, D, g, k, fs);
     p2u_mhd(G, ps, us, g, k);
@@ -547,6 +570,31 @@ __global__ void __launch_bounds__(128, MB) k_flux(Grid G, Box b, const double *s
       else fl = (-al * fR + ar * fL + al * ar * (uR - uL)) / (ar - al);
     }
     out[iv * nf] = fl;
+  }
+}
+
+template <int D, int MB = KGPU_FLUX_MIN_BLOCKS, bool SPLIT = false>
+__global__ void __launch_bounds__(128, MB) k_flux(Grid G, Box b, const double *sl, const double *sr) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const bool valid = t < 2 * b.n();
+  const unsigned pairmask = __ballot_sync(0xffffffffu, valid);
+  if (!valid) return;
+  face_flux<D, SPLIT, true>(G, b, sl, sr, t >> 1, (int)(t & 1), pairmask);
+}
+
+// The faces k_flux left to the magnetic floor: a lane pair per face, all
+// registers the floor's inversion wants.  The loop runs warp-uniformly.
+template <int D, bool SPLIT>
+__global__ void __launch_bounds__(128) k_flux_fix(Grid G, Box b, const double *sl, const double *sr) {
+  const int n = *(volatile int *)(G.fqn + D);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(G.cnt + C_FACE_FLOOR, (unsigned long long)n);
+  const long warp = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+  const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+  const int lane = (int)(threadIdx.x & 31);
+  for (long base = warp * 16; base < n; base += nwarps * 16) {
+    const long q = base + (lane >> 1);
+    const unsigned pairmask = __ballot_sync(0xffffffffu, q < n);
+    if (q < n) face_flux<D, SPLIT, false>(G, b, sl, sr, G.fq[D][q], lane & 1, pairmask);
   }
 }
 
@@ -1531,6 +1579,14 @@ static void launch_flux_split(int mb, unsigned nb, cudaStream_t st, const Grid &
     default: k_flux<D, 7, true><<<nb, 128, 0, st>>>(G, b, sl, sr); break;
   }
 }
+// the faces of direction D that k_flux left to the magnetic floor: two
+// blocks per SM loop over the queue (empty on most steps)
+template <int D>
+static void launch_flux_fix(bool split, int sms, cudaStream_t st, const Grid &G, Box b, const double *sl,
+                            const double *sr) {
+  if (split) k_flux_fix<D, true><<<2 * sms, 128, 0, st>>>(G, b, sl, sr);
+  else k_flux_fix<D, false><<<2 * sms, 128, 0, st>>>(G, b, sl, sr);
+}
 static void launch_update(int mb, unsigned nb, cudaStream_t st, const Grid &G, Box b, const double *dtp, double fac,
                           double *save) {
   switch (mb) {
@@ -1776,6 +1832,8 @@ extern "C" int kgpu_create(const kgpu_config *cfg, kgpu_ctx **out) {
   AL(kr, G.nmet * 64 * d8); G.gkr = kr;
   AL(G.emf, 3L * (G.nx + 1) * (G.ny + 1) * (G.nz + 1) * d8);
   AL(G.flag, G.ncell * sizeof(int));
+  for (int d = 0; d < 3; d++) AL(G.fq[d], G.nface[d] * sizeof(int));
+  AL(G.fqn, 3 * sizeof(int));
   AL(c->fixmark, G.ncell * sizeof(int));
   AL(c->u2pq.slow, G.ncell * sizeof(int));
   AL(c->u2pq.ent, G.ncell * sizeof(int));
@@ -2171,17 +2229,22 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
   int ex0 = -1, enx = G.nx + 2;
   if (G.nx > 1) {
     Box b{0, ey0, ez0, G.nx + 1, eny, enz};
+    CK(cudaMemsetAsync(G.fqn + 0, 0, sizeof(int), c->stream));
     if (c->flux_split) {
       { LaunchScope ls(c, K_RECON0);
         k_recon<0><<<nblocks(b.n() * NVMAX, 256), 256, 0, c->stream>>>(G, b, c->fsl, c->fsr); }
       CKL("k_recon<0>");
-      LaunchScope ls(c, K_FLUX0);
-      launch_flux_split<0>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b, c->fsl, c->fsr);
-    } else {
-      LaunchScope ls(c, K_FLUX0);
-      launch_flux<0>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b);
     }
-    CKL("k_flux<0>");
+    {
+      // the face flux and its magnetic-floor pass, timed as one
+      LaunchScope ls(c, K_FLUX0);
+      if (c->flux_split) launch_flux_split<0>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b, c->fsl, c->fsr);
+      else launch_flux<0>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b);
+      CKL("k_flux<0>");
+      c->launches++;
+      launch_flux_fix<0>(c->flux_split != 0, c->sm_count, c->stream, G, b, c->fsl, c->fsr);
+      CKL("k_flux_fix<0>");
+    }
     if (G.rad) {
       LaunchScope ls(c, K_FLUXRAD0);
       k_flux_rad<0><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);
@@ -2190,17 +2253,22 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
   }
   if (G.ny > 1) {
     Box b{ex0, 0, ez0, enx, G.ny + 1, enz};
+    CK(cudaMemsetAsync(G.fqn + 1, 0, sizeof(int), c->stream));
     if (c->flux_split) {
       { LaunchScope ls(c, K_RECON1);
         k_recon<1><<<nblocks(b.n() * NVMAX, 256), 256, 0, c->stream>>>(G, b, c->fsl, c->fsr); }
       CKL("k_recon<1>");
-      LaunchScope ls(c, K_FLUX1);
-      launch_flux_split<1>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b, c->fsl, c->fsr);
-    } else {
-      LaunchScope ls(c, K_FLUX1);
-      launch_flux<1>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b);
     }
-    CKL("k_flux<1>");
+    {
+      // the face flux and its magnetic-floor pass, timed as one
+      LaunchScope ls(c, K_FLUX1);
+      if (c->flux_split) launch_flux_split<1>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b, c->fsl, c->fsr);
+      else launch_flux<1>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b);
+      CKL("k_flux<1>");
+      c->launches++;
+      launch_flux_fix<1>(c->flux_split != 0, c->sm_count, c->stream, G, b, c->fsl, c->fsr);
+      CKL("k_flux_fix<1>");
+    }
     if (G.rad) {
       LaunchScope ls(c, K_FLUXRAD1);
       k_flux_rad<1><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);
@@ -2209,17 +2277,22 @@ static int launch_explicit(kgpu_ctx *c, const double *dtp, double fac, double *s
   }
   if (G.nz > 1) {
     Box b{ex0, ey0, 0, enx, eny, G.nz + 1};
+    CK(cudaMemsetAsync(G.fqn + 2, 0, sizeof(int), c->stream));
     if (c->flux_split) {
       { LaunchScope ls(c, K_RECON2);
         k_recon<2><<<nblocks(b.n() * NVMAX, 256), 256, 0, c->stream>>>(G, b, c->fsl, c->fsr); }
       CKL("k_recon<2>");
-      LaunchScope ls(c, K_FLUX2);
-      launch_flux_split<2>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b, c->fsl, c->fsr);
-    } else {
-      LaunchScope ls(c, K_FLUX2);
-      launch_flux<2>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b);
     }
-    CKL("k_flux<2>");
+    {
+      // the face flux and its magnetic-floor pass, timed as one
+      LaunchScope ls(c, K_FLUX2);
+      if (c->flux_split) launch_flux_split<2>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b, c->fsl, c->fsr);
+      else launch_flux<2>(c->flux_blocks, nblocks(2 * b.n(), 128), c->stream, G, b);
+      CKL("k_flux<2>");
+      c->launches++;
+      launch_flux_fix<2>(c->flux_split != 0, c->sm_count, c->stream, G, b, c->fsl, c->fsr);
+      CKL("k_flux_fix<2>");
+    }
     if (G.rad) {
       LaunchScope ls(c, K_FLUXRAD2);
       k_flux_rad<2><<<nblocks(2 * b.n(), 128), 128, 0, c->stream>>>(G, b);

@@ -48,6 +48,8 @@ struct Grid {
   double *emf;                       // [3][(nx+1)(ny+1)(nz+1)]
   double *al[3], *ar[3];             // wavespeeds per cell and direction
   int *flag;                         // HD fixup request per cell
+  int *fq[3];                        // faces whose magnetic floor the face flux left to k_flux_fix
+  int *fqn;                          // their number per direction
   const double *rhofl_c, *rhofl_f;   // density floor per x-index (centres, x-faces), or null
   int bc[3];                         // boundary kind per axis (KGPU_BC_*)
   double *scal;                      // device scalars (see ScalarSlot)
@@ -87,6 +89,7 @@ enum CounterSlot {
                      // (10..16 are the solver's own statistics, in its order)
   C_IMP_SOLVES = 17, // implicit source solves
   C_RADFLOOR = 18,   // cells whose radiation floors acted
+  C_FACE_FLOOR = 19, // faces whose state needed the magnetic floor (computed by k_flux_fix)
   C_NCNT = 20
 };
 
@@ -754,8 +757,13 @@ KG_HD int u2p(const Grid &G, const double *uu0, double *pp, const Geom &g, int &
 // the returned primitives (neither the magnetic floor nor the Lorentz-factor
 // ceiling changed velocities or field; the density and energy floors do
 // not enter them), so a caller can skip computing them again.
+// defer (optional): where the magnetic floor applies, set *defer and return
+// at once, leaving pp part-floored; the caller then discards pp and runs
+// the whole floor again without defer (the face flux hands such faces to a
+// second kernel so that the floor's nested inversion stays out of its
+// register budget).
 KG_HD int check_floors_mhd(const Grid &G, double *pp, const Geom &g, double rhofloor_bh = -1., Kin *kout = nullptr,
-                           bool *kvalid = nullptr) {
+                           bool *kvalid = nullptr, bool *defer = nullptr) {
   int ret = 0;
   if (kvalid) *kvalid = false;
   const bool magn = kMagn;
@@ -803,6 +811,10 @@ KG_HD int check_floors_mhd(const Grid &G, double *pp, const Geom &g, double rhof
     }
     if (magpre > G.b2rhoratiomax * pp[RHO]) {
       if (kvalid) *kvalid = false;
+      if (defer) {
+        *defer = true;
+        return -1;
+      }
       // normal observer as a relative velocity (relele.c:569-575, 282-307)
       double alp = 1. / sqrt(-g.GG[0][0]);
       double ncov[4] = {-alp, 0., 0., 0.}, etacon[4];

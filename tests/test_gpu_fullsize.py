@@ -84,6 +84,7 @@ def test_torus_192x96x64_steps_from_reference_state(kgpu, oracle):
                   np.count_nonzero(g[..., nonent] != r[..., nonent]))
         t_ref = R.scalar("tstepdenmax")
         assert abs(s.tstepdenmax - t_ref) <= 1e-12 * t_ref
+    print("faces whose state needed the magnetic floor (second flux pass):", s.counters()["face_floors"])
 
 
 @pytest.fixture(scope="module")

@@ -178,6 +178,7 @@ def test_u2p_pause_and_resume_is_exact(kgpu, oracle):
         cnt = s.counters()
         if n == 1:
             assert cnt["paused"] > 0
+        print(f"pass limit {n}: faces whose state needed the magnetic floor over 20 steps: {cnt['face_floors']}")
     for u, p in states[1:]:
         assert np.array_equal(u, states[0][0]) and np.array_equal(p, states[0][1])
 
