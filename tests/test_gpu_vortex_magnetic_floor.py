@@ -6,7 +6,8 @@ floor (u2p.c:617-671) to a second kernel (k_flux_fix), which computes that
 face whole; the vortex with B2RHORATIOMAX = 0.3 (b^2/rho up to 0.7 in the
 initial state) sends faces there on every step.  Bar: as for the other
 vortex runs, every variable but the entropy bit for bit, the entropy to
-1e-12 relative.
+1e-12 relative.  The oracle at this ceiling equals the reference compiled
+with B2RHORATIOMAX = 0.3 bit for bit (tests/test_oracle.py).
 """
 import numpy as np
 import pytest
