@@ -13,8 +13,9 @@ now and then, so the recovered primitives agree to 1e-12 relative.  The
 implicit solve iterates a Newton method whose residual calls pow (the
 Planck function, the Kramers law) and log (the entropy); it is held to the
 reference's own sensitivity to a one-ulp nudge of its input (see that
-test).  Compiled for the host with the host's libm, the same device code
-matches the reference bit for bit in every cell.
+test).  Compiled for the host, with the C library's pow in place of the
+solver's two own powers, the same source matches the reference bit for
+bit in every cell (tests/test_host_physics.py, on the CPU).
 """
 import numpy as np
 import pytest
