@@ -118,7 +118,10 @@ int kgpu_set_density_floor(kgpu_ctx *ctx, const double *centres, const double *x
 /* Flat spacetime (MINKCOORDS) tables generated on the device. */
 int kgpu_set_minkowski_metric(kgpu_ctx *ctx);
 
-/* Conserved (u) and primitive (p) arrays, whole padded grid. */
+/* Conserved (u) and primitive (p) arrays, whole padded grid, in the layout
+ * of KORAL's global arrays u and p (ko.h:275-280, indexed by get_u,
+ * ko.h:505: [SZ][SY][SX][NV], ghost cells included).  download_array reads
+ * one of the context's arrays (KGPU_ARR_*) in the same layout. */
 int kgpu_upload_state(kgpu_ctx *ctx, const double *u, const double *p);
 int kgpu_download_state(kgpu_ctx *ctx, double *u, double *p);
 int kgpu_download_array(kgpu_ctx *ctx, int which, double *out);
@@ -312,7 +315,9 @@ const char *kgpu_u2p_cells_static_error(void);
 int kgpu_get_stream(kgpu_ctx *ctx, void **stream);
 /* When enabled, every launch outside a CUDA graph is bracketed by CUDA
  * events; kgpu_profile_read returns the summed device time and launch count
- * of one kernel kind (0 <= kernel < kgpu_num_kernels()) and its name. */
+ * of one kernel kind (0 <= kernel < kgpu_num_kernels()) and its name.  The
+ * face flux of a direction (k_flux_x/y/z) is timed and counted together
+ * with its magnetic-floor pass, as one. */
 int kgpu_profile_enable(kgpu_ctx *ctx, int on);
 int kgpu_profile_read(kgpu_ctx *ctx, int kernel, double *total_ms, long long *count, const char **name);
 int kgpu_profile_reset(kgpu_ctx *ctx);
