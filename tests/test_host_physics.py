@@ -10,7 +10,8 @@ operation for operation:
 * MHD, at metric points of the Kerr torus: p2u, the three flux rows, the
   wave speeds, the inversion (u2p.c:176, energy and entropy equations and
   the failure path), the floors with the magnetisation ceiling at 100 and
-  at 0.3, PPM and MP5 reconstruction: bit for bit against the oracle.
+  at 0.3; the inversion in flat spacetime up to Lorentz factors of a few
+  hundred; PPM and MP5 reconstruction: bit for bit against the oracle.
 * Radiation, on cells of the batched implicit-solve workload: p2u of the 13
   variables and the M1 inversion (with superluminal fluxes and negative
   energies, which take its corrections) bit for bit against the reference
@@ -179,6 +180,34 @@ def test_mhd_inversion_and_floors_bit_identical(host, torus_cells):
         print(f"floors, ceiling {b2rho}: acted in {np.mean(ra != 0):.3f} of the states")
         assert np.mean(ra != 0) > 0.5
         assert np.array_equal(ra, rb) and np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("vscale", [2., 10., 50.])
+def test_mhd_inversion_flat_high_lorentz_bit_identical(host, oracle, vscale):
+    """Flat spacetime, spatial four-velocity components of scale vscale
+    (Lorentz factors up to a few hundred at 50)."""
+    rng = np.random.default_rng(int(vscale))
+    n = 20000
+    g, G = np.zeros((n, 20)), np.zeros((n, 20))
+    for a, v in ((0, -1.), (6, 1.), (12, 1.), (18, 1.), (19, 1.)):
+        g[:, a] = v
+    for a, v in ((0, -1.), (6, 1.), (12, 1.), (18, 1.)):
+        G[:, a] = v
+    pp = np.zeros((n, 9))
+    pp[:, 0] = 10 ** rng.uniform(-4, 1, n)
+    pp[:, 1] = pp[:, 0] * 10 ** rng.uniform(-4, 1.5, n)
+    pp[:, 2:5] = rng.normal(0, vscale, (n, 3))
+    pp[:, 6:9] = rng.normal(0, 1, (n, 3)) * np.sqrt(pp[:, :1]) * 10 ** rng.uniform(-2, 1, (n, 1))
+    pp[:, 5] = pp[:, 0] * np.log(((2 / 3) * pp[:, 1]) ** 1.5 / pp[:, 0] ** 2.5)
+    O = oracle.OracleGrid(8, 8, 1, 3, 9)
+    O.set_physics(5. / 3., 0.5, 2, 0)
+    uu = O.p2u_batch(pp, g, G)
+    guess = pp * (1 + rng.uniform(-0.1, 0.1, pp.shape))
+    po, so, fo = O.u2p_batch(uu, guess, g, G)
+    ph, rh, fh = guess.copy(), np.zeros(n, np.int32), np.zeros(n, np.int32)
+    host.hp_u2p(ctypes.c_long(n), 0, ctypes.c_double(5. / 3.), ctypes.c_double(100.), P(uu), P(ph), P(g), P(G), I(rh),
+                I(fh))
+    assert np.array_equal(rh, so) and np.array_equal(fh, fo) and np.array_equal(ph, po)
 
 
 @pytest.mark.parametrize("order", [2, 4])
